@@ -1,0 +1,335 @@
+/*
+ * peasoup_b200.h -- C ABI of the B200-native acceleration search.
+ *
+ * Drop-in boundary for Peasoup's per-DM acceleration-search path.  Each
+ * entry point names the reference interface it replaces (file:line in
+ * ewanbarr/peasoup).  Conventions, which differ from the reference on
+ * purpose:
+ *
+ *   - Plain pointers and sizes only; "d_" arguments are device pointers,
+ *     "h_" arguments host pointers.  Complex spectra are interleaved
+ *     (re, im) float pairs, the layout of cufftComplex.
+ *   - Every call returns an int status (PSX_OK == 0); psx_last_error()
+ *     gives a message for the calling thread.  The reference threw
+ *     std::runtime_error instead (include/utils/exceptions.hpp:64-74).
+ *   - Device work is enqueued on the given CUDA stream (0 = legacy default
+ *     stream) and is NOT followed by a device synchronisation; the
+ *     reference synchronised after every launch.  Calls that return host
+ *     values (psx_stats, psx_remove_baseline, psx_find_peaks,
+ *     psx_search_dm) synchronise the given stream only.
+ *   - Nothing here falls back to the CPU: without a usable CUDA device the
+ *     calls fail with PSX_ERR_CUDA.
+ */
+#ifndef PEASOUP_B200_H
+#define PEASOUP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* psx_stream_t; /* == cudaStream_t */
+
+enum {
+    PSX_OK = 0,
+    PSX_ERR_INVALID = 1,     /* bad argument or size */
+    PSX_ERR_CUDA = 2,        /* CUDA runtime error (incl. no device) */
+    PSX_ERR_CUFFT = 3,       /* cuFFT error */
+    PSX_ERR_ALLOC = 4,       /* device or host allocation failed */
+    PSX_ERR_OVERFLOW = 5,    /* caller buffer too small; *n_out has the need */
+    PSX_ERR_UNSUPPORTED = 6, /* valid request this build does not support */
+    PSX_ERR_IO = 7,          /* file could not be read (zap list) */
+    PSX_ERR_BUSY = 8         /* served loop: admission refused / queue full */
+};
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* psx_last_error(void);
+/* Static text for a status code. */
+const char* psx_status_string(int status);
+/* Library version string. */
+const char* psx_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Stage kernels (one launch each, asynchronous on `stream`)           */
+/* ------------------------------------------------------------------ */
+
+/* out[i] = in[rn(i + i*k*(i-size))], k = float(acc*tsamp)/(2c) in double.
+   Replaces device_resampleII (include/kernels/kernels.h:126, src/kernels.cu:355-369)
+   behind TimeDomainResampler::resampleII (include/transforms/resampler.hpp:26-31). */
+int psx_resampleII(const float* d_in, float* d_out, size_t size, float acc,
+                   float tsamp, psx_stream_t stream);
+
+/* Centred form: out[i] = in[rn(i + k*((i-size/2)^2 - (size/2)^2))].
+   Replaces device_resample (kernels.h:118, src/kernels.cu:371-386) behind
+   TimeDomainResampler::resample (resampler.hpp:19-24). */
+int psx_resample(const float* d_in, float* d_out, size_t size, float acc,
+                 float tsamp, psx_stream_t stream);
+
+/* ntrials resampleII outputs of one input, d_out[t*size + i]; h_accs is a
+   host array of ntrials accelerations.  Batched form of device_resampleII
+   (no reference counterpart; the reference resamples one trial per call,
+   src/pipeline_multi.cu:249). */
+int psx_resampleII_batch(const float* d_in, float* d_out, size_t size,
+                         const float* h_accs, int ntrials, float tsamp,
+                         psx_stream_t stream);
+
+/* way 0: amplitude |X_k| (z*rsqrtf(z), 0 where z == 0);
+   way 1: interbinned amplitude sqrt(max(|X_k|^2, 0.5|X_k - X_{k-1}|^2)).
+   Replaces device_form_power_series (kernels.h:111, src/kernels.cu:294-311)
+   behind SpectrumFormer::form / form_interpolated (spectrumformer.hpp:8-22). */
+int psx_form_power_series(const float* d_fseries, float* d_out, size_t nbins,
+                          int way, psx_stream_t stream);
+
+/* out[i] = median of in[5i..5i+4] for i < count/5; counts 1..4 give one
+   value.  Replaces median_scrunch5 (kernels.h:252, src/kernels.cu:974-1008). */
+int psx_median_scrunch5(const float* d_in, size_t count, float* d_out,
+                        psx_stream_t stream);
+
+/* Linear interpolation of in_count samples onto out_count.  Replaces
+   linear_stretch (kernels.h:256, src/kernels.cu:1025-1038). */
+int psx_linear_stretch(const float* d_in, size_t in_count, float* d_out,
+                       size_t out_count, psx_stream_t stream);
+
+/* Bytes of device scratch psx_running_median / psx_deredden need. */
+size_t psx_running_median_scratch_bytes(size_t nbins);
+
+/* Spliced 5/25/125-bin running median of an amplitude spectrum (splice at
+   b5 and b25 Hz).  Replaces Dereddener::calculate_median
+   (include/transforms/dereddener.hpp:41-62). */
+int psx_running_median(const float* d_powers, size_t nbins, double bin_width,
+                       float b5, float b25, float* d_median, void* d_scratch,
+                       psx_stream_t stream);
+
+/* X_k /= f_k (complex / real), bins 0..4 zeroed.  Replaces
+   device_divide_c_by_f (kernels.h:262, src/kernels.cu:1040-1061) behind
+   Dereddener::deredden (dereddener.hpp:64-66). */
+int psx_divide_c_by_f(float* d_fseries, const float* d_f, size_t nbins,
+                      psx_stream_t stream);
+
+/* Running median of d_powers and the division of d_fseries by it in one
+   pass (the median is never written).  Replaces the pair
+   Dereddener::calculate_median + Dereddener::deredden
+   (dereddener.hpp:41-66) as called at src/pipeline_multi.cu:213-217. */
+int psx_deredden(float* d_fseries, const float* d_powers, size_t nbins,
+                 double bin_width, float b5, float b25, void* d_scratch,
+                 psx_stream_t stream);
+
+/* Sets bins [floor((f-w)/bw), ceil((f+w)/bw)) of each birdie to 1+0i.
+   Replaces device_zap_birdies (kernels.h:268, src/kernels.cu:1063-1096)
+   behind Zapper::zap (birdiezapper.hpp:61-71). */
+int psx_zap_birdies(float* d_fseries, const float* d_freqs,
+                    const float* d_widths, float bin_width, size_t nbirdies,
+                    size_t nbins, psx_stream_t stream);
+
+/* Parses a zap list ("freq width" per line, birdiezapper.hpp:35-46) into
+   host arrays.  With h_freqs == NULL only *n is set. */
+int psx_read_zaplist(const char* path, float* h_freqs, float* h_widths,
+                     size_t cap, size_t* n);
+
+/* mean, rms and std = sqrt(rms^2 - mean^2) of d_x[first..n).  Synchronous
+   (synchronises `stream`).  Replaces stats::stats / GPU_mean / GPU_rms
+   (include/utils/stats.hpp:25-33, src/kernels.cu:433-461). */
+int psx_stats(const float* d_x, size_t n, size_t first, float* h_mean,
+              float* h_rms, float* h_std, psx_stream_t stream);
+
+/* x = (x - mean) / sigma in place.  Replaces device_normalise
+   (kernels.h:144, src/kernels.cu:496-521) behind stats::normalise
+   (stats.hpp:35-40). */
+int psx_normalise(float* d_x, float mean, float sigma, size_t n,
+                  psx_stream_t stream);
+
+/* Iterative mean removal (until |mean| <= 5e-7 n, at most 102 passes);
+   synchronous.  Replaces GPU_remove_baseline (src/kernels.cu:463-479)
+   behind DeviceTimeSeries::remove_baseline (timeseries.hpp:282-287).
+   *h_passes (may be NULL) receives the number of passes. */
+int psx_remove_baseline(float* d_x, size_t n, int* h_passes,
+                        psx_stream_t stream);
+
+/* d_x[0..n) = value.  Replaces GPU_fill (src/kernels.cu:482-488). */
+int psx_fill(float* d_x, size_t n, float value, psx_stream_t stream);
+
+/* Type conversion to float.  Replaces device_conversion<X,float>
+   (kernels.h:322, src/kernels.cu:1171-1200). */
+int psx_convert_u8_f32(const uint8_t* d_in, float* d_out, size_t n,
+                       psx_stream_t stream);
+int psx_convert_i8_f32(const int8_t* d_in, float* d_out, size_t n,
+                       psx_stream_t stream);
+
+/* Fractional harmonic sums: nharms (0..5) output spectra of n bins, output
+   h_out_ptrs[h] = device pointer for fold h+1.  The pointer array is read
+   on the host and passed by value (no copy to the device).  Replaces
+   device_harmonic_sum (kernels.h:104, src/kernels.cu:34-100, 200-209)
+   behind HarmonicFolder::fold (harmonicfolder.hpp:26-38). */
+int psx_harmonic_sum(const float* d_in, float* const* h_out_ptrs, size_t n,
+                     int nharms, psx_stream_t stream);
+
+/* Order-preserving compaction of (index, value) pairs with value > thresh
+   over [start, n) into device arrays of capacity `cap`; *h_count receives
+   the number above threshold (may exceed cap: then PSX_ERR_OVERFLOW).
+   Synchronous.  Replaces device_find_peaks (kernels.h:134-142,
+   src/kernels.cu:398-423), whose Thrust types cannot cross a C ABI. */
+int psx_find_peaks(const float* d_spec, int n, int start, float thresh,
+                   int* d_idx, float* d_val, int cap, int* h_count,
+                   psx_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* Real transforms (cuFFT)                                             */
+/* ------------------------------------------------------------------ */
+
+typedef struct psx_fft_plan psx_fft_plan;
+enum { PSX_FFT_R2C = 0, PSX_FFT_C2R = 1 };
+
+/* Unnormalised R2C / C2R plan of length `size`, `batch` transforms with
+   input/output distances size and size/2+1.  Replaces CuFFTerR2C /
+   CuFFTerC2R (include/transforms/ffter.hpp:90-146). */
+int psx_fft_plan_create(psx_fft_plan** plan, size_t size, long long batch,
+                        int kind);
+int psx_fft_exec(psx_fft_plan* plan, const void* d_in, void* d_out,
+                 psx_stream_t stream);
+int psx_fft_plan_destroy(psx_fft_plan* plan);
+
+/* ------------------------------------------------------------------ */
+/* Host logic (no GPU)                                                 */
+/* ------------------------------------------------------------------ */
+
+/* Same field order and size as the reference's CandidatePOD
+   (include/data_types/candidates.hpp:10-17), the record written to
+   candidates.peasoup. */
+typedef struct {
+    float dm;
+    int dm_idx;
+    float acc;
+    int nh;
+    float snr;
+    float freq;
+} psx_candidate;
+
+/* Acceleration trial list of one DM.  Replaces
+   AccelerationPlan::generate_accel_list (include/utils/utils.hpp:198-232);
+   all arithmetic in float as there.  With h_out == NULL only *n is set. */
+int psx_accel_list(float acc_lo, float acc_hi, float tol, float pulse_width_s,
+                   size_t nsamps, float tsamp, float cfreq_hz, float ch_bw_hz,
+                   float dm, float cdm, float* h_out, size_t cap, size_t* n);
+
+/* Search range [*start, *end) and frequency factor of a spectrum with
+   harmonic number nh.  Restates peakfinder.hpp:123-134. */
+int psx_peak_range(unsigned nbins, double bin_width, int nh, float min_freq,
+                   float max_freq, int* start, int* end, float* factor);
+
+/* Cluster sorted above-threshold bins (min_gap rule of
+   PeakFinder::identify_unique_peaks, peakfinder.hpp:72-101). */
+size_t psx_identify_unique_peaks(const int* idx, const float* snr,
+                                 size_t count, int min_gap, int* out_idx,
+                                 float* out_snr);
+
+enum { PSX_DISTILL_HARMONIC = 0, PSX_DISTILL_ACCEL = 1, PSX_DISTILL_DM = 2 };
+
+/* Candidate distillation in place: cands are sorted by descending S/N and
+   the survivors are moved to the front, in that order; returns their
+   count.  h_nassoc (may be NULL, n entries) receives each survivor's
+   association count (Candidate::count_assoc when keep_related is set).
+   kind HARMONIC: HarmonicDistiller(tol, max_harm, keep_related,
+   fractional) (distiller.hpp:63-108); ACCEL: AccelerationDistiller(tobs,
+   tol, keep_related) (:115-163); DM: DMDistiller(tol, keep_related)
+   (:167-196). */
+size_t psx_distill(int kind, psx_candidate* cands, size_t n, float tol,
+                   float max_harm, float tobs, int keep_related,
+                   int fractional, int* h_nassoc);
+
+/* ------------------------------------------------------------------ */
+/* Per-DM acceleration search (the fused hot path)                     */
+/* ------------------------------------------------------------------ */
+
+enum {
+    PSX_MODE_PLAIN = 0,   /* one acceleration trial per launch sequence */
+    PSX_MODE_BATCHED = 1  /* many trials per launch, graph-captured */
+};
+
+typedef struct {
+    size_t fft_size;           /* N: 2^k or 3*2^k, 1024 <= N <= 2^28 */
+    float tsamp;               /* s */
+    float cdm;                 /* coherent DM of the acceleration plan */
+    float acc_lo, acc_hi;      /* m/s^2 */
+    float acc_tol;             /* AccelerationPlan tolerance (1.10) */
+    float acc_pulse_width;     /* s (64e-6) */
+    float cfreq_hz, ch_bw_hz;  /* centre frequency and channel width */
+    int nharmonics;            /* folds, 0..5 (4) */
+    float min_snr;             /* (9) */
+    float min_freq, max_freq;  /* Hz (0.1, 1100) */
+    int min_gap;               /* bins (30) */
+    float freq_tol;            /* (1e-4) */
+    float max_harm;            /* (16) */
+    float boundary_5_freq;     /* (0.05) */
+    float boundary_25_freq;    /* (0.5) */
+    const float* birdie_freqs; /* host, may be NULL */
+    const float* birdie_widths;
+    size_t nbirdies;
+    int mode;                  /* PSX_MODE_* */
+    int batch;                 /* trials per launch (batched); 0 = tuned */
+    int use_fft_callback;      /* batched: fuse the resample into cuFFT */
+    int use_graph;             /* batched: capture the trial schedule */
+} psx_search_config;
+
+/* Fills `cfg` with the reference's defaults (include/utils/cmdline.hpp:
+   99-191) for a transform of `fft_size` samples of `tsamp` s. */
+void psx_search_config_defaults(psx_search_config* cfg, size_t fft_size,
+                                float tsamp);
+
+typedef struct psx_search psx_search;
+
+/* Device memory one search instance holds (admission model). */
+size_t psx_search_footprint(const psx_search_config* cfg);
+
+/* Allocates buffers and plans for `cfg` on the current device.  Replaces
+   the per-thread set-up of Worker::start (src/pipeline_multi.cu:114-152). */
+int psx_search_create(const psx_search_config* cfg, psx_search** s);
+int psx_search_destroy(psx_search* s);
+/* Stream used by the instance (default: a private non-blocking stream). */
+int psx_search_set_stream(psx_search* s, psx_stream_t stream);
+
+enum {
+    PSX_OUT_TRIAL = 0,  /* per-trial harmonic-distilled candidates */
+    PSX_OUT_DM = 1      /* plus the per-DM acceleration distillation:
+                           the reference Worker's dm_trial_cands */
+};
+
+/* Searches one dedispersed series: the body of the reference's DM loop,
+   src/pipeline_multi.cu:161-294 (copy, baseline removal, padding, R2C,
+   dereddening, zapping, statistics, C2R, then every acceleration trial:
+   resample, R2C, interbinning, normalisation, harmonic sums, peak
+   finding, harmonic distillation).  `series` is host memory unless
+   series_on_device.  Candidates are written to h_out in the reference's
+   order; h_nassoc (may be NULL) gets association counts (PSX_OUT_DM);
+   h_trial (may be NULL) gets each candidate's acceleration-trial index.
+   Synchronous.  PSX_ERR_OVERFLOW when cap is too small (*n_out = need). */
+int psx_search_dm(psx_search* s, const float* series, size_t nsamps,
+                  int series_on_device, float dm, int dm_idx, int output,
+                  psx_candidate* h_out, int* h_nassoc, int* h_trial,
+                  size_t cap, size_t* n_out);
+
+typedef struct {
+    int ntrials;          /* acceleration trials of the last call */
+    int nbatches;         /* launch groups of the last call */
+    int kernel_launches;  /* kernels this library launched */
+    int fft_launches;     /* cuFFT executions */
+    long long above_threshold; /* (bin, fold) pairs above threshold */
+    int fft_callback;     /* 1 if the resample ran inside cuFFT */
+    int graph;            /* 1 if the trial schedule ran as a CUDA graph */
+    int batch;            /* trials per launch used */
+} psx_search_info;
+
+int psx_search_last_info(const psx_search* s, psx_search_info* info);
+
+/* Debug tap: the dereddened series of the last call (N floats, scaled by
+   N as the reference leaves it) and, for trial `trial` of the last call,
+   its resampled series (N floats) and normalised interbinned spectrum
+   (N/2+1 floats), recomputed on the device.  Any pointer may be NULL. */
+int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
+                         float* h_tim_r, float* h_pspec, float* h_norm2);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PEASOUP_B200_H */

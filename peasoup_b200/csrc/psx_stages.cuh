@@ -1,0 +1,40 @@
+// psx_stages.cuh -- launchers of the single-stage kernels, shared with the
+// search engine (psx_search.cu).  All are asynchronous on `s`.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace psx {
+
+double accel_fact(float acc, float tsamp);
+
+// ntrials outputs; trial t uses d_ktab[t] (or k when d_ktab is null) and is
+// written at d_out + t*out_pitch.
+int launch_resample(const float* d_in, float* d_out, size_t n, const double* d_ktab, double k,
+                    int ntrials, size_t out_pitch, bool centred, cudaStream_t s);
+
+size_t median_scratch_bytes(size_t nbins);
+
+// Median levels + splice; writes the median (d_median) and/or divides the
+// spectrum d_X by it (bins 0..4 zeroed).
+int launch_running_median(const float* d_powers, size_t nbins, double bin_width, float b5,
+                          float b25, float* d_median, float* d_X, void* d_scratch,
+                          cudaStream_t s);
+
+int launch_zap(float* d_X, const float* d_freqs, const float* d_widths, float bin_width,
+               size_t nbirdies, size_t nbins, cudaStream_t s);
+
+int reduction_blocks();
+
+// Sums of x (or of the interbinned amplitude of the complex spectrum x)
+// over [first, n); d_stat (5 floats) receives mean, rms, std,
+// mean*scale, std*scale.
+int launch_stats(const float* d_x, bool interbinned, size_t first, size_t n, double2* d_partials,
+                 double* d_sums, float* d_stat, float scale, cudaStream_t s);
+
+int remove_baseline_pass(float* d_x, size_t n, double2* d_partials, double* d_sums,
+                         float* d_mean, cudaStream_t s);
+
+int launch_fill(float* d_x, size_t n, float value, cudaStream_t s);
+
+}  // namespace psx

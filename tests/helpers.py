@@ -1,0 +1,41 @@
+"""Comparison helpers shared by the parity tests."""
+import numpy as np
+
+
+def rel_err(a, b, floor_frac=1e-3):
+    """max |a-b| / max(|b|, floor) with the floor a fraction of the RMS of
+    b, so that bins near zero are judged against the spectrum's scale."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.sqrt(np.mean(np.abs(b) ** 2)) if b.size else 1.0
+    den = np.maximum(np.abs(b), floor_frac * scale + 1e-300)
+    return float(np.max(np.abs(a - b) / den)) if a.size else 0.0
+
+
+def err_vs_rms(a, b):
+    """max |a-b| relative to the RMS of b."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.sqrt(np.mean(np.abs(b) ** 2)) if b.size else 1.0
+    return float(np.max(np.abs(a - b)) / scale) if a.size else 0.0
+
+
+def cand_key(c):
+    return (int(c["dm_idx"]), float(c["acc"]), int(c["nh"]), float(c["freq"]))
+
+
+def match_candidates(a, b, thresh, snr_rtol=1e-3, margin=2e-3):
+    """Compare two candidate lists (structured arrays with dm_idx, acc, nh,
+    freq, snr).  Exact (dm_idx, acc, nh, freq) identity is required for
+    every candidate whose S/N clears the threshold by more than `margin`
+    (relative); S/N of matched pairs must agree within snr_rtol.  Returns
+    (n_matched, unmatched_a, unmatched_b, worst_snr_rel)."""
+    ka = {cand_key(c): float(c["snr"]) for c in a}
+    kb = {cand_key(c): float(c["snr"]) for c in b}
+    matched = set(ka) & set(kb)
+    worst = 0.0
+    for k in matched:
+        worst = max(worst, abs(ka[k] - kb[k]) / max(abs(kb[k]), 1e-30))
+    ua = [(k, s) for k, s in ka.items() if k not in kb and s > thresh * (1 + margin)]
+    ub = [(k, s) for k, s in kb.items() if k not in ka and s > thresh * (1 + margin)]
+    return len(matched), ua, ub, worst

@@ -1,0 +1,99 @@
+"""The C-ABI library on the CPU: it loads, exports every entry point the
+public header declares, and its host logic (acceleration plan, peak
+ranges, clustering, distillers, zap-list parsing) matches the oracle and
+the reference.  No GPU work is issued here."""
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from peasoup_b200 import _lib
+
+
+def test_library_exports_every_declared_symbol(psx):
+    declared = _lib.declared_symbols()
+    assert len(declared) >= 36
+    missing = [s for s in declared if not hasattr(psx, s)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert set(declared) <= exported
+    # every declared function has a ctypes signature in the binding
+    assert set(declared) == set(_lib.SIGNATURES)
+
+
+def test_library_is_built_for_sm100a():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH],
+                         capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+def test_status_and_version_strings(psx):
+    assert b"sm_100a" in psx.psx_version()
+    assert psx.psx_status_string(0) == b"ok"
+    assert psx.psx_status_string(_lib.PSX_ERR_OVERFLOW) == b"output buffer too small"
+
+
+def test_invalid_arguments_fail_loudly(psx):
+    assert psx.psx_resampleII(None, None, 0, 1.0, 1e-4, None) == _lib.PSX_ERR_INVALID
+    assert b"resample" in psx.psx_last_error()
+    assert psx.psx_harmonic_sum(C.c_void_p(8), None, 16, 6, None) == _lib.PSX_ERR_INVALID
+    cfg = _lib.SearchConfig()
+    psx.psx_search_config_defaults(C.byref(cfg), 1000, 64e-6)  # not 2^k or 3*2^k
+    h = C.c_void_p()
+    assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
+    psx.psx_search_config_defaults(C.byref(cfg), 1 << 16, 64e-6)
+    cfg.nharmonics = 6
+    assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
+    assert b"nharmonics" in psx.psx_last_error()
+
+
+def test_no_cpu_fallback_without_device(psx):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    cfg = _lib.SearchConfig()
+    psx.psx_search_config_defaults(C.byref(cfg), 1 << 16, 64e-6)
+    h = C.c_void_p()
+    rc = psx.psx_search_create(C.byref(cfg), C.byref(h))
+    assert rc in (_lib.PSX_ERR_CUDA, _lib.PSX_ERR_ALLOC)
+    from peasoup_b200 import transforms
+    with pytest.raises(_lib.PsxError):
+        transforms.DeviceTimeSeries(16)
+
+
+def test_footprint_model(psx):
+    from peasoup_b200.search import SearchParams, footprint
+    small = footprint(SearchParams(fft_size=1 << 20, tsamp=64e-6))
+    big = footprint(SearchParams(fft_size=1 << 23, tsamp=76e-6))
+    assert 0 < small < big
+    plain = footprint(SearchParams(fft_size=1 << 23, tsamp=76e-6, mode="plain"))
+    assert plain < big
+
+
+def test_zaplist_parsing(psx):
+    fd, path = tempfile.mkstemp(suffix=".txt")
+    with os.fdopen(fd, "w") as f:
+        f.write("50.000 0.100\n\n100.00 0.15\n  150.00   0.15  extra\n")
+    try:
+        n = C.c_size_t()
+        assert psx.psx_read_zaplist(path.encode(), None, None, 0, C.byref(n)) == 0
+        assert n.value == 3
+        fr = np.zeros(3, np.float32)
+        wd = np.zeros(3, np.float32)
+        assert psx.psx_read_zaplist(path.encode(), fr.ctypes.data, wd.ctypes.data, 3,
+                                    C.byref(n)) == 0
+        assert list(fr) == [50.0, 100.0, 150.0]
+        assert np.allclose(wd, [0.1, 0.15, 0.15])
+        assert psx.psx_read_zaplist(path.encode(), fr.ctypes.data, wd.ctypes.data, 2,
+                                    C.byref(n)) == _lib.PSX_ERR_OVERFLOW
+    finally:
+        os.unlink(path)
+    assert psx.psx_read_zaplist(b"/nonexistent/zaplist", None, None, 0,
+                                C.byref(C.c_size_t())) == _lib.PSX_ERR_IO
