@@ -1,0 +1,476 @@
+#!/usr/bin/env python
+"""Benchmark of the per-DM acceleration search (Peasoup's hot loop) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl psx|reference]
+
+Workload (the survey-shape configuration the headline metric is quoted on):
+256 DM trials x 2^23 float32 samples, tsamp 76 us, uint8-quantised noise
+(mean 128, sigma 20) with 1/f^1.5 red noise below 1 Hz, 5 injected
+accelerated pulsars, 20 birdies injected and zapped, acceleration range
+-100..100 m/s^2 at the default tolerance, 5 harmonic folds, S/N threshold 9
+(the reference's default).  Data are seeded synthetic series made on the
+GPU (no survey data offline).  A step searches `--dms-per-step` DM trials
+(prologue + every acceleration trial + candidate distillation); K steps
+cover K*S DM trials of the 256 (weak scaling over ranks: rank r takes its
+own DM trials).  Every step's series (8 x 32 MB) exceed L2.
+
+Printed: one JSON line.  `value` = DM x acceleration trials per second of
+the batched path with the series resident in HBM; `e2e` = the same through
+the C ABI (psx_search_block) from pinned host buffers (host->device copies
+inside the timed region, candidates copied back); `plain` = the one-trial-
+per-launch path on a sample of the same workload; `roofline` = the
+dominant stage's achieved HBM bytes/s against the measured copy bandwidth;
+`cpu_baseline` = the FP64 CPU oracle on a bounded sample.
+
+`--impl reference` times the reference's own implementation of the path
+(its src/kernels.cu, transforms and unmodified Worker, built for sm_100a
+into oracle/_ref) on the same workload, one DM trial per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DM×accel trials/s at 2^23 pts batched vs plain, %HBM roofline; served p50/p99"
+N_FFT = 1 << 23
+TSAMP = 76e-6
+ACC = 100.0
+NFOLDS = 5
+NDM = 256
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = str(index)
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(index).uuid)
+            self.index = u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            pass
+        self.proc = None
+        self.f = tempfile.TemporaryFile(mode="w+")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def dm_schedule(rank, ws, steps, per_step, offset=0):
+    """DM indices of each step of this rank (rank-interleaved blocks)."""
+    out = []
+    for s in range(steps):
+        base = ((offset + s) * ws + rank) * per_step
+        out.append([(base + j) % NDM for j in range(per_step)])
+    return out
+
+
+def trials_of(plan, dm_list):
+    from peasoup_b200 import synth
+    from peasoup_b200.transforms import AccelerationPlan
+    ap = AccelerationPlan(-ACC, ACC, 1.10, 64e-6, N_FFT, TSAMP, synth.CFREQ_HZ, synth.CH_BW_HZ)
+    return sum(len(ap.generate_accel_list(float(plan.dms[d]), 0.0)) for d in dm_list)
+
+
+def make_params(plan, mode="batched", batch=0):
+    from peasoup_b200 import search, synth
+    return search.SearchParams(fft_size=N_FFT, tsamp=TSAMP, acc_lo=-ACC, acc_hi=ACC,
+                               nharmonics=NFOLDS, cfreq_hz=synth.CFREQ_HZ,
+                               ch_bw_hz=synth.CH_BW_HZ, birdie_freqs=plan.birdie_freqs,
+                               birdie_widths=plan.birdie_widths, mode=mode, batch=batch)
+
+
+# ----------------------------------------------------------------- reference
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    if not os.path.exists(O.REF_GPU_PATH):
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "unavailable": "oracle/_ref/libpeasoup_ref_gpu.so not built "
+                                         "(build() compiles it where the reference sources "
+                                         "exist)"}), flush=True)
+        return 0
+    import torch
+    from peasoup_b200 import synth
+    plan = synth.survey_plan(ndm=NDM, nsamps=N_FFT, tsamp=TSAMP)
+    sched = dm_schedule(0, 1, args.warmup + args.steps, 1)
+    dmsel = sorted({d for st in sched for d in st})
+    block = synth.survey_block_torch(plan, dm_indices=dmsel)
+    host = {d: block[i].cpu().numpy() for i, d in enumerate(dmsel)}
+    del block
+    torch.cuda.empty_cache()
+    p = O.SearchParams(fft_size=N_FFT, tsamp=TSAMP, acc_lo=-ACC, acc_hi=ACC, nharmonics=NFOLDS,
+                       cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ)
+    fd, zap = tempfile.mkstemp(suffix=".txt")
+    with os.fdopen(fd, "w") as f:
+        f.write(plan.zaplist_text())
+    try:
+        for st in sched[:args.warmup]:
+            d = st[0]
+            O.ref_worker_search(host[d][None, :], TSAMP, plan.dms[d:d + 1], N_FFT, p, zap)
+        torch.cuda.synchronize()
+        ntr = 0
+        t0 = time.perf_counter()
+        for st in sched[args.warmup:]:
+            d = st[0]
+            O.ref_worker_search(host[d][None, :], TSAMP, plan.dms[d:d + 1], N_FFT, p, zap)
+            ntr += trials_of(plan, [d])
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    finally:
+        os.unlink(zap)
+    v = ntr / dt
+    sample = (f"{args.steps} DM trials of the survey workload (one per step, "
+              f"{ntr} acceleration trials), reference kernels.cu + unmodified Worker on the GPU")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "trials/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "survey-2^23 (256 DM x 2^23, tsamp 76us, acc +-100, 5 folds, "
+                               "20 birdies)", "dms_per_step": 1},
+        "cpu_baseline": {"value": v, "unit": "trials/s", "cores": 1, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": "trials/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_baseline(plan, block_row, dm):
+    """FP64 oracle on a bounded sample: one DM trial with 1 and with 3
+    acceleration trials; per-trial and per-DM costs are separated and the
+    throughput extrapolated to the workload's trials per DM."""
+    from oracle import oracle as O
+    from peasoup_b200 import synth
+    x = block_row
+
+    def run(lo, hi):
+        p = O.SearchParams(fft_size=N_FFT, tsamp=TSAMP, dm=float(dm), acc_lo=lo, acc_hi=hi,
+                           nharmonics=NFOLDS, cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ,
+                           birdie_freqs=plan.birdie_freqs, birdie_widths=plan.birdie_widths)
+        t0 = time.perf_counter()
+        O.search_dm(x, p)
+        return time.perf_counter() - t0
+
+    t1 = run(0.0, 0.0)
+    t3 = run(-1.0, 1.0)      # {-1, 0, 1}: three trials
+    per_trial = max(1e-9, (t3 - t1) / 2.0)
+    per_dm = max(0.0, t1 - per_trial)
+    return per_trial, per_dm, t1 + t3
+
+
+# ----------------------------------------------------------------- main arm
+def run_psx(args, ws, rank, local):
+    import torch
+    from peasoup_b200 import search, synth
+    from peasoup_b200.build import build
+    build()
+    peak, peak_kind = peaks()
+    S = args.dms_per_step
+    plan = synth.survey_plan(ndm=NDM, nsamps=N_FFT, tsamp=TSAMP)
+    warm = dm_schedule(rank, ws, args.warmup, S, offset=args.steps)
+    timed = dm_schedule(rank, ws, args.steps, S)
+    need = sorted({d for st in warm + timed for d in st})
+    t0 = time.perf_counter()
+    block = synth.survey_block_torch(plan, dm_indices=need)
+    torch.cuda.synchronize()
+    row = {d: i for i, d in enumerate(need)}
+    log(f"[rank {rank}] synthesised {len(need)} series in {time.perf_counter() - t0:.1f}s")
+
+    stream = torch.cuda.Stream()
+    eng = search.AccelSearch(make_params(plan, "batched", args.batch))
+    eng.set_stream(stream.cuda_stream)
+
+    def do_step(dm_list, src):
+        rows = [src[row[d]] for d in dm_list] if src is block else [src[d] for d in dm_list]
+        return eng.search_block(rows, plan.dms[dm_list], np.array(dm_list, np.int32))
+
+    # ---- warm-up (untimed)
+    for st in warm:
+        do_step(st, block)
+    torch.cuda.synchronize()
+
+    # ---- timed: series resident in HBM
+    eng.set_profile(True)
+    eng.profile(reset=True)
+    ntr = sum(trials_of(plan, st) for st in timed)
+    launches = 0
+    ncand = 0
+    with ClockSampler(local) as clk:
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for st in timed:
+            c = do_step(st, block)[0]
+            ncand += len(c)
+            launches += eng.info()["kernel_launches"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+    dt = e0.elapsed_time(e1) / 1e3
+    prof = eng.profile(reset=True)
+    eng.set_profile(False)
+    batch_used = eng.info()["batch"]
+    dt_max = max_over_ranks(ws, dt)
+    tot_trials = sum_over_ranks(ws, ntr)
+    value = tot_trials / dt_max
+    clocks = clk.summary()
+
+    # ---- e2e through the C ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        host = {}
+        for st in timed + warm[:1]:
+            for d in st:
+                if d not in host:
+                    h = torch.empty(N_FFT, dtype=torch.float32, pin_memory=True)
+                    h.copy_(block[row[d]])
+                    host[d] = h.numpy()
+        do_step(warm[0] if warm else timed[0], host)
+        torch.cuda.synchronize()
+        barrier(ws)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        nc2 = 0
+        for st in timed:
+            c = do_step(st, host)[0]
+            nc2 += len(c)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        dte = max_over_ranks(ws, f0.elapsed_time(f1) / 1e3)
+        e2e = {"value": tot_trials / dte, "unit": "trials/s",
+               "h2d_bytes_per_step": S * N_FFT * 4,
+               "d2h_bytes_per_step": int(nc2 / max(1, len(timed))) * 24}
+        del host
+
+    # ---- plain path (one trial per launch) on a sample
+    plain = None
+    if not args.no_plain:
+        eng_p = search.AccelSearch(make_params(plan, "plain"))
+        eng_p.set_stream(stream.cuda_stream)
+        ps = timed[:max(1, len(timed) // 4)]
+        eng_p.search_block([block[row[d]] for d in ps[0][:1]], plan.dms[ps[0][:1]])
+        torch.cuda.synchronize()
+        barrier(ws)
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for st in ps:
+            eng_p.search_block([block[row[d]] for d in st], plan.dms[st])
+        g1.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        dtp = max_over_ranks(ws, g0.elapsed_time(g1) / 1e3)
+        ntp = sum_over_ranks(ws, sum(trials_of(plan, st) for st in ps))
+        plain = {"value": ntp / dtp, "unit": "trials/s", "steps": len(ps),
+                 "batched_over_plain": value / (ntp / dtp)}
+        eng_p.close()
+
+    # ---- roofline of the dominant stage (CUDA events on the engine stream)
+    B = N_FFT // 2 + 1
+    per_trial_bytes = {  # algorithmic bytes per acceleration trial and stage
+        "resample": 8.0 * N_FFT,          # read + write the series
+        "fft": 4.0 * N_FFT + 8.0 * B,     # read the series, write the spectrum
+        "form": 8.0 * B + 4.0 * B,        # read the spectrum, write the amplitudes
+        "harm": 4.0 * B,                  # read the normalised spectrum once
+    }
+    stage_ms = {"resample": prof["resample_ms"], "fft": prof["fft_ms"],
+                "form": prof["form_ms"], "harm": prof["harm_ms"]}
+    trials_prof = max(1, prof["trials"])
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+    stages = {}
+    for k, ms in stage_ms.items():
+        sec = ms / 1e3 / trials_prof
+        stages[k] = {"us_per_trial": sec * 1e6,
+                     "gbs": per_trial_bytes[k] / sec / 1e9 if sec > 0 else None}
+    achieved = stages[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                "traffic": traffic, "peak_kind": peak_kind,
+                "bytes_per_trial": per_trial_bytes[dom], "stages": stages}
+    # end-to-end algorithmic roofline of the whole search (12N per trial,
+    # 24N per DM prologue)
+    ndm_total = sum_over_ranks(ws, sum(len(st) for st in timed))
+    alg = (ndm_total * 24.0 * N_FFT + tot_trials * 12.0 * N_FFT) / dt_max
+    hbm_frac = alg / (peak * 1e9)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        d0 = timed[0][0]
+        x = block[row[d0]].cpu().numpy()
+        per_trial, per_dm, spent = cpu_baseline(plan, x, plan.dms[d0])
+        avg_trials = ntr / max(1, sum(len(st) for st in timed))
+        cpu_v = avg_trials / (per_dm + avg_trials * per_trial)
+        cpu = {"value": cpu_v, "unit": "trials/s", "cores": 1, "kind": "port",
+               "sample": (f"FP64 oracle, one 2^23 DM trial with 1 and with 3 acceleration "
+                          f"trials ({spent:.1f}s): {per_trial:.2f}s per trial, "
+                          f"{per_dm:.2f}s per DM prologue, extrapolated to "
+                          f"{avg_trials:.1f} trials per DM")}
+    eng.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt_max / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded survey-shape series made on the GPU)",
+            "config": {"workload": "survey-2^23: 256 DM trials x 2^23 samples, tsamp 76us, "
+                                   "acc -100..100, 5 folds, S/N 9, 20 birdies zapped",
+                       "dms_per_step": S, "mode": "batched",
+                       "batch": batch_used,
+                       "parallelism": f"dm-sharded x{ws}",
+                       "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
+            "hbm_roofline_frac": hbm_frac,
+            "plain": plain, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clocks, "gpu_launches": launches, "candidates": ncand,
+            "trials": int(tot_trials),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=32)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="psx", choices=["psx", "reference"])
+    ap.add_argument("--dms-per-step", type=int, default=8)
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, ws, rank)
+        else:
+            rc = run_psx(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

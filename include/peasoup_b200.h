@@ -309,6 +309,17 @@ int psx_search_dm(psx_search* s, const float* series, size_t nsamps,
                   psx_candidate* h_out, int* h_nassoc, int* h_trial,
                   size_t cap, size_t* n_out);
 
+/* Searches `ndm` dedispersed series (series[d], host pointers unless
+   series_on_device) of the same length: the reference Worker's DM loop
+   (src/pipeline_multi.cu:155-295) for a block of DM trials.  The host
+   clusters and distils DM d while the GPU already searches DM d+1.
+   Output as psx_search_dm for every DM in turn; h_dm (may be NULL)
+   receives each candidate's position in the block.  Synchronous. */
+int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
+                     int series_on_device, const float* dms, const int* dm_idx,
+                     int ndm, int output, psx_candidate* h_out, int* h_nassoc,
+                     int* h_trial, int* h_dm, size_t cap, size_t* n_out);
+
 typedef struct {
     int ntrials;          /* acceleration trials of the last call */
     int nbatches;         /* launch groups of the last call */
@@ -318,9 +329,26 @@ typedef struct {
     int fft_callback;     /* 1 if the resample ran inside cuFFT */
     int graph;            /* 1 if the trial schedule ran as a CUDA graph */
     int batch;            /* trials per launch used */
+    int baseline_passes;  /* mean-removal passes of the last DM (-1: host loop) */
 } psx_search_info;
 
 int psx_search_last_info(const psx_search* s, psx_search_info* info);
+
+/* Per-stage device time from CUDA events recorded on the instance's
+   stream around every launch group (when enabled). */
+typedef struct {
+    double prologue_ms;   /* per-DM prologue */
+    double resample_ms;   /* resample gathers */
+    double fft_ms;        /* trial R2C transforms */
+    double form_ms;       /* interbin + normalise */
+    double harm_ms;       /* harmonic sums + threshold + compaction */
+    long long groups;     /* launch groups timed */
+    long long trials;     /* acceleration trials timed */
+    long long dms;        /* DM trials timed */
+} psx_search_profile;
+
+int psx_search_set_profile(psx_search* s, int on);
+int psx_search_get_profile(psx_search* s, psx_search_profile* out, int reset);
 
 /* Debug tap: the dereddened series of the last call (N floats, scaled by
    N as the reference leaves it) and, for trial `trial` of the last call,

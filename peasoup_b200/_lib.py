@@ -64,7 +64,14 @@ class SearchConfig(C.Structure):
 class SearchInfo(C.Structure):
     _fields_ = [("ntrials", C.c_int), ("nbatches", C.c_int), ("kernel_launches", C.c_int),
                 ("fft_launches", C.c_int), ("above_threshold", C.c_longlong),
-                ("fft_callback", C.c_int), ("graph", C.c_int), ("batch", C.c_int)]
+                ("fft_callback", C.c_int), ("graph", C.c_int), ("batch", C.c_int),
+                ("baseline_passes", C.c_int)]
+
+
+class SearchProfile(C.Structure):
+    _fields_ = [("prologue_ms", C.c_double), ("resample_ms", C.c_double),
+                ("fft_ms", C.c_double), ("form_ms", C.c_double), ("harm_ms", C.c_double),
+                ("groups", C.c_longlong), ("trials", C.c_longlong), ("dms", C.c_longlong)]
 
 
 _vp = C.c_void_p
@@ -111,7 +118,11 @@ SIGNATURES = {
     "psx_search_destroy": (_i, [_vp]),
     "psx_search_set_stream": (_i, [_vp, _vp]),
     "psx_search_dm": (_i, [_vp, _vp, _sz, _i, _f, _i, _i, _vp, _vp, _vp, _sz, C.POINTER(_sz)]),
+    "psx_search_block": (_i, [_vp, _vp, _sz, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _sz,
+                              C.POINTER(_sz)]),
     "psx_search_last_info": (_i, [_vp, C.POINTER(SearchInfo)]),
+    "psx_search_set_profile": (_i, [_vp, _i]),
+    "psx_search_get_profile": (_i, [_vp, C.POINTER(SearchProfile), _i]),
     "psx_search_debug_tap": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
 }
 

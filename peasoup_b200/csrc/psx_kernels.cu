@@ -396,6 +396,12 @@ struct InterbinSrc {
 
 int reduction_blocks() { return sm_count() * 2; }
 
+int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_t s)
+{
+    k_sum_partials<PlainSrc><<<reduction_blocks(), 256, 0, s>>>(PlainSrc{d_x}, 0, n, d_partials);
+    return launch_status("partial sums kernel");
+}
+
 int launch_stats(const float* d_x, bool interbinned, size_t first, size_t n, double2* d_partials,
                  double* d_sums, float* d_stat, float scale, cudaStream_t s)
 {
@@ -436,6 +442,13 @@ __global__ void k_convert(const T* __restrict__ in, float* __restrict__ out, siz
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
         out[i] = static_cast<float>(in[i]);
+}
+
+int launch_sub_scalar(float* d_x, size_t n, const float* d_v, cudaStream_t s)
+{
+    if (n == 0) return PSX_OK;
+    k_sub_scalar<<<grid_for(n, 256), 256, 0, s>>>(d_x, n, d_v);
+    return launch_status("subtract kernel");
 }
 
 int launch_fill(float* d_x, size_t n, float value, cudaStream_t s)

@@ -1,44 +1,41 @@
 // psx_search.cu -- the per-DM acceleration search engine behind
-// psx_search_dm: the body of the reference's DM loop
+// psx_search_dm / psx_search_block: the body of the reference's DM loop
 // (src/pipeline_multi.cu:161-294) re-organised for a B200.
 //
-// Per DM (prologue, once):
-//   H2D copy -> baseline removal -> zero padding -> R2C -> amplitude ->
-//   5/25/125-bin running median fused with the division of the spectrum
-//   -> birdie zapping -> interbin statistics (device-resident mean*N,
-//   std*N) -> C2R into the resident dereddened series.
+// Per DM (prologue, once, no host round trip):
+//   copy in -> baseline removal (device-side do/while, up to four passes
+//   before the host takes over) -> zero padding -> R2C -> amplitude ->
+//   5/25/125-bin running median fused with the division of the spectrum ->
+//   birdie zapping -> interbin statistics (device-resident mean*N, std*N)
+//   -> C2R into the resident dereddened series.
 // Per acceleration trial (the hot loop), in launch groups of `batch`:
-//   [resample gather -> R2C] (one batched cuFFT; with the LTO load callback
-//   the resample happens inside the transform) -> k_form_norm (interbin +
-//   normalise, one pass over the complex spectra) -> k_harm_peaks
-//   (fractional harmonic sums + threshold + warp-aggregated compaction of
-//   every (trial, fold, bin, S/N) above threshold).  Nothing per trial is
-//   copied to the host; the compacted records of the whole DM come back
-//   in one copy, and the host clusters (peakfinder.hpp:72-101), forms
-//   frequencies and distils them (distiller.hpp).
+//   resample gather -> R2C (one batched cuFFT, or with the resample inside
+//   cuFFT through a load callback where cuFFT supports it) -> k_form_norm
+//   (interbin + normalise in one pass) -> k_harm_tiles (fractional harmonic
+//   sums + threshold + warp-aggregated compaction of every (trial, fold,
+//   bin, S/N) above threshold).  The trial schedule of a DM can be captured
+//   as one CUDA graph.  Nothing per trial goes to the host: the records of
+//   a DM come back in one copy, and the host clusters them
+//   (peakfinder.hpp:72-101), forms frequencies and distils them
+//   (distiller.hpp) while the GPU already runs the next DM (two record
+//   slots, psx_search_block).
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
 #include <new>
+#include <thread>
 #include <vector>
 #include "psx_common.cuh"
 #include "psx_device.cuh"
 #include "psx_fft.cuh"
+#include "psx_harm.cuh"
 #include "psx_host.h"
 #include "psx_stages.cuh"
 
 namespace psx {
-
-// Search range of each spectrum (fold 0 = the normalised interbinned
-// spectrum, fold h = harmonic sum h) and the union [lo, hi).
-struct PeakParams {
-    int start[6];
-    int end[6];
-    unsigned lo, hi;
-    float thresh;
-};
 
 // ------------------------------------------------------------ kernels
 // Interbinned amplitude normalised with the DM's statistics
@@ -73,102 +70,140 @@ __global__ void __launch_bounds__(256) k_form_norm(const float* __restrict__ X, 
     }
 }
 
-// Warp-aggregated append of the lanes whose `hit` is set: one atomic per
-// warp and fold, records {trial, fold, bin, S/N bits}.
-__device__ __forceinline__ void emit(bool hit, int trial, int fold, unsigned bin, float val,
-                                     int4* __restrict__ rec, unsigned* __restrict__ counter,
-                                     unsigned cap, unsigned lane)
+// One pass of the device-side baseline loop (reference src/kernels.cu:
+// 463-479): while state[0] (active) is set, the float mean of the block
+// partials (float sum / float count, as the reference forms it) is
+// written for subtraction and state[0] becomes |mean| > 5e-7 n; once
+// inactive the pass subtracts zero.  state[1] counts the passes.
+__global__ void k_baseline_step(const double2* __restrict__ partials, int nparts, double count,
+                                float* __restrict__ mean_out, unsigned* __restrict__ state)
 {
-    const unsigned m = __ballot_sync(0xffffffffu, hit);
-    if (m == 0u) return;
-    const int leader = __ffs(m) - 1;
-    unsigned base = 0;
-    if ((int)lane == leader) base = atomicAdd(counter, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (hit) {
-        const unsigned pos = base + __popc(m & ((1u << lane) - 1u));
-        if (pos < cap) rec[pos] = make_int4(trial, fold, (int)bin, __float_as_int(val));
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a = 0.0;
+    for (int i = 0; i < nparts; ++i) a += partials[i].x;
+    const float mean = __fdiv_rn((float)a, (float)count);
+    if (state[0]) {
+        *mean_out = mean;
+        state[1] += 1;
+        state[0] = (fabsf(mean) > 5e-7 * count) ? 1u : 0u;
+    } else {
+        *mean_out = 0.0f;
     }
 }
 
-__device__ __forceinline__ bool in_range(const PeakParams& pp, int h, unsigned i)
+__global__ void k_baseline_reset(unsigned* __restrict__ state)
 {
-    return (int)i >= pp.start[h] && (int)i < pp.end[h];
+    state[0] = 1u;
+    state[1] = 0u;
 }
 
-// Fractional harmonic sums of each row with the reference's summation
-// order and scales (src/kernels.cu:41-96), threshold test on the
-// normalised spectrum and on every fold inside its search range, and
-// compaction of the hits.  One warp covers 32 consecutive bins, so the
-// gathers of fraction m/2^h touch about 32m/2^h + 1 consecutive floats.
+// Fused harmonic sums + threshold + compaction: tile shape and launcher.
+constexpr int kHarmTile = 1024;
+constexpr int kHarmThreads = 256;
+
 template <int F>
-__global__ void __launch_bounds__(256) k_harm_peaks(const float* __restrict__ p, size_t ppitch,
-                                                    PeakParams pp, int trial0,
-                                                    int4* __restrict__ rec,
-                                                    unsigned* __restrict__ counter, unsigned cap)
+static int launch_harm_f(const float* p, size_t ppitch, unsigned row_len, const PeakParams& pp,
+                         int trial0, int rows, int4* rec, unsigned* counter, unsigned cap,
+                         cudaStream_t s)
 {
-    const int t = blockIdx.y;
-    const int trial = trial0 + t;
-    const float* __restrict__ row = p + (size_t)t * ppitch;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned warp_first = blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
-    const unsigned stride = gridDim.x * blockDim.x;
-    const float thr = pp.thresh;
-    for (unsigned base = pp.lo + warp_first; base < pp.hi; base += stride) {
-        const unsigned i = base + lane;
-        const bool valid = i < pp.hi;
-        const unsigned ii = valid ? i : pp.hi - 1;
-        float val = row[ii];
-        emit(valid && in_range(pp, 0, i) && val > thr, trial, 0, i, val, rec, counter, cap, lane);
-        if (F > 0) {
-            val += row[frac_index<1>(ii, 1)];
-            const float s = val * rsqrt(2.0);
-            emit(valid && in_range(pp, 1, i) && s > thr, trial, 1, i, s, rec, counter, cap, lane);
-        }
-        if (F > 1) {
-            val += row[frac_index<2>(ii, 3)];
-            val += row[frac_index<2>(ii, 1)];
-            const float s = val * 0.5;
-            emit(valid && in_range(pp, 2, i) && s > thr, trial, 2, i, s, rec, counter, cap, lane);
-        }
-        if (F > 2) {
-#pragma unroll
-            for (unsigned m = 1; m < 8; m += 2) val += row[frac_index<3>(ii, m)];
-            const float s = val * rsqrt(8.0);
-            emit(valid && in_range(pp, 3, i) && s > thr, trial, 3, i, s, rec, counter, cap, lane);
-        }
-        if (F > 3) {
-#pragma unroll
-            for (unsigned m = 1; m < 16; m += 2) val += row[frac_index<4>(ii, m)];
-            const float s = val * 0.25;
-            emit(valid && in_range(pp, 4, i) && s > thr, trial, 4, i, s, rec, counter, cap, lane);
-        }
-        if (F > 4) {
-#pragma unroll
-            for (unsigned m = 1; m < 32; m += 2) val += row[frac_index<5>(ii, m)];
-            const float s = val * rsqrt(32.0);
-            emit(valid && in_range(pp, 5, i) && s > thr, trial, 5, i, s, rec, counter, cap, lane);
-        }
-    }
+    constexpr size_t smem = sizeof(float) * harm_smem_floats(F, kHarmTile);
+    const unsigned ntiles = (pp.hi - pp.lo + kHarmTile - 1) / kHarmTile;
+    dim3 grid(ntiles, (unsigned)rows);
+    k_harm_tiles<F, kHarmTile, kHarmThreads><<<grid, kHarmThreads, smem, s>>>(
+        p, ppitch, row_len, pp, trial0, rec, counter, cap);
+    return launch_status("harmonic-sum kernel");
 }
 
-typedef void (*HarmKernel)(const float*, size_t, PeakParams, int, int4*, unsigned*, unsigned);
+template <int F>
+static int configure_harm_f()
+{
+    constexpr size_t smem = sizeof(float) * harm_smem_floats(F, kHarmTile);
+    return cuda_status(cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmThreads>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                       "harmonic-sum kernel attribute");
+}
 
-static HarmKernel harm_kernel(int F)
+// Opts the kernel for F folds into its dynamic shared memory (once per
+// device, before any launch or capture).
+static int configure_harm(int F)
 {
     switch (F) {
-    case 0: return k_harm_peaks<0>;
-    case 1: return k_harm_peaks<1>;
-    case 2: return k_harm_peaks<2>;
-    case 3: return k_harm_peaks<3>;
-    case 4: return k_harm_peaks<4>;
-    default: return k_harm_peaks<5>;
+    case 0: return configure_harm_f<0>();
+    case 1: return configure_harm_f<1>();
+    case 2: return configure_harm_f<2>();
+    case 3: return configure_harm_f<3>();
+    case 4: return configure_harm_f<4>();
+    default: return configure_harm_f<5>();
     }
 }
+
+static int launch_harm(int F, const float* p, size_t ppitch, unsigned row_len,
+                       const PeakParams& pp, int trial0, int rows, int4* rec, unsigned* counter,
+                       unsigned cap, cudaStream_t s)
+{
+    switch (F) {
+    case 0: return launch_harm_f<0>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 1: return launch_harm_f<1>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 2: return launch_harm_f<2>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 3: return launch_harm_f<3>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 4: return launch_harm_f<4>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    default: return launch_harm_f<5>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    }
+}
+
+constexpr int kDeviceBaselinePasses = 4;
 
 }  // namespace psx
 
 using namespace psx;
+
+namespace {
+
+size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+int default_batch(size_t n)
+{
+    size_t b = ((size_t)1 << 25) / n;
+    if (b < 1) b = 1;
+    if (b > 32) b = 32;
+    size_t p = 1;
+    while (p * 2 <= b) p *= 2;
+    return (int)p;
+}
+
+// Per-DM state that must not be shared by two DMs in flight.
+struct Slot {
+    int4* d_rec = nullptr;
+    unsigned* d_count = nullptr;  // [0] hits, [1] baseline active, [2] passes
+    size_t rec_cap = 0;
+    int4* h_rec = nullptr;
+    unsigned* h_count = nullptr;
+    double* d_ktab = nullptr;
+    double* h_ktab = nullptr;
+    size_t ktab_cap = 0;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t copied = nullptr;
+    std::vector<cudaEvent_t> ev;  // profiling: 2 + 4 per launch group
+    // job
+    std::vector<float> accs;
+    const float* series = nullptr;
+    size_t nsamps = 0;
+    bool on_device = false;
+    bool host_baseline = false;
+    float dm = 0.f;
+    int dm_idx = 0;
+    int groups = 0;
+    int launches = 0;
+    int ffts = 0;
+    bool profiled = false;
+};
+
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0, ffts = 0, groups = 0;
+};
+
+}  // namespace
 
 struct psx_search {
     psx_search_config cfg{};
@@ -177,7 +212,8 @@ struct psx_search {
     int F = 0;
     int batch = 1;
     int device = 0;
-    cudaStream_t st = nullptr;
+    cudaStream_t st = nullptr;   // compute
+    cudaStream_t cst = nullptr;  // record copies
     bool own_stream = false;
     double bin_width = 0.0;
     float bin_width_f = 0.f;
@@ -196,57 +232,62 @@ struct psx_search {
     float* d_mean = nullptr;
     float* d_bf = nullptr;
     float* d_bw = nullptr;
-    double* d_ktab = nullptr;
     double* d_kbatch = nullptr;
-    size_t ktab_cap = 0;
-    double* h_ktab = nullptr;
-    int4* d_rec = nullptr;
-    unsigned* d_count = nullptr;
-    size_t rec_cap = 0;
-    int4* h_rec = nullptr;
-    unsigned* h_count = nullptr;
+    float* h_mean = nullptr;
 
+    Slot slot[2];
     FftPlan r2c1, c2r1;
     std::map<int, FftPlan*> r2cb;
-    std::map<int, cudaGraphExec_t> graphs;
-    struct GraphCounts {
-        int launches, ffts, groups;
-    };
-    std::map<int, GraphCounts> graph_counts;
+    std::map<long long, GraphEntry> graphs;
 
-    std::vector<float> accs;
+    int last_slot = 0;
+    bool profile = false;
+    psx_search_profile prof{};
     psx_search_info info{};
-    int launches = 0;
-    int ffts = 0;
+    int nthreads = 1;
 
     ~psx_search() { release(); }
 
+    void drop_graphs()
+    {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second.exec);
+        graphs.clear();
+    }
+
     void release()
     {
-        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
-        graphs.clear();
+        if (st) cudaStreamSynchronize(st);
+        if (cst) cudaStreamSynchronize(cst);
+        drop_graphs();
         for (auto& p : r2cb) delete p.second;
         r2cb.clear();
         r2c1.destroy();
         c2r1.destroy();
-        void* dev[] = {d_tim, d_tr, d_X, d_p, d_med, d_part, d_sums, d_stat, d_mean,
-                       d_bf, d_bw, d_ktab, d_kbatch, d_rec, d_count};
+        void* dev[] = {d_tim, d_tr, d_X, d_p, d_med, d_part, d_sums, d_stat, d_mean, d_bf, d_bw,
+                       d_kbatch};
         for (void* q : dev)
             if (q) cudaFree(q);
-        d_tim = d_tr = d_X = d_p = nullptr;
+        d_tim = d_tr = d_X = d_p = d_stat = d_mean = d_bf = d_bw = nullptr;
         d_med = nullptr;
         d_part = nullptr;
         d_sums = nullptr;
-        d_stat = d_mean = d_bf = d_bw = nullptr;
-        d_ktab = d_kbatch = nullptr;
-        d_rec = nullptr;
-        d_count = nullptr;
-        if (h_ktab) cudaFreeHost(h_ktab);
-        if (h_rec) cudaFreeHost(h_rec);
-        if (h_count) cudaFreeHost(h_count);
-        h_ktab = nullptr;
-        h_rec = nullptr;
-        h_count = nullptr;
+        d_kbatch = nullptr;
+        if (h_mean) cudaFreeHost(h_mean);
+        h_mean = nullptr;
+        for (Slot& s : slot) {
+            if (s.d_rec) cudaFree(s.d_rec);
+            if (s.d_count) cudaFree(s.d_count);
+            if (s.d_ktab) cudaFree(s.d_ktab);
+            if (s.h_rec) cudaFreeHost(s.h_rec);
+            if (s.h_count) cudaFreeHost(s.h_count);
+            if (s.h_ktab) cudaFreeHost(s.h_ktab);
+            if (s.done) cudaEventDestroy(s.done);
+            if (s.copied) cudaEventDestroy(s.copied);
+            for (cudaEvent_t e : s.ev) cudaEventDestroy(e);
+            s = Slot();
+        }
+        if (cst) cudaStreamDestroy(cst);
+        cst = nullptr;
         if (own_stream && st) cudaStreamDestroy(st);
         st = nullptr;
         own_stream = false;
@@ -256,26 +297,20 @@ struct psx_search {
     bool callback() const { return batched() && cfg.use_fft_callback; }
 
     int get_plan(int b, FftPlan** out);
-    int grow_records(size_t need);
-    int grow_ktab(size_t need);
-    int prologue(const float* series, size_t nsamps, bool on_device);
-    int trials_enqueue(int nacc);
-    int run_trials(int nacc);
-    int collect(float dm, int dm_idx, int output, std::vector<psx_candidate>& out,
-                std::vector<int>& nassoc, std::vector<int>& trial_of);
+    int grow_records(Slot& s, size_t need);
+    int grow_ktab(Slot& s, size_t need);
+    int ensure_events(Slot& s, int groups);
+    int prologue(Slot& s);
+    int trials_enqueue(Slot& s, int nacc);
+    int run_trials(Slot& s, int nacc);
+    int enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
+                int dm_idx);
+    int finish(Slot& s, int output, std::vector<psx_candidate>& out, std::vector<int>& nassoc,
+               std::vector<int>& trial_of);
+    void collect(Slot& s, size_t nrec, int output, std::vector<psx_candidate>& out,
+                 std::vector<int>& nassoc, std::vector<int>& trial_of);
+    void read_profile(Slot& s);
 };
-
-static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
-
-static int default_batch(size_t n)
-{
-    size_t b = ((size_t)1 << 26) / n;
-    if (b < 1) b = 1;
-    if (b > 64) b = 64;
-    size_t p = 1;
-    while (p * 2 <= b) p *= 2;
-    return (int)p;
-}
 
 int psx_search::get_plan(int b, FftPlan** out)
 {
@@ -297,150 +332,188 @@ int psx_search::get_plan(int b, FftPlan** out)
     return PSX_OK;
 }
 
-int psx_search::grow_records(size_t need)
+int psx_search::grow_records(Slot& s, size_t need)
 {
-    if (need <= rec_cap) return PSX_OK;
-    size_t cap = round_up(need + need / 4, 4096);
-    if (d_rec) cudaFree(d_rec);
-    if (h_rec) cudaFreeHost(h_rec);
-    d_rec = nullptr;
-    h_rec = nullptr;
-    rec_cap = 0;
-    PSX_CUDA(cudaMalloc(&d_rec, sizeof(int4) * cap));
-    PSX_CUDA(cudaMallocHost(&h_rec, sizeof(int4) * cap));
-    rec_cap = cap;
-    // captured schedules hold the old buffer
-    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
-    graphs.clear();
-    return PSX_OK;
-}
-
-int psx_search::grow_ktab(size_t need)
-{
-    if (need <= ktab_cap) return PSX_OK;
-    size_t cap = round_up(need + need / 2, 256);
+    if (need <= s.rec_cap) return PSX_OK;
+    const size_t cap = round_up(need + need / 4, 4096);
     PSX_CUDA(cudaStreamSynchronize(st));
-    if (d_ktab) cudaFree(d_ktab);
-    if (h_ktab) cudaFreeHost(h_ktab);
-    d_ktab = nullptr;
-    h_ktab = nullptr;
-    ktab_cap = 0;
-    PSX_CUDA(cudaMalloc(&d_ktab, sizeof(double) * cap));
-    PSX_CUDA(cudaMallocHost(&h_ktab, sizeof(double) * cap));
-    ktab_cap = cap;
-    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
-    graphs.clear();
+    PSX_CUDA(cudaStreamSynchronize(cst));
+    if (s.d_rec) cudaFree(s.d_rec);
+    if (s.h_rec) cudaFreeHost(s.h_rec);
+    s.d_rec = nullptr;
+    s.h_rec = nullptr;
+    s.rec_cap = 0;
+    PSX_CUDA(cudaMalloc(&s.d_rec, sizeof(int4) * cap));
+    PSX_CUDA(cudaMallocHost(&s.h_rec, sizeof(int4) * cap));
+    s.rec_cap = cap;
+    drop_graphs();  // captured schedules hold the old buffer
     return PSX_OK;
 }
 
-// src/pipeline_multi.cu:170-238 for one series.
-int psx_search::prologue(const float* series, size_t nsamps, bool on_device)
+int psx_search::grow_ktab(Slot& s, size_t need)
 {
-    const size_t ncopy = std::min(nsamps, N);
-    PSX_CUDA(cudaMemcpyAsync(d_tim, series, sizeof(float) * ncopy,
-                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    if (need <= s.ktab_cap) return PSX_OK;
+    const size_t cap = round_up(need + need / 2, 256);
+    PSX_CUDA(cudaStreamSynchronize(st));
+    if (s.d_ktab) cudaFree(s.d_ktab);
+    if (s.h_ktab) cudaFreeHost(s.h_ktab);
+    s.d_ktab = nullptr;
+    s.h_ktab = nullptr;
+    s.ktab_cap = 0;
+    PSX_CUDA(cudaMalloc(&s.d_ktab, sizeof(double) * cap));
+    PSX_CUDA(cudaMallocHost(&s.h_ktab, sizeof(double) * cap));
+    s.ktab_cap = cap;
+    drop_graphs();
+    return PSX_OK;
+}
+
+int psx_search::ensure_events(Slot& s, int groups)
+{
+    const size_t need = 2 + 4 * (size_t)groups;
+    while (s.ev.size() < need) {
+        cudaEvent_t e;
+        PSX_CUDA(cudaEventCreate(&e));
+        s.ev.push_back(e);
+    }
+    return PSX_OK;
+}
+
+// src/pipeline_multi.cu:170-238 for one series, all on the compute stream.
+int psx_search::prologue(Slot& s)
+{
+    const size_t ncopy = std::min(s.nsamps, N);
+    PSX_CUDA(cudaMemcpyAsync(d_tim, s.series, sizeof(float) * ncopy,
+                             s.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
     // baseline removal over the copied samples (timeseries.hpp:282-287,
     // src/kernels.cu:463-479)
-    int count = 0;
-    float mean = 0.f;
-    do {
-        PSX_TRY(remove_baseline_pass(d_tim, ncopy, d_part, d_sums, d_mean, st));
-        launches += 4;
-        PSX_CUDA(cudaMemcpyAsync(h_count + 2, d_mean, sizeof(float), cudaMemcpyDeviceToHost, st));
-        PSX_CUDA(cudaStreamSynchronize(st));
-        std::memcpy(&mean, h_count + 2, sizeof(float));
-        if (count++ > 100) break;
-    } while (std::fabs(mean) > 5e-7 * (double)ncopy);
+    const int nb = reduction_blocks();
+    if (!s.host_baseline) {
+        k_baseline_reset<<<1, 1, 0, st>>>(s.d_count + 1);
+        ++s.launches;
+        for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
+            PSX_TRY(launch_partials(d_tim, ncopy, d_part, st));
+            k_baseline_step<<<1, 32, 0, st>>>(d_part, nb, (double)ncopy, d_mean, s.d_count + 1);
+            PSX_TRY(launch_sub_scalar(d_tim, ncopy, d_mean, st));
+            s.launches += 3;
+        }
+    } else {
+        int count = 0;
+        float mean = 0.f;
+        do {
+            PSX_TRY(remove_baseline_pass(d_tim, ncopy, d_part, d_sums, d_mean, st));
+            s.launches += 4;
+            PSX_CUDA(cudaMemcpyAsync(h_mean, d_mean, sizeof(float), cudaMemcpyDeviceToHost, st));
+            PSX_CUDA(cudaStreamSynchronize(st));
+            mean = *h_mean;
+            if (count++ > 100) break;
+        } while (std::fabs(mean) > 5e-7 * (double)ncopy);
+    }
     // zero padding (pipeline_multi.cu:179-187)
     if (ncopy < N) {
         PSX_TRY(launch_fill(d_tim + ncopy, N - ncopy, 0.f, st));
-        ++launches;
+        ++s.launches;
     }
     PSX_TRY(r2c1.exec(d_tim, d_X, st));
-    ++ffts;
+    ++s.ffts;
     // amplitude spectrum into the first row of d_p (spectrumformer.hpp:16-22)
     PSX_TRY(psx_form_power_series(d_X, d_p, B, 0, reinterpret_cast<psx_stream_t>(st)));
-    ++launches;
+    ++s.launches;
     // running median and division (dereddener.hpp:41-66)
     PSX_TRY(launch_running_median(d_p, B, bin_width, cfg.boundary_5_freq, cfg.boundary_25_freq,
                                   nullptr, d_X, d_med, st));
-    launches += 4;
+    s.launches += 4;
     if (!bf.empty()) {
         PSX_TRY(launch_zap(d_X, d_bf, d_bw, bin_width_f, bf.size(), B, st));
-        ++launches;
+        ++s.launches;
     }
     // interbin statistics (pipeline_multi.cu:230-234) -> mean*N, std*N
     PSX_TRY(launch_stats(d_X, true, 0, B, d_part, d_sums, d_stat, (float)N, st));
-    launches += 2;
+    s.launches += 2;
     PSX_TRY(c2r1.exec(d_X, d_tim, st));
-    ++ffts;
+    ++s.ffts;
     return PSX_OK;
 }
 
 // Enqueues every acceleration trial of the DM (k factors already in
-// d_ktab) plus the reset of the record counter.
-int psx_search::trials_enqueue(int nacc)
+// s.d_ktab) plus the reset of the record counter.
+int psx_search::trials_enqueue(Slot& s, int nacc)
 {
-    PSX_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned) * 2, st));
+    PSX_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned), st));
     const unsigned T = 256;
-    HarmKernel hk = harm_kernel(F);
     const unsigned span = pk.hi > pk.lo ? pk.hi - pk.lo : 0;
-    int t0 = 0, groups = 0;
+    int t0 = 0, g = 0;
     while (t0 < nacc) {
         int b = 1;
-        const float* xin = d_tr;
         if (batched()) {
             b = batch;
             while (b > nacc - t0) b >>= 1;
             FftPlan* plan = nullptr;
             PSX_TRY(get_plan(b, &plan));
             if (callback()) {
-                PSX_CUDA(cudaMemcpyAsync(d_kbatch, d_ktab + t0, sizeof(double) * b,
+                PSX_CUDA(cudaMemcpyAsync(d_kbatch, s.d_ktab + t0, sizeof(double) * b,
                                          cudaMemcpyDeviceToDevice, st));
             } else {
-                PSX_TRY(launch_resample(d_tim, d_tr, N, d_ktab + t0, 0.0, b, N, false, st));
-                ++launches;
+                PSX_TRY(launch_resample(d_tim, d_tr, N, s.d_ktab + t0, 0.0, b, N, false, st));
+                ++s.launches;
             }
-            PSX_TRY(plan->exec(xin, d_X, st));
-            ++ffts;
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g], st));
+            PSX_TRY(plan->exec(d_tr, d_X, st));
+            ++s.ffts;
         } else {
-            PSX_TRY(launch_resample(d_tim, d_tr, N, d_ktab + t0, 0.0, 1, N, false, st));
-            ++launches;
+            PSX_TRY(launch_resample(d_tim, d_tr, N, s.d_ktab + t0, 0.0, 1, N, false, st));
+            ++s.launches;
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g], st));
             PSX_TRY(r2c1.exec(d_tr, d_X, st));
-            ++ffts;
+            ++s.ffts;
         }
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 1], st));
         dim3 gf(grid_for(B / 2 + 1, T, 4), (unsigned)b);
         k_form_norm<<<gf, T, 0, st>>>(d_X, 2 * Bp, d_p, Bp, (unsigned)B, d_stat);
-        ++launches;
+        ++s.launches;
+        PSX_TRY(launch_status("form kernel"));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 2], st));
         if (span) {
-            dim3 gh(grid_for(span, T, 8), (unsigned)b);
-            hk<<<gh, T, 0, st>>>(d_p, Bp, pk, t0, d_rec, d_count, (unsigned)rec_cap);
-            ++launches;
+            PSX_TRY(launch_harm(F, d_p, Bp, (unsigned)Bp, pk, t0, b, s.d_rec, s.d_count,
+                                (unsigned)s.rec_cap, st));
+            ++s.launches;
         }
-        PSX_TRY(launch_status("search trial kernels"));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 3], st));
         t0 += b;
-        ++groups;
+        ++g;
     }
-    info.nbatches = groups;
+    s.groups = g;
     return PSX_OK;
 }
 
-int psx_search::run_trials(int nacc)
+static int count_groups(int nacc, bool batched, int batch)
+{
+    if (!batched) return nacc;
+    int t0 = 0, g = 0;
+    while (t0 < nacc) {
+        int b = batch;
+        while (b > nacc - t0) b >>= 1;
+        t0 += b;
+        ++g;
+    }
+    return g;
+}
+
+int psx_search::run_trials(Slot& s, int nacc)
 {
     const bool graph = batched() && cfg.use_graph;
-    info.graph = 0;
-    if (!graph) return trials_enqueue(nacc);
-    auto it = graphs.find(nacc);
+    if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
+    if (!graph) return trials_enqueue(s, nacc);
+    const long long key = ((long long)nacc << 2) | ((&s == &slot[1]) ? 2 : 0) | (s.profiled ? 1 : 0);
+    auto it = graphs.find(key);
     if (it == graphs.end()) {
-        // plans must exist before capture (creation allocates and syncs)
+        // plans must exist before capture (creation allocates)
         for (int b = batch; b >= 1; b >>= 1) {
             FftPlan* p = nullptr;
             PSX_TRY(get_plan(b, &p));
         }
-        PSX_CUDA(cudaStreamSynchronize(st));
-        const int l0 = launches, f0 = ffts;
+        const int l0 = s.launches, f0 = s.ffts;
         PSX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        int rc = trials_enqueue(nacc);
+        int rc = trials_enqueue(s, nacc);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (rc != PSX_OK) {
@@ -448,102 +521,216 @@ int psx_search::run_trials(int nacc)
             return rc;
         }
         PSX_CUDA(e);
-        cudaGraphExec_t ge = nullptr;
-        e = cudaGraphInstantiate(&ge, g, 0);
+        GraphEntry ge;
+        e = cudaGraphInstantiate(&ge.exec, g, 0);
         cudaGraphDestroy(g);
         PSX_CUDA(e);
-        it = graphs.emplace(nacc, ge).first;
-        // the captured work is counted at every replay below
-        graph_counts[nacc] = GraphCounts{launches - l0, ffts - f0, info.nbatches};
-        launches = l0;
-        ffts = f0;
+        ge.launches = s.launches - l0;
+        ge.ffts = s.ffts - f0;
+        ge.groups = s.groups;
+        s.launches = l0;
+        s.ffts = f0;
+        it = graphs.emplace(key, ge).first;
     }
-    PSX_CUDA(cudaGraphLaunch(it->second, st));
-    const GraphCounts& gc = graph_counts[nacc];
-    launches += gc.launches;
-    ffts += gc.ffts;
-    info.nbatches = gc.groups;
-    info.graph = 1;
+    PSX_CUDA(cudaGraphLaunch(it->second.exec, st));
+    s.launches += it->second.launches;
+    s.ffts += it->second.ffts;
+    s.groups = it->second.groups;
     return PSX_OK;
 }
 
-// Host side of one DM: record copy-back, clustering per (trial, fold),
-// candidate frequencies, per-trial harmonic distillation and optionally
-// the per-DM acceleration distillation (pipeline_multi.cu:283-294).
-int psx_search::collect(float dm, int dm_idx, int output, std::vector<psx_candidate>& out,
-                        std::vector<int>& nassoc, std::vector<int>& trial_of)
+int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
+                        int dm_idx)
 {
-    const size_t nrec = h_count[0];
-    if (nrec) {
-        PSX_CUDA(cudaMemcpyAsync(h_rec, d_rec, sizeof(int4) * nrec, cudaMemcpyDeviceToHost, st));
-        PSX_CUDA(cudaStreamSynchronize(st));
+    const psx_search_config& c = cfg;
+    s.series = series;
+    s.nsamps = nsamps;
+    s.on_device = on_device;
+    s.dm = dm;
+    s.dm_idx = dm_idx;
+    s.launches = 0;
+    s.ffts = 0;
+    s.groups = 0;
+    s.profiled = profile;
+    s.accs = accel_list(c.acc_lo, c.acc_hi, c.acc_tol, c.acc_pulse_width, N, c.tsamp, c.cfreq_hz,
+                        c.ch_bw_hz, dm, c.cdm);
+    const int nacc = (int)s.accs.size();
+    PSX_TRY(grow_ktab(s, (size_t)nacc));
+    for (int t = 0; t < nacc; ++t) s.h_ktab[t] = accel_fact(s.accs[t], c.tsamp);
+    if (s.profiled) {
+        PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
+        PSX_CUDA(cudaEventRecord(s.ev[0], st));
     }
-    // order by (trial, fold, bin): the bins of one spectrum ascending, as
-    // the reference's order-preserving copy_if leaves them
-    std::sort(h_rec, h_rec + nrec, [](const int4& a, const int4& b) {
-        if (a.x != b.x) return a.x < b.x;
-        if (a.y != b.y) return a.y < b.y;
-        return a.z < b.z;
-    });
+    PSX_TRY(prologue(s));
+    if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[1], st));
+    PSX_CUDA(cudaMemcpyAsync(s.d_ktab, s.h_ktab, sizeof(double) * nacc, cudaMemcpyHostToDevice, st));
+    PSX_TRY(run_trials(s, nacc));
+    PSX_CUDA(cudaMemcpyAsync(s.h_count, s.d_count, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, st));
+    PSX_CUDA(cudaEventRecord(s.done, st));
+    return PSX_OK;
+}
+
+void psx_search::read_profile(Slot& s)
+{
+    if (!s.profiled) return;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s.ev[0], s.ev[1]) == cudaSuccess) prof.prologue_ms += ms;
+    for (int g = 0; g < s.groups; ++g) {
+        cudaEvent_t prev = g == 0 ? s.ev[1] : s.ev[2 + 4 * (g - 1) + 3];
+        cudaEvent_t* e = &s.ev[2 + 4 * g];
+        if (cudaEventElapsedTime(&ms, prev, e[0]) == cudaSuccess) prof.resample_ms += ms;
+        if (cudaEventElapsedTime(&ms, e[0], e[1]) == cudaSuccess) prof.fft_ms += ms;
+        if (cudaEventElapsedTime(&ms, e[1], e[2]) == cudaSuccess) prof.form_ms += ms;
+        if (cudaEventElapsedTime(&ms, e[2], e[3]) == cudaSuccess) prof.harm_ms += ms;
+    }
+    prof.groups += s.groups;
+    prof.trials += (long long)s.accs.size();
+    prof.dms += 1;
+    cudaGetLastError();
+}
+
+// Host side of one DM: bucket the records by (trial, fold), order each
+// bucket by bin (the order the reference's copy_if leaves them in),
+// cluster (peakfinder.hpp:72-101), form candidate frequencies, distil per
+// trial (pipeline_multi.cu:283-289) and optionally per DM (:294).
+void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candidate>& out,
+                         std::vector<int>& nassoc, std::vector<int>& trial_of)
+{
+    const int nacc = (int)s.accs.size();
+    const int nf = F + 1;
+    const size_t nkeys = (size_t)nacc * nf;
+    std::vector<unsigned> off(nkeys + 1, 0);
+    for (size_t r = 0; r < nrec; ++r) {
+        const int4 q = s.h_rec[r];
+        if (q.x >= 0 && q.x < nacc && q.y >= 0 && q.y < nf) ++off[(size_t)q.x * nf + q.y + 1];
+    }
+    for (size_t k = 0; k < nkeys; ++k) off[k + 1] += off[k];
+    std::vector<std::pair<int, float>> items(off[nkeys]);
+    {
+        std::vector<unsigned> pos(off.begin(), off.end() - 1);
+        for (size_t r = 0; r < nrec; ++r) {
+            const int4 q = s.h_rec[r];
+            if (q.x < 0 || q.x >= nacc || q.y < 0 || q.y >= nf) continue;
+            float v;
+            std::memcpy(&v, &q.w, sizeof v);
+            items[pos[(size_t)q.x * nf + q.y]++] = std::make_pair(q.z, v);
+        }
+    }
+    // per-trial work in parallel when there is enough of it
+    std::vector<std::vector<psx_candidate>> per(nacc);
+    auto work = [&](int t_begin, int t_end) {
+        std::vector<int> idx, pidx;
+        std::vector<float> snr, psnr;
+        std::vector<psx_candidate> tc;
+        for (int t = t_begin; t < t_end; ++t) {
+            tc.clear();
+            for (int h = 0; h < nf; ++h) {
+                const size_t k = (size_t)t * nf + h;
+                auto b = items.begin() + off[k], e = items.begin() + off[k + 1];
+                if (b == e) continue;
+                std::sort(b, e, [](const std::pair<int, float>& x, const std::pair<int, float>& y) {
+                    return x.first < y.first;
+                });
+                const size_t n = (size_t)(e - b);
+                idx.resize(n);
+                snr.resize(n);
+                for (size_t i = 0; i < n; ++i) {
+                    idx[i] = b[i].first;
+                    snr[i] = b[i].second;
+                }
+                pidx.resize(n);
+                psnr.resize(n);
+                const size_t np = unique_peaks(idx.data(), snr.data(), n, cfg.min_gap, pidx.data(),
+                                               psnr.data());
+                for (size_t i = 0; i < np; ++i)
+                    tc.push_back(psx_candidate{s.dm, s.dm_idx, s.accs[t], h, psnr[i],
+                                               (float)pidx[i] * factor[h]});
+            }
+            if (tc.empty()) continue;
+            const size_t keep = distill(PSX_DISTILL_HARMONIC, tc.data(), tc.size(), cfg.freq_tol,
+                                        cfg.max_harm, tobs, 0, 1, nullptr);
+            per[t].assign(tc.begin(), tc.begin() + keep);
+        }
+    };
+    const int nth = (nrec > 20000 && nthreads > 1) ? std::min(nthreads, nacc) : 1;
+    if (nth <= 1) {
+        work(0, nacc);
+    } else {
+        std::vector<std::thread> th;
+        std::atomic<int> next{0};
+        const int chunk = std::max(1, nacc / (nth * 4));
+        for (int i = 0; i < nth; ++i)
+            th.emplace_back([&] {
+                for (;;) {
+                    const int b = next.fetch_add(chunk);
+                    if (b >= nacc) break;
+                    work(b, std::min(nacc, b + chunk));
+                }
+            });
+        for (auto& x : th) x.join();
+    }
     out.clear();
     nassoc.clear();
     trial_of.clear();
-    std::vector<int> idx, pidx;
-    std::vector<float> snr, psnr;
-    std::vector<psx_candidate> tc;
-    size_t r = 0;
-    const int nacc = (int)accs.size();
-    for (int t = 0; t < nacc; ++t) {
-        tc.clear();
-        for (int h = 0; h <= F; ++h) {
-            idx.clear();
-            snr.clear();
-            while (r < nrec && h_rec[r].x == t && h_rec[r].y == h) {
-                idx.push_back(h_rec[r].z);
-                float v;
-                std::memcpy(&v, &h_rec[r].w, sizeof v);
-                snr.push_back(v);
-                ++r;
-            }
-            if (idx.empty()) continue;
-            pidx.resize(idx.size());
-            psnr.resize(idx.size());
-            const size_t np = unique_peaks(idx.data(), snr.data(), idx.size(), cfg.min_gap,
-                                           pidx.data(), psnr.data());
-            for (size_t k = 0; k < np; ++k)
-                tc.push_back(psx_candidate{dm, dm_idx, accs[t], h, psnr[k],
-                                           (float)pidx[k] * factor[h]});
-        }
-        // skip records of folds that were not consumed (cannot happen for
-        // folds 0..F, kept for robustness)
-        while (r < nrec && h_rec[r].x == t) ++r;
-        if (tc.empty()) continue;
-        const size_t keep = distill(PSX_DISTILL_HARMONIC, tc.data(), tc.size(), cfg.freq_tol,
-                                    cfg.max_harm, tobs, 0, 1, nullptr);
-        for (size_t k = 0; k < keep; ++k) {
-            out.push_back(tc[k]);
+    for (int t = 0; t < nacc; ++t)
+        for (const psx_candidate& c : per[t]) {
+            out.push_back(c);
             trial_of.push_back(t);
         }
-    }
     if (output == PSX_OUT_DM && !out.empty()) {
-        // The acceleration distiller reorders candidates; carry the trial
-        // index through it by tagging the S/N-sorted order afterwards.
         std::vector<psx_candidate> c = out;
         nassoc.assign(c.size(), 0);
         const size_t keep = distill(PSX_DISTILL_ACCEL, c.data(), c.size(), cfg.freq_tol,
                                     cfg.max_harm, tobs, 1, 1, nassoc.data());
         c.resize(keep);
         nassoc.resize(keep);
-        // trial index of each survivor: its acceleration's position in the list
         trial_of.assign(keep, -1);
         for (size_t k = 0; k < keep; ++k) {
-            auto it = std::lower_bound(accs.begin(), accs.end(), c[k].acc);
-            if (it != accs.end() && *it == c[k].acc) trial_of[k] = (int)(it - accs.begin());
+            auto it = std::lower_bound(s.accs.begin(), s.accs.end(), c[k].acc);
+            if (it != s.accs.end() && *it == c[k].acc) trial_of[k] = (int)(it - s.accs.begin());
         }
         out.swap(c);
     } else {
         nassoc.assign(out.size(), 0);
     }
+}
+
+int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
+                       std::vector<int>& nassoc, std::vector<int>& trial_of)
+{
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        PSX_CUDA(cudaEventSynchronize(s.done));
+        const size_t hits = s.h_count[0];
+        const bool baseline_pending = !s.host_baseline && s.h_count[1] != 0;
+        if (hits <= s.rec_cap && !baseline_pending) break;
+        // Rare: more hits than the record slot holds, or a baseline that
+        // needed more passes than the device loop makes.  Run the DM again
+        // (after everything queued so far) with a larger slot / the host
+        // loop; the result is as if it had run once.
+        if (hits > s.rec_cap) PSX_TRY(grow_records(s, hits));
+        if (baseline_pending) s.host_baseline = true;
+        if (attempt == 2) {
+            set_error("search: could not complete DM %d", s.dm_idx);
+            return PSX_ERR_OVERFLOW;
+        }
+        PSX_TRY(enqueue(s, s.series, s.nsamps, s.on_device, s.dm, s.dm_idx));
+    }
+    const size_t nrec = s.h_count[0];
+    info.baseline_passes = s.host_baseline ? -1 : (int)s.h_count[2];
+    s.host_baseline = false;
+    if (nrec) {
+        PSX_CUDA(cudaStreamWaitEvent(cst, s.done, 0));
+        PSX_CUDA(cudaMemcpyAsync(s.h_rec, s.d_rec, sizeof(int4) * nrec, cudaMemcpyDeviceToHost, cst));
+        PSX_CUDA(cudaEventRecord(s.copied, cst));
+        PSX_CUDA(cudaEventSynchronize(s.copied));
+    }
+    read_profile(s);
+    info.ntrials += (int)s.accs.size();
+    info.nbatches += s.groups;
+    info.kernel_launches += s.launches;
+    info.fft_launches += s.ffts;
+    info.above_threshold += (long long)nrec;
+    collect(s, nrec, output, out, nassoc, trial_of);
     return PSX_OK;
 }
 
@@ -573,7 +760,7 @@ void psx_search_config_defaults(psx_search_config* c, size_t fft_size, float tsa
     c->boundary_25_freq = 0.5f;
     c->mode = PSX_MODE_BATCHED;
     c->batch = 0;
-    c->use_fft_callback = 1;
+    c->use_fft_callback = 0;
     c->use_graph = 1;
 }
 
@@ -635,7 +822,7 @@ size_t psx_search_footprint(const psx_search_config* c)
     bytes += sizeof(float) * 2 * Bp * b;              // complex spectra
     bytes += sizeof(float) * Bp * b;                  // normalised spectra
     bytes += median_scratch_bytes(B);
-    bytes += sizeof(int4) * ((size_t)1 << 20);        // initial record buffer
+    bytes += 2 * sizeof(int4) * ((size_t)1 << 20);    // two initial record slots
     // cuFFT work areas: about one transform's worth per batched plan size
     bytes += sizeof(float) * 2 * Bp * (2 * b + 2);
     return bytes;
@@ -661,6 +848,8 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->Bp = round_up(s->B, 64);
     s->F = cfg->nharmonics;
     s->batch = effective_batch(cfg);
+    unsigned hc = std::thread::hardware_concurrency();
+    s->nthreads = (int)std::max(1u, std::min(8u, hc ? hc : 1u));
     // pipeline_multi.cu:126-128: tobs and bin width are floats
     s->tobs = (float)s->N * cfg->tsamp;
     s->bin_width_f = (float)(1.0 / (double)s->tobs);
@@ -685,7 +874,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
             hi = std::max(hi, (unsigned)en);
         }
     }
-    s->pk.lo = hi > lo ? lo : 0;
+    s->pk.lo = hi > lo ? (lo & ~127u) : 0;
     s->pk.hi = hi > lo ? hi : 0;
     s->pk.thresh = cfg->min_snr;
 
@@ -695,10 +884,14 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
         return code;
     };
     if ((rc = cuda_status(cudaGetDevice(&s->device), "cudaGetDevice")) != PSX_OK) return fail(rc);
+    if ((rc = configure_harm(s->F)) != PSX_OK) return fail(rc);
     if ((rc = cuda_status(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking),
                           "cudaStreamCreate")) != PSX_OK)
         return fail(rc);
     s->own_stream = true;
+    if ((rc = cuda_status(cudaStreamCreateWithFlags(&s->cst, cudaStreamNonBlocking),
+                          "cudaStreamCreate")) != PSX_OK)
+        return fail(rc);
     const size_t N = s->N, Bp = s->Bp;
     const size_t b = (size_t)s->batch;
     const bool cb = s->callback();
@@ -717,15 +910,22 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     ALLOC(s->d_stat, sizeof(float) * 8);
     ALLOC(s->d_mean, sizeof(float) * 2);
     ALLOC(s->d_kbatch, sizeof(double) * b);
-    ALLOC(s->d_count, sizeof(unsigned) * 2);
+    for (Slot& sl : s->slot) ALLOC(sl.d_count, sizeof(unsigned) * 4);
     if (!s->bf.empty()) {
         ALLOC(s->d_bf, sizeof(float) * s->bf.size());
         ALLOC(s->d_bw, sizeof(float) * s->bw.size());
     }
 #undef ALLOC
-    if ((rc = cuda_status(cudaMallocHost(&s->h_count, sizeof(unsigned) * 4), "cudaMallocHost")) !=
-        PSX_OK)
-        return fail(PSX_ERR_ALLOC);
+    if (cudaMallocHost(&s->h_mean, sizeof(float) * 4) != cudaSuccess) return fail(PSX_ERR_ALLOC);
+    for (Slot& sl : s->slot) {
+        if (cudaMallocHost(&sl.h_count, sizeof(unsigned) * 4) != cudaSuccess)
+            return fail(PSX_ERR_ALLOC);
+        if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming) != cudaSuccess)
+            return fail(PSX_ERR_CUDA);
+        if ((rc = s->grow_records(sl, (size_t)1 << 20)) != PSX_OK) return fail(rc);
+        if ((rc = s->grow_ktab(sl, 1024)) != PSX_OK) return fail(rc);
+    }
     if (!s->bf.empty()) {
         cudaMemcpy(s->d_bf, s->bf.data(), sizeof(float) * s->bf.size(), cudaMemcpyHostToDevice);
         cudaMemcpy(s->d_bw, s->bw.data(), sizeof(float) * s->bw.size(), cudaMemcpyHostToDevice);
@@ -734,8 +934,6 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     cudaMemsetAsync(s->d_X, 0, sizeof(float) * 2 * Bp * b, s->st);
     cudaMemsetAsync(s->d_p, 0, sizeof(float) * Bp * b, s->st);
     cudaMemsetAsync(s->d_kbatch, 0, sizeof(double) * b, s->st);
-    if ((rc = s->grow_records((size_t)1 << 20)) != PSX_OK) return fail(rc);
-    if ((rc = s->grow_ktab(1024)) != PSX_OK) return fail(rc);
     if ((rc = s->r2c1.create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
     if ((rc = s->c2r1.create(N, 1, PSX_FFT_C2R, 0, 0, false)) != PSX_OK) return fail(rc);
     if (s->batched()) {
@@ -754,7 +952,6 @@ int psx_search_destroy(psx_search* s)
 {
     clear_error();
     if (!s) return PSX_OK;
-    if (s->st) cudaStreamSynchronize(s->st);
     delete s;
     return PSX_OK;
 }
@@ -767,7 +964,80 @@ int psx_search_set_stream(psx_search* s, psx_stream_t stream)
     if (s->own_stream) cudaStreamDestroy(s->st);
     s->own_stream = false;
     s->st = cs(stream);
-    // graphs are stream independent; nothing else holds the stream
+    return PSX_OK;
+}
+
+int psx_search_set_profile(psx_search* s, int on)
+{
+    if (!s) return PSX_ERR_INVALID;
+    s->profile = on != 0;
+    return PSX_OK;
+}
+
+int psx_search_get_profile(psx_search* s, psx_search_profile* out, int reset)
+{
+    if (!s || !out) return PSX_ERR_INVALID;
+    *out = s->prof;
+    if (reset) s->prof = psx_search_profile{};
+    return PSX_OK;
+}
+
+int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
+                     int series_on_device, const float* dms, const int* dm_idx, int ndm,
+                     int output, psx_candidate* h_out, int* h_nassoc, int* h_trial, int* h_dm,
+                     size_t cap, size_t* n_out)
+{
+    clear_error();
+    if (!s || !series || !dms || !n_out || ndm <= 0 || nsamps == 0 ||
+        (output != PSX_OUT_TRIAL && output != PSX_OUT_DM)) {
+        set_error("search: bad arguments");
+        return PSX_ERR_INVALID;
+    }
+    for (int d = 0; d < ndm; ++d)
+        if (!series[d]) {
+            set_error("search: null series %d", d);
+            return PSX_ERR_INVALID;
+        }
+    *n_out = 0;
+    PSX_CUDA(cudaSetDevice(s->device));
+    const int bp = s->info.batch, cbk = s->info.fft_callback;
+    s->info = psx_search_info{};
+    s->info.batch = bp;
+    s->info.fft_callback = cbk;
+    s->info.graph = s->batched() && s->cfg.use_graph ? 1 : 0;
+    std::vector<psx_candidate> all, out;
+    std::vector<int> all_na, all_tr, all_dm, na, tr;
+    int rc = s->enqueue(s->slot[0], series[0], nsamps, series_on_device != 0, dms[0],
+                        dm_idx ? dm_idx[0] : 0);
+    for (int d = 0; d < ndm && rc == PSX_OK; ++d) {
+        if (d + 1 < ndm)
+            rc = s->enqueue(s->slot[(d + 1) & 1], series[d + 1], nsamps, series_on_device != 0,
+                            dms[d + 1], dm_idx ? dm_idx[d + 1] : d + 1);
+        if (rc != PSX_OK) break;
+        s->last_slot = d & 1;
+        rc = s->finish(s->slot[d & 1], output, out, na, tr);
+        if (rc != PSX_OK) break;
+        all.insert(all.end(), out.begin(), out.end());
+        all_na.insert(all_na.end(), na.begin(), na.end());
+        all_tr.insert(all_tr.end(), tr.begin(), tr.end());
+        all_dm.insert(all_dm.end(), out.size(), d);
+    }
+    if (rc != PSX_OK) {
+        cudaStreamSynchronize(s->st);
+        cudaStreamSynchronize(s->cst);
+        return rc;
+    }
+    *n_out = all.size();
+    if (all.size() > cap || (!h_out && !all.empty())) {
+        set_error("search: %zu candidates, buffer holds %zu", all.size(), cap);
+        return PSX_ERR_OVERFLOW;
+    }
+    if (!all.empty()) std::memcpy(h_out, all.data(), sizeof(psx_candidate) * all.size());
+    for (size_t k = 0; k < all.size(); ++k) {
+        if (h_nassoc) h_nassoc[k] = all_na[k];
+        if (h_trial) h_trial[k] = all_tr[k];
+        if (h_dm) h_dm[k] = all_dm[k];
+    }
     return PSX_OK;
 }
 
@@ -775,56 +1045,9 @@ int psx_search_dm(psx_search* s, const float* series, size_t nsamps, int series_
                   float dm, int dm_idx, int output, psx_candidate* h_out, int* h_nassoc,
                   int* h_trial, size_t cap, size_t* n_out)
 {
-    clear_error();
-    if (!s || !series || !n_out || nsamps == 0 || (output != PSX_OUT_TRIAL && output != PSX_OUT_DM)) {
-        set_error("search_dm: bad arguments");
-        return PSX_ERR_INVALID;
-    }
-    *n_out = 0;
-    s->launches = 0;
-    s->ffts = 0;
-    const int dev_rc = cuda_status(cudaSetDevice(s->device), "cudaSetDevice");
-    if (dev_rc != PSX_OK) return dev_rc;
-    PSX_TRY(s->prologue(series, nsamps, series_on_device != 0));
-    const psx_search_config& c = s->cfg;
-    s->accs = accel_list(c.acc_lo, c.acc_hi, c.acc_tol, c.acc_pulse_width, s->N, c.tsamp,
-                         c.cfreq_hz, c.ch_bw_hz, dm, c.cdm);
-    const int nacc = (int)s->accs.size();
-    PSX_TRY(s->grow_ktab((size_t)nacc));
-    for (int t = 0; t < nacc; ++t) s->h_ktab[t] = accel_fact(s->accs[t], c.tsamp);
-    PSX_CUDA(cudaMemcpyAsync(s->d_ktab, s->h_ktab, sizeof(double) * nacc, cudaMemcpyHostToDevice,
-                             s->st));
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        PSX_TRY(s->run_trials(nacc));
-        PSX_CUDA(cudaMemcpyAsync(s->h_count, s->d_count, sizeof(unsigned) * 2,
-                                 cudaMemcpyDeviceToHost, s->st));
-        PSX_CUDA(cudaStreamSynchronize(s->st));
-        if (s->h_count[0] <= s->rec_cap) break;
-        // more hits than the record buffer holds: grow it and run again
-        PSX_TRY(s->grow_records(s->h_count[0]));
-        if (attempt == 1) {
-            set_error("search_dm: record buffer overflow");
-            return PSX_ERR_OVERFLOW;
-        }
-    }
-    s->info.ntrials = nacc;
-    s->info.above_threshold = (long long)s->h_count[0];
-    std::vector<psx_candidate> out;
-    std::vector<int> nassoc, trial_of;
-    PSX_TRY(s->collect(dm, dm_idx, output, out, nassoc, trial_of));
-    s->info.kernel_launches = s->launches;
-    s->info.fft_launches = s->ffts;
-    *n_out = out.size();
-    if (out.size() > cap || (!h_out && out.size())) {
-        set_error("search_dm: %zu candidates, buffer holds %zu", out.size(), cap);
-        return PSX_ERR_OVERFLOW;
-    }
-    if (!out.empty()) std::memcpy(h_out, out.data(), sizeof(psx_candidate) * out.size());
-    for (size_t k = 0; k < out.size(); ++k) {
-        if (h_nassoc) h_nassoc[k] = nassoc[k];
-        if (h_trial) h_trial[k] = trial_of[k];
-    }
-    return PSX_OK;
+    const float* one[1] = {series};
+    return psx_search_block(s, one, nsamps, series_on_device, &dm, &dm_idx, 1, output, h_out,
+                            h_nassoc, h_trial, nullptr, cap, n_out);
 }
 
 int psx_search_last_info(const psx_search* s, psx_search_info* info)
@@ -839,6 +1062,9 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
 {
     clear_error();
     if (!s) return PSX_ERR_INVALID;
+    // the dereddened series on the device is the last DM's
+    Slot& sl = s->slot[s->last_slot];
+    const std::vector<float>& accs = sl.accs;
     if (h_tim_dered)
         PSX_CUDA(cudaMemcpyAsync(h_tim_dered, s->d_tim, sizeof(float) * s->N,
                                  cudaMemcpyDeviceToHost, s->st));
@@ -846,12 +1072,12 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
         PSX_CUDA(cudaMemcpyAsync(h_norm2, s->d_stat + 3, sizeof(float) * 2, cudaMemcpyDeviceToHost,
                                  s->st));
     if (h_tim_r || h_pspec) {
-        if (trial < 0 || trial >= (int)s->accs.size()) {
+        if (trial < 0 || trial >= (int)accs.size()) {
             set_error("debug_tap: trial %d out of range", trial);
             return PSX_ERR_INVALID;
         }
         PSX_TRY(launch_resample(s->d_tim, s->d_tr, s->N, nullptr,
-                                accel_fact(s->accs[trial], s->cfg.tsamp), 1, s->N, false, s->st));
+                                accel_fact(accs[trial], s->cfg.tsamp), 1, s->N, false, s->st));
         if (h_tim_r)
             PSX_CUDA(cudaMemcpyAsync(h_tim_r, s->d_tr, sizeof(float) * s->N,
                                      cudaMemcpyDeviceToHost, s->st));

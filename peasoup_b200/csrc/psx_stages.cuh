@@ -37,4 +37,10 @@ int remove_baseline_pass(float* d_x, size_t n, double2* d_partials, double* d_su
 
 int launch_fill(float* d_x, size_t n, float value, cudaStream_t s);
 
+// Per-block partial sums of x and x^2 over [0, n) (reduction_blocks() of them).
+int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_t s);
+
+// x[i] -= *d_v.
+int launch_sub_scalar(float* d_x, size_t n, const float* d_v, cudaStream_t s);
+
 }  // namespace psx

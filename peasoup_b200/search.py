@@ -18,7 +18,7 @@ from typing import List, Optional
 import numpy as np
 
 from . import _lib
-from ._lib import SearchConfig, SearchInfo, check, load
+from ._lib import SearchConfig, SearchInfo, SearchProfile, check, load
 
 CAND_DTYPE = np.dtype([("dm", "<f4"), ("dm_idx", "<i4"), ("acc", "<f4"),
                        ("nh", "<i4"), ("snr", "<f4"), ("freq", "<f4")])
@@ -50,7 +50,11 @@ class SearchParams:
     birdie_widths: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
     mode: str = "batched"          # "plain": one trial per launch
     batch: int = 0                 # 0: chosen from the transform length
-    fft_callback: bool = True      # batched: resample inside cuFFT
+    # batched: resample inside cuFFT through an LTO load callback.  Off by
+    # default: the cuFFT 11.4 library of CUDA 12.9 fails plan creation for
+    # LTO callbacks on sm_100 (CUFFT_INTERNAL_ERROR), so the resample runs as
+    # its own kernel.
+    fft_callback: bool = False
     graph: bool = True             # batched: CUDA-graph trial schedule
 
     def to_c(self):
@@ -143,6 +147,57 @@ class AccelSearch:
         del keep
         k = nout.value
         return self._out[:k].copy(), self._na[:k].copy(), self._tr[:k].copy()
+
+    def search_block(self, series, dms, dm_idx=None, per_dm: bool = True):
+        """Search a block of DM trials (a sequence of host arrays, a 2-D
+        array, or a sequence / 2-D CUDA tensor), overlapping the host-side
+        clustering of one DM with the GPU search of the next.  Returns
+        (candidates, nassoc, trial_index, dm_position)."""
+        rows = [series[i] for i in range(len(series))]
+        n = len(rows)
+        on_dev = int(hasattr(rows[0], "is_cuda") and rows[0].is_cuda)
+        keep = []
+        if on_dev:
+            ptrs = (C.c_void_p * n)(*[r.data_ptr() for r in rows])
+            nsamps = rows[0].numel()
+        else:
+            arrs = [np.ascontiguousarray(r, np.float32) for r in rows]
+            keep = arrs
+            ptrs = (C.c_void_p * n)(*[a.ctypes.data for a in arrs])
+            nsamps = arrs[0].size
+        dm_arr = np.ascontiguousarray(dms, np.float32)
+        idx_arr = np.ascontiguousarray(np.arange(n) if dm_idx is None else dm_idx, np.int32)
+        out_mode = _lib.PSX_OUT_DM if per_dm else _lib.PSX_OUT_TRIAL
+        nout = C.c_size_t()
+        L = load()
+        while True:
+            dmpos = np.zeros(self._cap, np.int32)
+            rc = L.psx_search_block(self._handle, ptrs, nsamps, on_dev, dm_arr.ctypes.data,
+                                    idx_arr.ctypes.data, n, out_mode, self._out.ctypes.data,
+                                    self._na.ctypes.data, self._tr.ctypes.data,
+                                    dmpos.ctypes.data, self._cap, C.byref(nout))
+            if rc == _lib.PSX_ERR_OVERFLOW and nout.value > self._cap:
+                self._cap = int(nout.value * 1.5) + 1024
+                self._out = np.zeros(self._cap, CAND_DTYPE)
+                self._na = np.zeros(self._cap, np.int32)
+                self._tr = np.zeros(self._cap, np.int32)
+                continue
+            check(rc, "search_block")
+            break
+        del keep
+        k = nout.value
+        return (self._out[:k].copy(), self._na[:k].copy(), self._tr[:k].copy(),
+                dmpos[:k].copy())
+
+    def set_profile(self, on: bool = True) -> None:
+        """Record CUDA events around every launch group (stage timings)."""
+        check(load().psx_search_set_profile(self._handle, int(on)), "search_set_profile")
+
+    def profile(self, reset: bool = False) -> dict:
+        p = SearchProfile()
+        check(load().psx_search_get_profile(self._handle, C.byref(p), int(reset)),
+              "search_get_profile")
+        return {f: getattr(p, f) for f, _ in SearchProfile._fields_}
 
     def info(self) -> dict:
         i = SearchInfo()

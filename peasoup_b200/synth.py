@@ -146,39 +146,53 @@ def survey_series_np(plan: SurveyBlock, dm_index: int, seed: int = 2) -> np.ndar
 
 
 def survey_block_torch(plan: SurveyBlock, seed: int = 2, device: str = "cuda",
-                       dm_indices=None):
+                       dm_indices=None, chunk: int = 8, out=None):
     """The survey block generated on the GPU with torch (fast at 2^23):
-    returns a float32 tensor [len(dm_indices), nsamps]."""
+    returns a float32 tensor [len(dm_indices), nsamps].  Rows are made in
+    chunks; the birdie sinusoids (common to every DM trial, as RFI is) are
+    summed once."""
     import torch
     idx = list(range(plan.ndm)) if dm_indices is None else list(dm_indices)
     n, ts = plan.nsamps, plan.tsamp
-    out = torch.empty((len(idx), n), dtype=torch.float32, device=device)
+    if out is None:
+        out = torch.empty((len(idx), n), dtype=torch.float32, device=device)
     nb = n // 2 + 1
     f = torch.arange(nb, device=device, dtype=torch.float64) / (n * ts)
     srel = torch.zeros(nb, device=device, dtype=torch.float64)
     m = (f > 0) & (f < 1.0)
     srel[m] = f[m] ** -1.5
-    amp_red = 20.0 * np.sqrt(n) * torch.sqrt(srel)
-    t = torch.arange(n, device=device, dtype=torch.float64) * ts
+    amp_red = (20.0 * np.sqrt(n) / np.sqrt(2.0)) * torch.sqrt(srel)
     g = torch.Generator(device=device)
-    for row, d in enumerate(idx):
-        g.manual_seed(int(seed) * 1000003 + int(d))
-        x = 128.0 + 20.0 * torch.randn(n, generator=g, device=device, dtype=torch.float64)
-        z = torch.complex(torch.randn(nb, generator=g, device=device, dtype=torch.float64),
-                          torch.randn(nb, generator=g, device=device, dtype=torch.float64))
-        x += torch.fft.irfft(amp_red * z / np.sqrt(2.0), n=n)
-        for j, p in enumerate(plan.pulsars):
-            if plan.pulsar_dm_idx[j] != d:
-                continue
-            k = p.accel * ts / (2.0 * C_LIGHT)
-            i = torch.arange(n, device=device, dtype=torch.float64)
-            phi = (i - k * i * (i - n)) * (ts / p.period) + p.phase0
-            dd = phi - torch.round(phi)
-            sig = p.duty / (2.0 * np.sqrt(2.0 * np.log(2.0)))
-            x += p.amp * torch.exp(-0.5 * (dd / sig) ** 2)
-        ph = torch.rand(len(plan.birdie_freqs), generator=g, device=device,
-                        dtype=torch.float64) * 2 * np.pi
-        for b, fb in enumerate(plan.birdie_freqs):
-            x += 2.0 * torch.sin(2 * np.pi * float(fb) * t + ph[b])
-        out[row] = torch.clamp(torch.round(x), 0, 255).to(torch.float32)
+    g.manual_seed(int(seed) * 7919 + 17)
+    t = torch.arange(n, device=device, dtype=torch.float64) * ts
+    ph = torch.rand(len(plan.birdie_freqs), generator=g, device=device,
+                    dtype=torch.float64) * 2 * np.pi
+    birdies = torch.zeros(n, device=device, dtype=torch.float64)
+    for b, fb in enumerate(plan.birdie_freqs):
+        birdies += 2.0 * torch.sin(2 * np.pi * float(fb) * t + ph[b])
+    del t
+    for c0 in range(0, len(idx), chunk):
+        rows = idx[c0:c0 + chunk]
+        g.manual_seed(int(seed) * 1000003 + int(rows[0]))
+        x = 128.0 + 20.0 * torch.randn((len(rows), n), generator=g, device=device,
+                                       dtype=torch.float64)
+        z = torch.complex(torch.randn((len(rows), nb), generator=g, device=device,
+                                      dtype=torch.float64),
+                          torch.randn((len(rows), nb), generator=g, device=device,
+                                      dtype=torch.float64))
+        x += torch.fft.irfft(z * amp_red, n=n)
+        del z
+        x += birdies
+        for r, d in enumerate(rows):
+            for j, p in enumerate(plan.pulsars):
+                if plan.pulsar_dm_idx[j] != d:
+                    continue
+                k = p.accel * ts / (2.0 * C_LIGHT)
+                i = torch.arange(n, device=device, dtype=torch.float64)
+                phi = (i - k * i * (i - n)) * (ts / p.period) + p.phase0
+                dd = phi - torch.round(phi)
+                sig = p.duty / (2.0 * np.sqrt(2.0 * np.log(2.0)))
+                x[r] += p.amp * torch.exp(-0.5 * (dd / sig) ** 2)
+        out[c0:c0 + len(rows)] = torch.clamp(torch.round(x), 0, 255).to(torch.float32)
+        del x
     return out

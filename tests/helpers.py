@@ -2,11 +2,16 @@
 import numpy as np
 
 
+def _wide(x):
+    x = np.asarray(x)
+    return x.astype(np.complex128) if np.iscomplexobj(x) else x.astype(np.float64)
+
+
 def rel_err(a, b, floor_frac=1e-3):
     """max |a-b| / max(|b|, floor) with the floor a fraction of the RMS of
     b, so that bins near zero are judged against the spectrum's scale."""
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    a = _wide(a)
+    b = _wide(b)
     scale = np.sqrt(np.mean(np.abs(b) ** 2)) if b.size else 1.0
     den = np.maximum(np.abs(b), floor_frac * scale + 1e-300)
     return float(np.max(np.abs(a - b) / den)) if a.size else 0.0
@@ -14,8 +19,8 @@ def rel_err(a, b, floor_frac=1e-3):
 
 def err_vs_rms(a, b):
     """max |a-b| relative to the RMS of b."""
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    a = _wide(a)
+    b = _wide(b)
     scale = np.sqrt(np.mean(np.abs(b) ** 2)) if b.size else 1.0
     return float(np.max(np.abs(a - b)) / scale) if a.size else 0.0
 

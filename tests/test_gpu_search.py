@@ -93,12 +93,12 @@ def test_plain_batched_callback_identical(S, n):
     kw = dict(acc_lo=-200.0, acc_hi=200.0, nharmonics=5, min_snr=6.0)
     outs = []
     for mode, cb, graph, batch in (("plain", False, False, 0), ("batched", False, False, 4),
-                                   ("batched", True, False, 8), ("batched", True, True, 8)):
+                                   ("batched", False, True, 8), ("batched", False, True, 1)):
         s = search.AccelSearch(_params(S, n, ts, mode=mode, fft_callback=cb, graph=graph,
                                        batch=batch, **kw))
         c, na, tr = s.search(x, 1.5, 3, per_dm=False)
         info = s.info()
-        assert info["fft_callback"] == int(cb and mode == "batched")
+        assert info["graph"] == int(graph and mode == "batched")
         outs.append((mode, cb, c, info))
         s.close()
     base = outs[0][2]
@@ -106,6 +106,52 @@ def test_plain_batched_callback_identical(S, n):
         nm, ua, ub, worst = match_candidates(c, base, 6.0, margin=0.0)
         exact = len(c) == len(base) and np.array_equal(c, base)
         assert exact or (not ua and not ub and worst < 1e-5), (mode, cb, ua[:3], ub[:3], worst)
+
+
+def test_fft_callback_path_fails_cleanly_or_matches(S):
+    """The resample-in-cuFFT path needs LTO callbacks, which cuFFT rejects
+    on sm_100 in this toolkit; creation must then fail with a cuFFT status
+    (never fall back silently).  Where it works it must match the default."""
+    search, synth = S
+    from peasoup_b200._lib import PSX_ERR_CUFFT, PsxError
+    n, ts = 1 << 16, 64e-6
+    x = synth.make_series_np(synth.SeriesSpec(nsamps=n, tsamp=ts), 3)
+    kw = dict(acc_lo=-100.0, acc_hi=100.0, nharmonics=3, min_snr=6.0)
+    try:
+        s = search.AccelSearch(_params(S, n, ts, fft_callback=True, batch=4, **kw))
+    except PsxError as e:
+        assert e.status == PSX_ERR_CUFFT
+        return
+    c = s.search(x)[0]
+    assert s.info()["fft_callback"] == 1
+    s.close()
+    ref = search.AccelSearch(_params(S, n, ts, batch=4, **kw))
+    nm, ua, ub, worst = match_candidates(c, ref.search(x)[0], 6.0, margin=0.0)
+    assert not ua and not ub and worst < 1e-5
+
+
+def test_block_equals_single_dm_calls(S):
+    search, synth = S
+    n, ts = 1 << 16, 64e-6
+    rng = np.random.default_rng(6)
+    xs = np.stack([synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(4e-3 * (d + 1), 10.0 * d, 0.05, 0.6)]), d)
+        for d in range(5)])
+    dms = np.array([0.0, 2.0, 4.0, 6.0, 8.0], np.float32)
+    p = _params(S, n, ts, acc_lo=-60.0, acc_hi=60.0, nharmonics=4, min_snr=6.5, batch=4)
+    s = search.AccelSearch(p)
+    s.set_profile(True)
+    blk, bna, btr, bdm = s.search_block(xs, dms)
+    prof = s.profile(reset=True)
+    assert prof["dms"] == 5 and prof["trials"] > 0 and prof["harm_ms"] > 0
+    one = [s.search(xs[d], float(dms[d]), d)[0] for d in range(5)]
+    assert np.array_equal(blk, np.concatenate(one))
+    assert np.array_equal(bdm, np.concatenate([np.full(len(o), d) for d, o in enumerate(one)]))
+    import torch
+    dev = torch.from_numpy(xs).cuda()
+    blk2 = s.search_block(dev, dms)[0]
+    assert np.array_equal(blk, blk2)
+    s.close()
 
 
 def test_repeatable_and_graph_replay(S):

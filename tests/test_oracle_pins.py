@@ -194,9 +194,10 @@ def test_oracle_stages_match_reference(oracle, rg):
     assert np.allclose([m, r, s], rg["stats_out"], rtol=1e-6)
     nrm = oracle.normalise(rg["stats_in"].astype(np.float64), 1.25, 0.75)
     assert rel_err(nrm, rg["norm_out"]) < 1e-6
+    # FP32 accumulation of up to 32 terms in the reference: ~3e-6 of RMS
     hs = oracle.harmonic_sums(rg["harm_in"].astype(np.float64), 5)
     for h in range(5):
-        assert err_vs_rms(hs[h], rg["harm_out"][h]) < 1e-6
+        assert err_vs_rms(hs[h], rg["harm_out"][h]) < 1e-5
     spec = rg["peaks_in"].astype(np.float64)
     for nh in range(6):
         _, sn, fr = oracle.find_peaks(spec, float(rg["peaks_bw"]), nh, 7.0, 0.1, 1100.0)
