@@ -164,11 +164,8 @@ def sum_over_ranks(ws, v):
 
 def dm_schedule(rank, ws, steps, per_step, offset=0):
     """DM indices of each step of this rank (rank-interleaved blocks)."""
-    out = []
-    for s in range(steps):
-        base = ((offset + s) * ws + rank) * per_step
-        out.append([(base + j) % NDM for j in range(per_step)])
-    return out
+    from peasoup_b200.replicas import dm_schedule as sched
+    return sched(NDM, rank, ws, steps, per_step, offset)
 
 
 def trials_of(plan, dm_list):

@@ -345,6 +345,8 @@ typedef struct {
     long long groups;     /* launch groups timed */
     long long trials;     /* acceleration trials timed */
     long long dms;        /* DM trials timed */
+    long long event_errors; /* event pairs that could not be timed */
+    int last_event_error;   /* cudaError_t of the last such pair */
 } psx_search_profile;
 
 int psx_search_set_profile(psx_search* s, int on);

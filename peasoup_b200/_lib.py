@@ -71,7 +71,8 @@ class SearchInfo(C.Structure):
 class SearchProfile(C.Structure):
     _fields_ = [("prologue_ms", C.c_double), ("resample_ms", C.c_double),
                 ("fft_ms", C.c_double), ("form_ms", C.c_double), ("harm_ms", C.c_double),
-                ("groups", C.c_longlong), ("trials", C.c_longlong), ("dms", C.c_longlong)]
+                ("groups", C.c_longlong), ("trials", C.c_longlong), ("dms", C.c_longlong),
+                ("event_errors", C.c_longlong), ("last_event_error", C.c_int)]
 
 
 _vp = C.c_void_p

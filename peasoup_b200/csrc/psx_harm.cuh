@@ -143,7 +143,9 @@ __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, 
             smem4[j] = g < len4 ? row4[g] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     }
-#pragma unroll 1
+    // fully unrolled: every fraction's slot offset and shape is a
+    // compile-time constant
+#pragma unroll
     for (int q = 0; q < nfrac(F); ++q) {
         const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
         const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);

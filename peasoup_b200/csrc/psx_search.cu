@@ -573,15 +573,24 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
 void psx_search::read_profile(Slot& s)
 {
     if (!s.profiled) return;
-    float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, s.ev[0], s.ev[1]) == cudaSuccess) prof.prologue_ms += ms;
+    auto span = [&](cudaEvent_t a, cudaEvent_t b, double& acc) {
+        float ms = 0.f;
+        const cudaError_t e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess) {
+            acc += ms;
+        } else {
+            ++prof.event_errors;
+            prof.last_event_error = (int)e;
+        }
+    };
+    span(s.ev[0], s.ev[1], prof.prologue_ms);
     for (int g = 0; g < s.groups; ++g) {
         cudaEvent_t prev = g == 0 ? s.ev[1] : s.ev[2 + 4 * (g - 1) + 3];
         cudaEvent_t* e = &s.ev[2 + 4 * g];
-        if (cudaEventElapsedTime(&ms, prev, e[0]) == cudaSuccess) prof.resample_ms += ms;
-        if (cudaEventElapsedTime(&ms, e[0], e[1]) == cudaSuccess) prof.fft_ms += ms;
-        if (cudaEventElapsedTime(&ms, e[1], e[2]) == cudaSuccess) prof.form_ms += ms;
-        if (cudaEventElapsedTime(&ms, e[2], e[3]) == cudaSuccess) prof.harm_ms += ms;
+        span(prev, e[0], prof.resample_ms);
+        span(e[0], e[1], prof.fft_ms);
+        span(e[1], e[2], prof.form_ms);
+        span(e[2], e[3], prof.harm_ms);
     }
     prof.groups += s.groups;
     prof.trials += (long long)s.accs.size();

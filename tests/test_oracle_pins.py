@@ -166,63 +166,90 @@ def test_search_recovers_injected_pulsar(oracle):
 
 
 # ------------------------------------------------------------ against the reference build
-def test_oracle_resample_index_matches_reference(oracle, rg):
-    accs, ts = rg["resample_accs"], float(rg["resample_tsamp"])
-    for n in (1 << 18, 3 << 16):
-        d = rg[f"resampleII_{n}_delta"]
-        for t, a in enumerate(accs):
-            got = oracle.resampleII_index(n, float(a), ts).astype(np.int64) - np.arange(n)
-            assert np.array_equal(got, d[t]), (n, a, np.count_nonzero(got != d[t]))
+@pytest.fixture(scope="module")
+def gi(rg):
+    """The seeded inputs the reference ran on, regenerated and checked."""
+    import sys
+    sys.path.insert(0, GOLD)
+    import golden_inputs as GI
+    inp = GI.inputs()
+    for k, v in inp.items():
+        assert GI.sha(v) == str(rg[f"sha_{k}"]), f"input {k} does not regenerate"
+    return GI, inp
 
 
-def test_oracle_stages_match_reference(oracle, rg):
-    x = rg["fft_in"].astype(np.float64)
+def test_oracle_resample_index_matches_reference(oracle, rg, gi):
+    GI, _ = gi
+    for n in GI.RESAMPLE_SIZES:
+        for nm, fn in (("resampleII", oracle.resampleII_index),):
+            d = rg[f"{nm}_{n}_delta"].astype(np.int64)
+            for t, a in enumerate(GI.RESAMPLE_ACCS):
+                got = fn(n, float(a), float(GI.RESAMPLE_TSAMP)).astype(np.int64) - np.arange(n)
+                assert np.array_equal(got, d[t]), (n, a, np.count_nonzero(got != d[t]))
+
+
+def test_centred_resample_index_matches_reference(oracle, rg, gi):
+    """The centred form's rounding depends on contraction; the reference's
+    maps must equal one of the two evaluations for every acceleration."""
+    GI, _ = gi
+    for n in GI.RESAMPLE_SIZES:
+        d = rg[f"resample_{n}_delta"].astype(np.int64)
+        for t, a in enumerate(GI.RESAMPLE_ACCS):
+            v = [oracle.resample_index(n, float(a), float(GI.RESAMPLE_TSAMP), f).astype(np.int64)
+                 - np.arange(n) for f in (0, 1)]
+            assert np.array_equal(v[0], d[t]) or np.array_equal(v[1], d[t]), (n, a)
+
+
+def test_oracle_stages_match_reference(oracle, rg, gi):
+    GI, inp = gi
+    x = inp["fft_in"].astype(np.float64)
     assert err_vs_rms(oracle.rfft(x), rg["fft_r2c"]) < 1e-5
-    Xc = rg["fft_c2r_in"].astype(np.complex128)
-    assert err_vs_rms(oracle.irfft(Xc, 1 << 14), rg["fft_c2r"]) < 1e-5
-    X = rg["form_in"].astype(np.complex128)
+    assert err_vs_rms(oracle.irfft(inp["fft_c2r_in"].astype(np.complex128), 1 << 12),
+                      rg["fft_c2r"]) < 1e-5
+    X = inp["form_in"].astype(np.complex128)
     assert rel_err(oracle.form_power(X), rg["form_power"]) < 1e-6
     assert rel_err(oracle.form_interbin(X), rg["form_interbin"]) < 1e-6
-    med = oracle.running_median(rg["median_in"].astype(np.float64), float(rg["median_bw"]))
+    med = oracle.running_median(inp["median_in"].astype(np.float64), GI.MEDIAN_BW)
     assert rel_err(med, rg["median_out"]) < 1e-6
-    Xd = oracle.deredden(rg["dered_X"].astype(np.complex128), med)
+    Xd = oracle.deredden(inp["dered_X"].astype(np.complex128), med)
     assert err_vs_rms(Xd, rg["dered_out"]) < 1e-5
-    Z = oracle.zap(rg["dered_X"].astype(np.complex128), float(np.float32(rg["median_bw"])),
-                   rg["zap_freqs"], rg["zap_widths"])
+    Z = oracle.zap(inp["dered_X"].astype(np.complex128), float(np.float32(GI.MEDIAN_BW)),
+                   GI.ZAP_FREQS, GI.ZAP_WIDTHS)
     assert np.array_equal(Z.astype(np.complex64), rg["zap_out"])
-    m, r, s = oracle.stats(rg["stats_in"].astype(np.float64))
-    assert np.allclose([m, r, s], rg["stats_out"], rtol=1e-6)
-    nrm = oracle.normalise(rg["stats_in"].astype(np.float64), 1.25, 0.75)
+    m, r, sd = oracle.stats(inp["stats_in"].astype(np.float64))
+    assert np.allclose([m, r, sd], rg["stats_out"], rtol=1e-6)
+    nrm = oracle.normalise(inp["stats_in"].astype(np.float64), 1.25, 0.75)
     assert rel_err(nrm, rg["norm_out"]) < 1e-6
+    base, _ = oracle.remove_baseline(inp["baseline_in"].astype(np.float64))
+    assert err_vs_rms(base, rg["baseline_out"]) < 1e-4
     # FP32 accumulation of up to 32 terms in the reference: ~3e-6 of RMS
-    hs = oracle.harmonic_sums(rg["harm_in"].astype(np.float64), 5)
+    hs = oracle.harmonic_sums(inp["harm_in"].astype(np.float64), 5)
     for h in range(5):
         assert err_vs_rms(hs[h], rg["harm_out"][h]) < 1e-5
-    spec = rg["peaks_in"].astype(np.float64)
+    spec = inp["peaks_in"].astype(np.float64)
     for nh in range(6):
-        _, sn, fr = oracle.find_peaks(spec, float(rg["peaks_bw"]), nh, 7.0, 0.1, 1100.0)
+        _, sn, fr = oracle.find_peaks(spec, GI.MEDIAN_BW, nh, 7.0, 0.1, 1100.0)
         assert np.array_equal(fr, rg[f"peaks_{nh}_freq"]), nh
         assert np.allclose(sn, rg[f"peaks_{nh}_snr"], rtol=1e-6), nh
 
 
 @pytest.mark.parametrize("case", ["w1", "w2"])
-def test_oracle_worker_matches_reference(oracle, rg, case):
+def test_oracle_worker_matches_reference(oracle, rg, gi, case):
     from peasoup_b200 import synth
-    series, dms, meta = rg[f"{case}_series"], rg[f"{case}_dms"], rg[f"{case}_meta"]
-    ts, n, lo, hi, F, thr, cdm = meta
-    zf = rg[f"{case}_zap_freqs"] if f"{case}_zap_freqs" in rg else np.zeros(0, np.float32)
-    zw = rg[f"{case}_zap_widths"] if f"{case}_zap_widths" in rg else np.zeros(0, np.float32)
+    GI, _ = gi
+    name, series, dms, ts, n, kw, zap = [c for c in GI.worker_cases() if c[0] == case][0]
+    assert GI.sha(series) == str(rg[f"sha_{case}_series"])
+    zf, zw = zap if zap is not None else (np.zeros(0, np.float32), np.zeros(0, np.float32))
+    tobs = float(np.float32(np.float32(n) * np.float32(ts)))
     got = []
-    tobs = float(np.float32(np.float32(int(n)) * np.float32(ts)))
     for d in range(len(dms)):
-        p = oracle.SearchParams(fft_size=int(n), tsamp=float(ts), dm=float(dms[d]), cdm=float(cdm),
-                                dm_idx=d, acc_lo=float(lo), acc_hi=float(hi), nharmonics=int(F),
-                                min_snr=float(thr), cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ,
-                                birdie_freqs=zf, birdie_widths=zw)
+        p = oracle.SearchParams(fft_size=n, tsamp=ts, dm=float(dms[d]), dm_idx=d,
+                                cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ, birdie_freqs=zf,
+                                birdie_widths=zw, **kw)
         c, _ = oracle.search_dm(series[d], p)
         surv, _, _, _ = oracle.accel_distill(c, tobs, 1e-4)
         got.append(surv)
-    got = np.concatenate(got) if got else np.zeros(0, oracle.CAND_DTYPE)
-    nm, ua, ub, worst = match_candidates(got, rg[f"{case}_cands"], float(thr))
+    got = np.concatenate(got)
+    nm, ua, ub, worst = match_candidates(got, rg[f"{case}_cands"], float(kw["min_snr"]))
     assert not ua and not ub, (ua[:5], ub[:5])
     assert nm > 0 and worst < 1e-3
