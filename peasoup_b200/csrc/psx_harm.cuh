@@ -6,14 +6,19 @@
 // spectrum (i0 a multiple of 128).  The fraction m/2^h of output bin
 // i0+j is input bin (i0*m >> h) + ((j*m + 2^(h-1)) >> h): every fraction
 // reads one contiguous window of about T*m/2^h bins that starts at the
-// exact integer i0*m/2^h.  The CTA stages the tile and the 2^F - 1
-// windows in shared memory with 128-bit loads, then each thread sums its
-// outputs with shared loads at per-fraction base offsets plus
-// compile-time immediates, in the reference's summation order, tests each
-// fold against the threshold inside its search range and appends the hits
-// with one atomic per warp and fold.
+// exact integer i0*m/2^h.  One thread stages the tile and the 2^F - 1
+// windows into shared memory with bulk asynchronous copies (the TMA
+// engine) completing on one mbarrier; every thread then sums its outputs
+// with shared loads at per-fraction base offsets plus compile-time
+// immediates, in the reference's summation order.
+//
+// Threshold crossings are rare, so the first pass only ORs "value >
+// threshold" into a flag.  A CTA in which any thread saw a crossing runs a
+// second pass over the staged data that applies each fold's search range
+// and appends the hits with one atomic per warp and fold.
 #pragma once
 #include <cuda_runtime.h>
+#include <stdint.h>
 #include "psx_device.cuh"
 
 namespace psx {
@@ -55,6 +60,68 @@ __host__ __device__ constexpr int harm_smem_floats(int F, int T)
     return slot_offset(nfrac(F), T);
 }
 
+// ---- bulk asynchronous copy (TMA engine) and mbarrier helpers ---------
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned), completing as transaction bytes on `bar`.  Not
+// multicast: the destination is this CTA's own shared memory.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Bounded wait: gives up after `limit` polls (each poll may suspend the
+// thread for a hardware-defined time) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase, unsigned limit)
+{
+    for (unsigned it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+// Status written to counter[1] when staging could not complete (the
+// engine keeps its hit count in counter[0] and this error word next to it).
+constexpr unsigned kHarmStagingTimeout = 0x5441u;
+
 __device__ __forceinline__ void emit_hit(bool hit, int trial, int fold, unsigned bin, float val,
                                          int4* __restrict__ rec, unsigned* __restrict__ counter,
                                          unsigned cap, unsigned lane)
@@ -81,43 +148,78 @@ template <> __device__ __forceinline__ float fold_scale<3>(float val) { return v
 template <> __device__ __forceinline__ float fold_scale<4>(float val) { return val * 0.25; }
 template <> __device__ __forceinline__ float fold_scale<5>(float val) { return val * rsqrt(32.0); }
 
-template <int Q, int F, int T, int BD>
+// Context of one thread's outputs: tile start, thread index, offsets.
+template <int F, int T, int BD>
+struct HarmThread {
+    static constexpr int K = T / BD;
+    static constexpr int NF = nfrac(F) > 0 ? nfrac(F) : 1;
+    const float* __restrict__ sm;
+    unsigned i0, tid, lane;
+    unsigned base[NF];
+};
+
+// Adds fraction Q to every output of the thread; at a fold boundary either
+// ORs the threshold test into `any` (EMIT false) or applies the fold's
+// search range and appends hits (EMIT true).  Recurses to Q+1.
+template <int Q, int F, int T, int BD, bool EMIT>
 struct FracStep {
-    // Adds fraction Q to every output of this thread (K outputs), emitting
-    // at fold boundaries, then recurses to fraction Q+1.
-    static __device__ __forceinline__ void run(const float* __restrict__ sm, float (&val)[T / BD],
-                                               const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                               unsigned i0, unsigned tid, unsigned lane,
-                                               const PeakParams& pp, int trial,
+    static __device__ __forceinline__ void run(const HarmThread<F, T, BD>& c, float (&val)[T / BD],
+                                               bool& any, const PeakParams& pp, int trial,
                                                int4* __restrict__ rec,
                                                unsigned* __restrict__ counter, unsigned cap)
     {
         constexpr int h = frac_h(Q), m = frac_m(Q);
         constexpr int step = (BD * m) >> h;  // exact: BD is a multiple of 32
 #pragma unroll
-        for (int k = 0; k < T / BD; ++k) val[k] += sm[base[Q] + k * step];
+        for (int k = 0; k < T / BD; ++k) val[k] += c.sm[c.base[Q] + k * step];
         if (Q == fold_last(h)) {
 #pragma unroll
             for (int k = 0; k < T / BD; ++k) {
-                const unsigned i = i0 + tid + k * BD;
                 const float s = fold_scale<h>(val[k]);
-                const bool hit = (int)i >= pp.start[h] && (int)i < pp.end[h] && s > pp.thresh;
-                emit_hit(hit, trial, h, i, s, rec, counter, cap, lane);
+                if (EMIT) {
+                    const unsigned i = c.i0 + c.tid + k * BD;
+                    const bool hit = (int)i >= pp.start[h] && (int)i < pp.end[h] && s > pp.thresh;
+                    emit_hit(hit, trial, h, i, s, rec, counter, cap, c.lane);
+                } else {
+                    any |= s > pp.thresh;
+                }
             }
         }
-        FracStep<Q + 1, F, T, BD>::run(sm, val, base, i0, tid, lane, pp, trial, rec, counter, cap);
+        FracStep<Q + 1, F, T, BD, EMIT>::run(c, val, any, pp, trial, rec, counter, cap);
     }
 };
 
-template <int F, int T, int BD>
-struct FracStep<(1 << F) - 1, F, T, BD> {
-    static __device__ __forceinline__ void run(const float*, float (&)[T / BD],
-                                               const unsigned (&)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                               unsigned, unsigned, unsigned, const PeakParams&,
-                                               int, int4*, unsigned*, unsigned)
+template <int F, int T, int BD, bool EMIT>
+struct FracStep<(1 << F) - 1, F, T, BD, EMIT> {
+    static __device__ __forceinline__ void run(const HarmThread<F, T, BD>&, float (&)[T / BD],
+                                               bool&, const PeakParams&, int, int4*, unsigned*,
+                                               unsigned)
     {
     }
 };
+
+template <int F, int T, int BD, bool EMIT>
+__device__ __forceinline__ bool harm_pass(const HarmThread<F, T, BD>& c, const PeakParams& pp,
+                                          int trial, int4* __restrict__ rec,
+                                          unsigned* __restrict__ counter, unsigned cap)
+{
+    float val[T / BD];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < T / BD; ++k) {
+        const unsigned j = c.tid + k * BD;
+        val[k] = c.sm[j];
+        if (EMIT) {
+            const unsigned i = c.i0 + j;
+            const bool hit = (int)i >= pp.start[0] && (int)i < pp.end[0] && val[k] > pp.thresh;
+            emit_hit(hit, trial, 0, i, val[k], rec, counter, cap, c.lane);
+        } else {
+            any |= val[k] > pp.thresh;
+        }
+    }
+    FracStep<0, F, T, BD, EMIT>::run(c, val, any, pp, trial, rec, counter, cap);
+    return any;
+}
 
 template <int F, int T, int BD>
 __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, size_t ppitch,
@@ -127,59 +229,87 @@ __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, 
 {
     static_assert(T % 128 == 0 && BD % 32 == 0 && T % BD == 0, "tile shape");
     extern __shared__ float4 smem4[];
+    __shared__ __align__(8) uint64_t bar;
     float* sm = reinterpret_cast<float*>(smem4);
     const int trial = trial0 + (int)blockIdx.y;
     const float* __restrict__ row = p + (size_t)blockIdx.y * ppitch;
-    const float4* __restrict__ row4 = reinterpret_cast<const float4*>(row);
-    const unsigned tid = threadIdx.x, lane = tid & 31u;
+    const unsigned tid = threadIdx.x;
     const unsigned i0 = pp.lo + blockIdx.x * T;
-    const unsigned len4 = row_len / 4;
 
-    // ---- stage the tile and every fraction's window (128-bit loads)
-    {
-        const unsigned a4 = i0 / 4;
-        for (unsigned j = tid; j < T / 4; j += BD) {
-            const unsigned g = a4 + j;
-            smem4[j] = g < len4 ? row4[g] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    }
-    // fully unrolled: every fraction's slot offset and shape is a
-    // compile-time constant
-#pragma unroll
-    for (int q = 0; q < nfrac(F); ++q) {
-        const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-        const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
-        const unsigned last = a + (unsigned)((((unsigned long long)(T - 1) * m) + (1u << (h - 1))) >> h);
-        const unsigned a4 = a & ~3u;
-        const unsigned n4 = (last + 1 - a4 + 3) / 4;
-        float4* dst = smem4 + slot_offset(q, T) / 4;
-        for (unsigned j = tid; j < n4; j += BD) {
-            const unsigned g = a4 / 4 + j;
-            dst[j] = g < len4 ? row4[g] : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+    // ---- stage the tile and every fraction's window: one thread issues
+    // the bulk copies, everyone waits on the mbarrier.  Parts of a window
+    // past the end of the row (only in the last tile) are zero-filled.
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
     }
     __syncthreads();
+    if (tid == 0) {
+        unsigned bytes = 0;
+        unsigned lens[nfrac(F) + 1];
+        {
+            const unsigned ok = i0 < row_len ? min((unsigned)T, row_len - i0) : 0u;
+            lens[0] = ok;
+            bytes += 4u * ok;
+        }
+#pragma unroll
+        for (int q = 0; q < nfrac(F); ++q) {
+            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
+            const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
+            const unsigned last = a + (unsigned)((((unsigned long long)(T - 1) * m) + (1u << (h - 1))) >> h);
+            const unsigned a4 = a & ~3u;
+            const unsigned n = ((last + 1 - a4) + 3u) & ~3u;
+            const unsigned ok = a4 < row_len ? min(n, row_len - a4) : 0u;
+            lens[q + 1] = ok;
+            bytes += 4u * ok;
+        }
+        mbar_arrive_expect_tx(&bar, bytes);
+        if (lens[0]) bulk_g2s(sm, row + i0, 4u * lens[0], &bar);
+#pragma unroll
+        for (int q = 0; q < nfrac(F); ++q) {
+            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
+            const unsigned a4 = (unsigned)(((unsigned long long)i0 * m) >> h) & ~3u;
+            if (lens[q + 1]) bulk_g2s(sm + slot_offset(q, T), row + a4, 4u * lens[q + 1], &bar);
+        }
+    }
+    // zero-fill what lies past the row end (last tile only)
+    if (i0 + T > row_len) {
+        for (unsigned j = tid; j < (unsigned)T; j += BD)
+            if (i0 + j >= row_len) sm[j] = 0.f;
+#pragma unroll
+        for (int q = 0; q < nfrac(F); ++q) {
+            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
+            const unsigned a4 = (unsigned)(((unsigned long long)i0 * m) >> h) & ~3u;
+            for (unsigned j = tid; j < (unsigned)slot_floats(q, T); j += BD)
+                if (a4 + j >= row_len) sm[slot_offset(q, T) + j] = 0.f;
+        }
+    }
+    // Bounded wait; the give-up decision is made for the whole CTA at one
+    // barrier every thread reaches, so no thread is left waiting at a later
+    // barrier.  On failure the copies still in flight get a second bounded
+    // wait before the CTA leaves, and the host sees the error word.
+    const bool staged = mbar_wait_bounded(&bar, 0, 1u << 22);
+    if (!__syncthreads_and(staged)) {
+        if (!staged) mbar_wait_bounded(&bar, 0, 1u << 22);
+        if (tid == 0) atomicExch(counter + 1, kHarmStagingTimeout);
+        return;
+    }
 
-    // ---- per-thread base offsets of each fraction
-    constexpr int NF = nfrac(F) > 0 ? nfrac(F) : 1;
-    unsigned base[NF];
+    HarmThread<F, T, BD> c;
+    c.sm = sm;
+    c.i0 = i0;
+    c.tid = tid;
+    c.lane = tid & 31u;
 #pragma unroll
     for (int q = 0; q < nfrac(F); ++q) {
         const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
         const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
-        base[q] = (unsigned)slot_offset(q, T) + (a & 3u) + ((tid * m + (1u << (h - 1))) >> h);
+        c.base[q] = (unsigned)slot_offset(q, T) + (a & 3u) + ((tid * m + (1u << (h - 1))) >> h);
     }
-
-    // ---- fold 0 and the running sums
-    float val[T / BD];
-#pragma unroll
-    for (int k = 0; k < T / BD; ++k) {
-        const unsigned j = tid + k * BD, i = i0 + j;
-        val[k] = sm[j];
-        const bool hit = (int)i >= pp.start[0] && (int)i < pp.end[0] && val[k] > pp.thresh;
-        emit_hit(hit, trial, 0, i, val[k], rec, counter, cap, lane);
-    }
-    FracStep<0, F, T, BD>::run(sm, val, base, i0, tid, lane, pp, trial, rec, counter, cap);
+    // ---- pass 1: sums and threshold test only
+    const bool any = harm_pass<F, T, BD, false>(c, pp, trial, rec, counter, cap);
+    // ---- pass 2 (rare): exact ranges and compaction
+    if (__syncthreads_or(any)) harm_pass<F, T, BD, true>(c, pp, trial, rec, counter, cap);
 }
 
 }  // namespace psx

@@ -174,7 +174,7 @@ int default_batch(size_t n)
 // Per-DM state that must not be shared by two DMs in flight.
 struct Slot {
     int4* d_rec = nullptr;
-    unsigned* d_count = nullptr;  // [0] hits, [1] baseline active, [2] passes
+    unsigned* d_count = nullptr;  // [0] hits, [1] kernel error, [2] baseline active, [3] passes
     size_t rec_cap = 0;
     int4* h_rec = nullptr;
     unsigned* h_count = nullptr;
@@ -388,11 +388,11 @@ int psx_search::prologue(Slot& s)
     // src/kernels.cu:463-479)
     const int nb = reduction_blocks();
     if (!s.host_baseline) {
-        k_baseline_reset<<<1, 1, 0, st>>>(s.d_count + 1);
+        k_baseline_reset<<<1, 1, 0, st>>>(s.d_count + 2);
         ++s.launches;
         for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
             PSX_TRY(launch_partials(d_tim, ncopy, d_part, st));
-            k_baseline_step<<<1, 32, 0, st>>>(d_part, nb, (double)ncopy, d_mean, s.d_count + 1);
+            k_baseline_step<<<1, 32, 0, st>>>(d_part, nb, (double)ncopy, d_mean, s.d_count + 2);
             PSX_TRY(launch_sub_scalar(d_tim, ncopy, d_mean, st));
             s.launches += 3;
         }
@@ -438,7 +438,7 @@ int psx_search::prologue(Slot& s)
 // s.d_ktab) plus the reset of the record counter.
 int psx_search::trials_enqueue(Slot& s, int nacc)
 {
-    PSX_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned), st));
+    PSX_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned) * 2, st));
     const unsigned T = 256;
     const unsigned span = pk.hi > pk.lo ? pk.hi - pk.lo : 0;
     int t0 = 0, g = 0;
@@ -500,7 +500,9 @@ static int count_groups(int nacc, bool batched, int batch)
 
 int psx_search::run_trials(Slot& s, int nacc)
 {
-    const bool graph = batched() && cfg.use_graph;
+    // events recorded inside a graph carry no timestamps: profiling runs
+    // the schedule without capture
+    const bool graph = batched() && cfg.use_graph && !s.profiled;
     if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
     if (!graph) return trials_enqueue(s, nacc);
     const long long key = ((long long)nacc << 2) | ((&s == &slot[1]) ? 2 : 0) | (s.profiled ? 1 : 0);
@@ -565,7 +567,7 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
     if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[1], st));
     PSX_CUDA(cudaMemcpyAsync(s.d_ktab, s.h_ktab, sizeof(double) * nacc, cudaMemcpyHostToDevice, st));
     PSX_TRY(run_trials(s, nacc));
-    PSX_CUDA(cudaMemcpyAsync(s.h_count, s.d_count, sizeof(unsigned) * 3, cudaMemcpyDeviceToHost, st));
+    PSX_CUDA(cudaMemcpyAsync(s.h_count, s.d_count, sizeof(unsigned) * 4, cudaMemcpyDeviceToHost, st));
     PSX_CUDA(cudaEventRecord(s.done, st));
     return PSX_OK;
 }
@@ -710,7 +712,11 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
     for (int attempt = 0; attempt < 3; ++attempt) {
         PSX_CUDA(cudaEventSynchronize(s.done));
         const size_t hits = s.h_count[0];
-        const bool baseline_pending = !s.host_baseline && s.h_count[1] != 0;
+        if (s.h_count[1] != 0) {
+            set_error("search: harmonic-sum staging did not complete (status 0x%x)", s.h_count[1]);
+            return PSX_ERR_CUDA;
+        }
+        const bool baseline_pending = !s.host_baseline && s.h_count[2] != 0;
         if (hits <= s.rec_cap && !baseline_pending) break;
         // Rare: more hits than the record slot holds, or a baseline that
         // needed more passes than the device loop makes.  Run the DM again
@@ -725,7 +731,7 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
         PSX_TRY(enqueue(s, s.series, s.nsamps, s.on_device, s.dm, s.dm_idx));
     }
     const size_t nrec = s.h_count[0];
-    info.baseline_passes = s.host_baseline ? -1 : (int)s.h_count[2];
+    info.baseline_passes = s.host_baseline ? -1 : (int)s.h_count[3];
     s.host_baseline = false;
     if (nrec) {
         PSX_CUDA(cudaStreamWaitEvent(cst, s.done, 0));
@@ -1013,7 +1019,7 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
     s->info = psx_search_info{};
     s->info.batch = bp;
     s->info.fft_callback = cbk;
-    s->info.graph = s->batched() && s->cfg.use_graph ? 1 : 0;
+    s->info.graph = s->batched() && s->cfg.use_graph && !s->profile ? 1 : 0;
     std::vector<psx_candidate> all, out;
     std::vector<int> all_na, all_tr, all_dm, na, tr;
     int rc = s->enqueue(s->slot[0], series[0], nsamps, series_on_device != 0, dms[0],
