@@ -2,20 +2,20 @@
 // compaction for the search loop (reference src/kernels.cu:34-100 and the
 // copy_if of src/kernels.cu:398-423, fused).
 //
-// One CTA handles a tile of T consecutive output bins [i0, i0+T) of one
-// spectrum (i0 a multiple of 128).  The fraction m/2^h of output bin
-// i0+j is input bin (i0*m >> h) + ((j*m + 2^(h-1)) >> h): every fraction
-// reads one contiguous window of about T*m/2^h bins that starts at the
-// exact integer i0*m/2^h.  One thread stages the tile and the 2^F - 1
-// windows into shared memory with bulk asynchronous copies (the TMA
-// engine) completing on one mbarrier; every thread then sums its outputs
-// with shared loads at per-fraction base offsets plus compile-time
-// immediates, in the reference's summation order.
+// Work item: a tile of T consecutive output bins [i0, i0+T) of one
+// spectrum (i0 a multiple of 128).  The fraction m/2^h of output bin i0+j
+// is input bin (i0*m >> h) + ((j*m + 2^(h-1)) >> h): every fraction reads
+// one contiguous window of about T*m/2^h bins that starts at the exact
+// integer i0*m/2^h.  One thread stages the tile and the 2^F - 1 windows
+// into shared memory with bulk asynchronous copies (the TMA engine)
+// completing on an mbarrier; every thread then sums its outputs with
+// shared loads at per-fraction base offsets plus compile-time immediates,
+// in the reference's summation order.  CTAs are persistent and keep two
+// stages, so the copies of the next item overlap the sums of this one.
 //
-// Threshold crossings are rare, so the first pass only ORs "value >
-// threshold" into a flag.  A CTA in which any thread saw a crossing runs a
-// second pass over the staged data that applies each fold's search range
-// and appends the hits with one atomic per warp and fold.
+// Threshold crossings are rare: each fold's test is one warp vote, and the
+// search-range check and the append (one atomic per warp and fold) run
+// only in warps where some lane crossed.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -148,110 +148,66 @@ template <> __device__ __forceinline__ float fold_scale<3>(float val) { return v
 template <> __device__ __forceinline__ float fold_scale<4>(float val) { return val * 0.25; }
 template <> __device__ __forceinline__ float fold_scale<5>(float val) { return val * rsqrt(32.0); }
 
-// Context of one thread's outputs: tile start, thread index, offsets.
-template <int F, int T, int BD>
-struct HarmThread {
-    static constexpr int K = T / BD;
-    static constexpr int NF = nfrac(F) > 0 ? nfrac(F) : 1;
-    const float* __restrict__ sm;
-    unsigned i0, tid, lane;
-    unsigned base[NF];
-};
+// One warp-level threshold test: the range check and the append only run
+// in warps where some lane crossed the threshold (rare).
+__device__ __forceinline__ void test_and_emit(float s, const PeakParams& pp, int h, unsigned i,
+                                              int trial, int4* __restrict__ rec,
+                                              unsigned* __restrict__ counter, unsigned cap,
+                                              unsigned lane)
+{
+    const bool over = s > pp.thresh;
+    if (__any_sync(0xffffffffu, over)) {
+        const bool hit = over && (int)i >= pp.start[h] && (int)i < pp.end[h];
+        emit_hit(hit, trial, h, i, s, rec, counter, cap, lane);
+    }
+}
 
-// Adds fraction Q to every output of the thread; at a fold boundary either
-// ORs the threshold test into `any` (EMIT false) or applies the fold's
-// search range and appends hits (EMIT true).  Recurses to Q+1.
-template <int Q, int F, int T, int BD, bool EMIT>
+// Adds fraction Q to every output of the thread (K = T/BD outputs, BD
+// apart), tests and emits at fold boundaries, recurses to Q+1.
+template <int Q, int F, int T, int BD>
 struct FracStep {
-    static __device__ __forceinline__ void run(const HarmThread<F, T, BD>& c, float (&val)[T / BD],
-                                               bool& any, const PeakParams& pp, int trial,
+    static __device__ __forceinline__ void run(const float* __restrict__ sm,
+                                               const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                               float (&val)[T / BD], unsigned i0, unsigned tid,
+                                               const PeakParams& pp, int trial,
                                                int4* __restrict__ rec,
                                                unsigned* __restrict__ counter, unsigned cap)
     {
         constexpr int h = frac_h(Q), m = frac_m(Q);
         constexpr int step = (BD * m) >> h;  // exact: BD is a multiple of 32
 #pragma unroll
-        for (int k = 0; k < T / BD; ++k) val[k] += c.sm[c.base[Q] + k * step];
+        for (int k = 0; k < T / BD; ++k) val[k] += sm[base[Q] + k * step];
         if (Q == fold_last(h)) {
 #pragma unroll
-            for (int k = 0; k < T / BD; ++k) {
-                const float s = fold_scale<h>(val[k]);
-                if (EMIT) {
-                    const unsigned i = c.i0 + c.tid + k * BD;
-                    const bool hit = (int)i >= pp.start[h] && (int)i < pp.end[h] && s > pp.thresh;
-                    emit_hit(hit, trial, h, i, s, rec, counter, cap, c.lane);
-                } else {
-                    any |= s > pp.thresh;
-                }
-            }
+            for (int k = 0; k < T / BD; ++k)
+                test_and_emit(fold_scale<h>(val[k]), pp, h, i0 + tid + k * BD, trial, rec,
+                              counter, cap, tid & 31u);
         }
-        FracStep<Q + 1, F, T, BD, EMIT>::run(c, val, any, pp, trial, rec, counter, cap);
+        FracStep<Q + 1, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
     }
 };
 
-template <int F, int T, int BD, bool EMIT>
-struct FracStep<(1 << F) - 1, F, T, BD, EMIT> {
-    static __device__ __forceinline__ void run(const HarmThread<F, T, BD>&, float (&)[T / BD],
-                                               bool&, const PeakParams&, int, int4*, unsigned*,
-                                               unsigned)
+template <int F, int T, int BD>
+struct FracStep<(1 << F) - 1, F, T, BD> {
+    static __device__ __forceinline__ void run(const float*, const unsigned (&)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                               float (&)[T / BD], unsigned, unsigned,
+                                               const PeakParams&, int, int4*, unsigned*, unsigned)
     {
     }
 };
 
-template <int F, int T, int BD, bool EMIT>
-__device__ __forceinline__ bool harm_pass(const HarmThread<F, T, BD>& c, const PeakParams& pp,
-                                          int trial, int4* __restrict__ rec,
-                                          unsigned* __restrict__ counter, unsigned cap)
-{
-    float val[T / BD];
-    bool any = false;
-#pragma unroll
-    for (int k = 0; k < T / BD; ++k) {
-        const unsigned j = c.tid + k * BD;
-        val[k] = c.sm[j];
-        if (EMIT) {
-            const unsigned i = c.i0 + j;
-            const bool hit = (int)i >= pp.start[0] && (int)i < pp.end[0] && val[k] > pp.thresh;
-            emit_hit(hit, trial, 0, i, val[k], rec, counter, cap, c.lane);
-        } else {
-            any |= val[k] > pp.thresh;
-        }
-    }
-    FracStep<0, F, T, BD, EMIT>::run(c, val, any, pp, trial, rec, counter, cap);
-    return any;
-}
-
+// Stage tile `i0` of `row` into the buffer `sm` (thread 0 issues the bulk
+// copies onto `bar`; everything past the row end is zero-filled by all
+// threads).  The caller guarantees the buffer is free.
 template <int F, int T, int BD>
-__global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, size_t ppitch,
-                                                   unsigned row_len, PeakParams pp, int trial0,
-                                                   int4* __restrict__ rec,
-                                                   unsigned* __restrict__ counter, unsigned cap)
+__device__ __forceinline__ void stage_tile(float* sm, uint64_t* bar, const float* __restrict__ row,
+                                           unsigned row_len, unsigned i0, unsigned tid)
 {
-    static_assert(T % 128 == 0 && BD % 32 == 0 && T % BD == 0, "tile shape");
-    extern __shared__ float4 smem4[];
-    __shared__ __align__(8) uint64_t bar;
-    float* sm = reinterpret_cast<float*>(smem4);
-    const int trial = trial0 + (int)blockIdx.y;
-    const float* __restrict__ row = p + (size_t)blockIdx.y * ppitch;
-    const unsigned tid = threadIdx.x;
-    const unsigned i0 = pp.lo + blockIdx.x * T;
-
-    // ---- stage the tile and every fraction's window: one thread issues
-    // the bulk copies, everyone waits on the mbarrier.  Parts of a window
-    // past the end of the row (only in the last tile) are zero-filled.
     if (tid == 0) {
-        mbar_init(&bar, 1);
-        mbar_init_fence();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        unsigned bytes = 0;
         unsigned lens[nfrac(F) + 1];
-        {
-            const unsigned ok = i0 < row_len ? min((unsigned)T, row_len - i0) : 0u;
-            lens[0] = ok;
-            bytes += 4u * ok;
-        }
+        unsigned bytes = 0;
+        lens[0] = i0 < row_len ? min((unsigned)T, row_len - i0) : 0u;
+        bytes += 4u * lens[0];
 #pragma unroll
         for (int q = 0; q < nfrac(F); ++q) {
             const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
@@ -259,20 +215,18 @@ __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, 
             const unsigned last = a + (unsigned)((((unsigned long long)(T - 1) * m) + (1u << (h - 1))) >> h);
             const unsigned a4 = a & ~3u;
             const unsigned n = ((last + 1 - a4) + 3u) & ~3u;
-            const unsigned ok = a4 < row_len ? min(n, row_len - a4) : 0u;
-            lens[q + 1] = ok;
-            bytes += 4u * ok;
+            lens[q + 1] = a4 < row_len ? min(n, row_len - a4) : 0u;
+            bytes += 4u * lens[q + 1];
         }
-        mbar_arrive_expect_tx(&bar, bytes);
-        if (lens[0]) bulk_g2s(sm, row + i0, 4u * lens[0], &bar);
+        mbar_arrive_expect_tx(bar, bytes);
+        if (lens[0]) bulk_g2s(sm, row + i0, 4u * lens[0], bar);
 #pragma unroll
         for (int q = 0; q < nfrac(F); ++q) {
             const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
             const unsigned a4 = (unsigned)(((unsigned long long)i0 * m) >> h) & ~3u;
-            if (lens[q + 1]) bulk_g2s(sm + slot_offset(q, T), row + a4, 4u * lens[q + 1], &bar);
+            if (lens[q + 1]) bulk_g2s(sm + slot_offset(q, T), row + a4, 4u * lens[q + 1], bar);
         }
     }
-    // zero-fill what lies past the row end (last tile only)
     if (i0 + T > row_len) {
         for (unsigned j = tid; j < (unsigned)T; j += BD)
             if (i0 + j >= row_len) sm[j] = 0.f;
@@ -284,32 +238,72 @@ __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, 
                 if (a4 + j >= row_len) sm[slot_offset(q, T) + j] = 0.f;
         }
     }
-    // Bounded wait; the give-up decision is made for the whole CTA at one
-    // barrier every thread reaches, so no thread is left waiting at a later
-    // barrier.  On failure the copies still in flight get a second bounded
-    // wait before the CTA leaves, and the host sees the error word.
-    const bool staged = mbar_wait_bounded(&bar, 0, 1u << 22);
-    if (!__syncthreads_and(staged)) {
-        if (!staged) mbar_wait_bounded(&bar, 0, 1u << 22);
-        if (tid == 0) atomicExch(counter + 1, kHarmStagingTimeout);
-        return;
-    }
+}
 
-    HarmThread<F, T, BD> c;
-    c.sm = sm;
-    c.i0 = i0;
-    c.tid = tid;
-    c.lane = tid & 31u;
-#pragma unroll
-    for (int q = 0; q < nfrac(F); ++q) {
-        const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-        const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
-        c.base[q] = (unsigned)slot_offset(q, T) + (a & 3u) + ((tid * m + (1u << (h - 1))) >> h);
+// Persistent CTA: work item w = (row, tile) taken round-robin; two shared
+// buffers form a ring so the TMA engine stages item w+1 while the threads
+// sum item w.
+template <int F, int T, int BD>
+__global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, size_t ppitch,
+                                                   unsigned row_len, PeakParams pp, int trial0,
+                                                   int rows, unsigned ntiles,
+                                                   int4* __restrict__ rec,
+                                                   unsigned* __restrict__ counter, unsigned cap)
+{
+    static_assert(T % 128 == 0 && BD % 32 == 0 && T % BD == 0, "tile shape");
+    constexpr int STAGE = harm_smem_floats(F, T);
+    extern __shared__ float4 smem4[];
+    __shared__ __align__(8) uint64_t bar[2];
+    float* smem = reinterpret_cast<float*>(smem4);
+    const unsigned tid = threadIdx.x;
+    const unsigned nitems = ntiles * (unsigned)rows;
+    unsigned w = blockIdx.x;
+    if (w >= nitems) return;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
     }
-    // ---- pass 1: sums and threshold test only
-    const bool any = harm_pass<F, T, BD, false>(c, pp, trial, rec, counter, cap);
-    // ---- pass 2 (rare): exact ranges and compaction
-    if (__syncthreads_or(any)) harm_pass<F, T, BD, true>(c, pp, trial, rec, counter, cap);
+    __syncthreads();
+    auto item_row = [&](unsigned it) { return it / ntiles; };
+    auto item_i0 = [&](unsigned it) { return pp.lo + (it % ntiles) * (unsigned)T; };
+    stage_tile<F, T, BD>(smem, &bar[0], p + (size_t)item_row(w) * ppitch, row_len, item_i0(w), tid);
+    unsigned phases = 0u;  // bit b: parity of the next completion of bar[b]
+    for (unsigned j = 0; w < nitems; ++j, w += gridDim.x) {
+        const unsigned cur = j & 1u;
+        const unsigned nxt = w + gridDim.x;
+        if (nxt < nitems)  // the other buffer was released at the end of the last item
+            stage_tile<F, T, BD>(smem + (cur ^ 1u) * STAGE, &bar[cur ^ 1u],
+                                 p + (size_t)item_row(nxt) * ppitch, row_len, item_i0(nxt), tid);
+        const unsigned ph = (phases >> cur) & 1u;
+        const bool staged = mbar_wait_bounded(&bar[cur], ph, 1u << 22);
+        phases ^= 1u << cur;
+        if (!__syncthreads_and(staged)) {
+            // copies still in flight get a second bounded wait, then leave
+            if (!staged) mbar_wait_bounded(&bar[cur], ph, 1u << 22);
+            if (nxt < nitems) mbar_wait_bounded(&bar[cur ^ 1u], (phases >> (cur ^ 1u)) & 1u, 1u << 22);
+            if (tid == 0) atomicExch(counter + 1, kHarmStagingTimeout);
+            return;
+        }
+        const float* sm = smem + cur * STAGE;
+        const unsigned i0 = item_i0(w);
+        const int trial = trial0 + (int)item_row(w);
+        unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
+#pragma unroll
+        for (int q = 0; q < nfrac(F); ++q) {
+            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
+            const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
+            base[q] = (unsigned)slot_offset(q, T) + (a & 3u) + ((tid * m + (1u << (h - 1))) >> h);
+        }
+        float val[T / BD];
+#pragma unroll
+        for (int k = 0; k < T / BD; ++k) {
+            val[k] = sm[tid + k * BD];
+            test_and_emit(val[k], pp, 0, i0 + tid + k * BD, trial, rec, counter, cap, tid & 31u);
+        }
+        FracStep<0, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
+        __syncthreads();  // buffer `cur` is free for item j+2
+    }
 }
 
 }  // namespace psx

@@ -98,26 +98,30 @@ __global__ void k_baseline_reset(unsigned* __restrict__ state)
 }
 
 // Fused harmonic sums + threshold + compaction: tile shape and launcher.
-constexpr int kHarmTile = 1024;
+// Persistent grid: kHarmCtasPerSm CTAs per SM (two 2^F-window stages of
+// shared memory each), looping over (trial, tile) items.
+constexpr int kHarmTile = 512;
 constexpr int kHarmThreads = 256;
+constexpr int kHarmCtasPerSm = 3;
 
 template <int F>
 static int launch_harm_f(const float* p, size_t ppitch, unsigned row_len, const PeakParams& pp,
                          int trial0, int rows, int4* rec, unsigned* counter, unsigned cap,
                          cudaStream_t s)
 {
-    constexpr size_t smem = sizeof(float) * harm_smem_floats(F, kHarmTile);
+    constexpr size_t smem = 2 * sizeof(float) * harm_smem_floats(F, kHarmTile);
     const unsigned ntiles = (pp.hi - pp.lo + kHarmTile - 1) / kHarmTile;
-    dim3 grid(ntiles, (unsigned)rows);
+    const unsigned items = ntiles * (unsigned)rows;
+    const unsigned grid = std::min(items, (unsigned)(sm_count() * kHarmCtasPerSm));
     k_harm_tiles<F, kHarmTile, kHarmThreads><<<grid, kHarmThreads, smem, s>>>(
-        p, ppitch, row_len, pp, trial0, rec, counter, cap);
+        p, ppitch, row_len, pp, trial0, rows, ntiles, rec, counter, cap);
     return launch_status("harmonic-sum kernel");
 }
 
 template <int F>
 static int configure_harm_f()
 {
-    constexpr size_t smem = sizeof(float) * harm_smem_floats(F, kHarmTile);
+    constexpr size_t smem = 2 * sizeof(float) * harm_smem_floats(F, kHarmTile);
     return cuda_status(cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmThreads>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                        "harmonic-sum kernel attribute");
