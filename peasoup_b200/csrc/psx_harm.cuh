@@ -150,15 +150,16 @@ template <> __device__ __forceinline__ float fold_scale<5>(float val) { return v
 
 // One warp-level threshold test: the range check and the append only run
 // in warps where some lane crossed the threshold (rare).
-__device__ __forceinline__ void test_and_emit(float s, const PeakParams& pp, int h, unsigned i,
+template <int H>
+__device__ __forceinline__ void test_and_emit(float s, const PeakParams& pp, unsigned i,
                                               int trial, int4* __restrict__ rec,
                                               unsigned* __restrict__ counter, unsigned cap,
                                               unsigned lane)
 {
     const bool over = s > pp.thresh;
     if (__any_sync(0xffffffffu, over)) {
-        const bool hit = over && (int)i >= pp.start[h] && (int)i < pp.end[h];
-        emit_hit(hit, trial, h, i, s, rec, counter, cap, lane);
+        const bool hit = over && (int)i >= pp.start[H] && (int)i < pp.end[H];
+        emit_hit(hit, trial, H, i, s, rec, counter, cap, lane);
     }
 }
 
@@ -180,8 +181,8 @@ struct FracStep {
         if (Q == fold_last(h)) {
 #pragma unroll
             for (int k = 0; k < T / BD; ++k)
-                test_and_emit(fold_scale<h>(val[k]), pp, h, i0 + tid + k * BD, trial, rec,
-                              counter, cap, tid & 31u);
+                test_and_emit<h>(fold_scale<h>(val[k]), pp, i0 + tid + k * BD, trial, rec,
+                                 counter, cap, tid & 31u);
         }
         FracStep<Q + 1, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
     }
@@ -196,55 +197,96 @@ struct FracStep<(1 << F) - 1, F, T, BD> {
     }
 };
 
-// Stage tile `i0` of `row` into the buffer `sm` (thread 0 issues the bulk
-// copies onto `bar`; everything past the row end is zero-filled by all
-// threads).  The caller guarantees the buffer is free.
+// Per-fraction copy parameters, indexed by lane (lane 0 = the tile):
+// numerator, log2 denominator and shared-memory offset of the slot.
+template <int T>
+struct WindowTable {
+    int m[32], h[32], off[32];
+    constexpr WindowTable() : m(), h(), off()
+    {
+        m[0] = 1;
+        h[0] = 0;
+        off[0] = 0;
+        for (int q = 0; q < 31; ++q) {
+            m[q + 1] = frac_m(q);
+            h[q + 1] = frac_h(q);
+            off[q + 1] = slot_offset(q, T);
+        }
+    }
+};
+
+// Stage item `i0` of `row` into the stage buffer `sm`: warp 0 issues one
+// bulk copy per lane (lane 0 the tile, lane q+1 fraction q) after lane 0
+// armed `bar` with the total byte count; parts past the row end are
+// zero-filled by all threads.  The caller guarantees the buffer is free.
 template <int F, int T, int BD>
-__device__ __forceinline__ void stage_tile(float* sm, uint64_t* bar, const float* __restrict__ row,
-                                           unsigned row_len, unsigned i0, unsigned tid)
+__device__ __forceinline__ void stage_item(float* sm, uint64_t* bar, const float* __restrict__ row,
+                                           unsigned row_len, unsigned i0, unsigned tid,
+                                           const WindowTable<T>& W)
 {
-    if (tid == 0) {
-        unsigned lens[nfrac(F) + 1];
-        unsigned bytes = 0;
-        lens[0] = i0 < row_len ? min((unsigned)T, row_len - i0) : 0u;
-        bytes += 4u * lens[0];
-#pragma unroll
-        for (int q = 0; q < nfrac(F); ++q) {
-            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-            const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
-            const unsigned last = a + (unsigned)((((unsigned long long)(T - 1) * m) + (1u << (h - 1))) >> h);
-            const unsigned a4 = a & ~3u;
-            const unsigned n = ((last + 1 - a4) + 3u) & ~3u;
-            lens[q + 1] = a4 < row_len ? min(n, row_len - a4) : 0u;
-            bytes += 4u * lens[q + 1];
+    constexpr int NW = nfrac(F) + 1;
+    if (tid < 32) {
+        const unsigned lane = tid;
+        unsigned a4 = 0, len = 0;
+        if (lane < (unsigned)NW) {
+            const unsigned m = (unsigned)W.m[lane], h = (unsigned)W.h[lane];
+            // i0 is a multiple of 128, so i0*m/2^h is a multiple of 4
+            a4 = (unsigned)(((unsigned long long)i0 * m) >> h);
+            const unsigned n = lane == 0 ? (unsigned)T
+                                         : (unsigned)(((((unsigned long long)(T - 1) * m) +
+                                                        (1u << (h - 1))) >> h) + 4u) & ~3u;
+            len = a4 < row_len ? min(n, row_len - a4) : 0u;
         }
-        mbar_arrive_expect_tx(bar, bytes);
-        if (lens[0]) bulk_g2s(sm, row + i0, 4u * lens[0], bar);
-#pragma unroll
-        for (int q = 0; q < nfrac(F); ++q) {
-            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-            const unsigned a4 = (unsigned)(((unsigned long long)i0 * m) >> h) & ~3u;
-            if (lens[q + 1]) bulk_g2s(sm + slot_offset(q, T), row + a4, 4u * lens[q + 1], bar);
-        }
+        const unsigned total = __reduce_add_sync(0xffffffffu, 4u * len);
+        if (lane == 0) mbar_arrive_expect_tx(bar, total);
+        __syncwarp();
+        if (len) bulk_g2s(sm + W.off[lane], row + a4, 4u * len, bar);
     }
     if (i0 + T > row_len) {
         for (unsigned j = tid; j < (unsigned)T; j += BD)
             if (i0 + j >= row_len) sm[j] = 0.f;
 #pragma unroll
         for (int q = 0; q < nfrac(F); ++q) {
-            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-            const unsigned a4 = (unsigned)(((unsigned long long)i0 * m) >> h) & ~3u;
+            const unsigned a4 =
+                (unsigned)(((unsigned long long)i0 * (unsigned)frac_m(q)) >> frac_h(q));
             for (unsigned j = tid; j < (unsigned)slot_floats(q, T); j += BD)
                 if (a4 + j >= row_len) sm[slot_offset(q, T) + j] = 0.f;
         }
     }
 }
 
-// Persistent CTA: work item w = (row, tile) taken round-robin; two shared
-// buffers form a ring so the TMA engine stages item w+1 while the threads
-// sum item w.
 template <int F, int T, int BD>
-__global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, size_t ppitch,
+__device__ __forceinline__ void sum_item(const float* __restrict__ sm,
+                                         const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                         unsigned i0, unsigned tid, const PeakParams& pp,
+                                         int trial, int4* __restrict__ rec,
+                                         unsigned* __restrict__ counter, unsigned cap)
+{
+    float val[T / BD];
+#pragma unroll
+    for (int k = 0; k < T / BD; ++k) {
+        val[k] = sm[tid + k * BD];
+        test_and_emit<0>(val[k], pp, i0 + tid + k * BD, trial, rec, counter, cap, tid & 31u);
+    }
+    FracStep<0, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
+}
+
+template <int T>
+struct WindowTables {
+    static __device__ const WindowTable<T>& get();
+};
+
+__constant__ WindowTable<512> kWindows512 = WindowTable<512>();
+__constant__ WindowTable<1024> kWindows1024 = WindowTable<1024>();
+template <> __device__ __forceinline__ const WindowTable<512>& WindowTables<512>::get() { return kWindows512; }
+template <> __device__ __forceinline__ const WindowTable<1024>& WindowTables<1024>::get() { return kWindows1024; }
+
+// Persistent CTA: work item w = (row, tile) taken round-robin; two stage
+// buffers form a ring so the TMA engine stages item w+grid while the
+// threads sum item w.  Items alternate between the stages, and the loop
+// is unrolled by two so each stage's base is a compile-time offset.
+template <int F, int T, int BD>
+__global__ void __launch_bounds__(BD, 3) k_harm_tiles(const float* __restrict__ p, size_t ppitch,
                                                    unsigned row_len, PeakParams pp, int trial0,
                                                    int rows, unsigned ntiles,
                                                    int4* __restrict__ rec,
@@ -255,6 +297,7 @@ __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, 
     extern __shared__ float4 smem4[];
     __shared__ __align__(8) uint64_t bar[2];
     float* smem = reinterpret_cast<float*>(smem4);
+    const WindowTable<T>& W = WindowTables<T>::get();
     const unsigned tid = threadIdx.x;
     const unsigned nitems = ntiles * (unsigned)rows;
     unsigned w = blockIdx.x;
@@ -264,46 +307,53 @@ __global__ void __launch_bounds__(BD) k_harm_tiles(const float* __restrict__ p, 
         mbar_init(&bar[1], 1);
         mbar_init_fence();
     }
-    __syncthreads();
-    auto item_row = [&](unsigned it) { return it / ntiles; };
-    auto item_i0 = [&](unsigned it) { return pp.lo + (it % ntiles) * (unsigned)T; };
-    stage_tile<F, T, BD>(smem, &bar[0], p + (size_t)item_row(w) * ppitch, row_len, item_i0(w), tid);
-    unsigned phases = 0u;  // bit b: parity of the next completion of bar[b]
-    for (unsigned j = 0; w < nitems; ++j, w += gridDim.x) {
-        const unsigned cur = j & 1u;
-        const unsigned nxt = w + gridDim.x;
-        if (nxt < nitems)  // the other buffer was released at the end of the last item
-            stage_tile<F, T, BD>(smem + (cur ^ 1u) * STAGE, &bar[cur ^ 1u],
-                                 p + (size_t)item_row(nxt) * ppitch, row_len, item_i0(nxt), tid);
-        const unsigned ph = (phases >> cur) & 1u;
-        const bool staged = mbar_wait_bounded(&bar[cur], ph, 1u << 22);
-        phases ^= 1u << cur;
-        if (!__syncthreads_and(staged)) {
-            // copies still in flight get a second bounded wait, then leave
-            if (!staged) mbar_wait_bounded(&bar[cur], ph, 1u << 22);
-            if (nxt < nitems) mbar_wait_bounded(&bar[cur ^ 1u], (phases >> (cur ^ 1u)) & 1u, 1u << 22);
-            if (tid == 0) atomicExch(counter + 1, kHarmStagingTimeout);
-            return;
-        }
-        const float* sm = smem + cur * STAGE;
-        const unsigned i0 = item_i0(w);
-        const int trial = trial0 + (int)item_row(w);
-        unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
+    // item-independent part of every fraction's shared-memory offset
+    unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
 #pragma unroll
-        for (int q = 0; q < nfrac(F); ++q) {
-            const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-            const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
-            base[q] = (unsigned)slot_offset(q, T) + (a & 3u) + ((tid * m + (1u << (h - 1))) >> h);
-        }
-        float val[T / BD];
-#pragma unroll
-        for (int k = 0; k < T / BD; ++k) {
-            val[k] = sm[tid + k * BD];
-            test_and_emit(val[k], pp, 0, i0 + tid + k * BD, trial, rec, counter, cap, tid & 31u);
-        }
-        FracStep<0, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
-        __syncthreads();  // buffer `cur` is free for item j+2
+    for (int q = 0; q < nfrac(F); ++q) {
+        const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
+        base[q] = (unsigned)slot_offset(q, T) + ((tid * m + (1u << (h - 1))) >> h);
     }
+    __syncthreads();
+    const unsigned lo = pp.lo;
+#define PSX_ROW(it) (p + (size_t)((it) / ntiles) * ppitch)
+#define PSX_I0(it) (lo + ((it) % ntiles) * (unsigned)T)
+    stage_item<F, T, BD>(smem, &bar[0], PSX_ROW(w), row_len, PSX_I0(w), tid, W);
+    unsigned ph0 = 0u, ph1 = 0u;
+    bool ok = true;
+    for (;;) {
+        // ---- item in stage 0
+        unsigned nxt = w + gridDim.x;
+        if (nxt < nitems)
+            stage_item<F, T, BD>(smem + STAGE, &bar[1], PSX_ROW(nxt), row_len, PSX_I0(nxt), tid, W);
+        if (!mbar_wait_bounded(&bar[0], ph0, 1u << 22)) {
+            ok = false;  // reported below; wait once more for the copies in flight
+            mbar_wait_bounded(&bar[0], ph0, 1u << 22);
+        }
+        ph0 ^= 1u;
+        sum_item<F, T, BD>(smem, base, PSX_I0(w), tid, pp, trial0 + (int)(w / ntiles), rec,
+                           counter, cap);
+        __syncthreads();  // stage 0 free
+        w = nxt;
+        if (w >= nitems) break;
+        // ---- item in stage 1
+        nxt = w + gridDim.x;
+        if (nxt < nitems)
+            stage_item<F, T, BD>(smem, &bar[0], PSX_ROW(nxt), row_len, PSX_I0(nxt), tid, W);
+        if (!mbar_wait_bounded(&bar[1], ph1, 1u << 22)) {
+            ok = false;  // reported below; wait once more for the copies in flight
+            mbar_wait_bounded(&bar[1], ph1, 1u << 22);
+        }
+        ph1 ^= 1u;
+        sum_item<F, T, BD>(smem + STAGE, base, PSX_I0(w), tid, pp, trial0 + (int)(w / ntiles),
+                           rec, counter, cap);
+        __syncthreads();  // stage 1 free
+        w = nxt;
+        if (w >= nitems) break;
+    }
+#undef PSX_ROW
+#undef PSX_I0
+    if (!ok && (tid & 31u) == 0) atomicExch(counter + 1, kHarmStagingTimeout);
 }
 
 }  // namespace psx
