@@ -34,8 +34,11 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", HOST_FLAGS,
 
 CU_SOURCES = ["psx_kernels.cu", "psx_fft.cu", "psx_search.cu"]
 CPP_SOURCES = ["psx_host.cpp"]
-HEADERS = ["psx_common.cuh", "psx_device.cuh", "psx_stages.cuh", "psx_fft.cuh",
-           "psx_fft_cb.h", "psx_host.h"]
+
+
+def _headers():
+    """Every header of csrc/ (any change rebuilds every object)."""
+    return sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 
 
 def _newer(target: str, deps) -> bool:
@@ -68,7 +71,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
     os.makedirs(BUILD, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "peasoup_b200.h")]
+    hdrs = [os.path.join(CSRC, h) for h in _headers()] + [os.path.join(INCLUDE, "peasoup_b200.h")]
 
     # 1. LTO callback for cuFFT, embedded as a byte array
     cb_src = os.path.join(CSRC, "psx_fft_cb.cu")
