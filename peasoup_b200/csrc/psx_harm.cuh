@@ -197,163 +197,143 @@ struct FracStep<(1 << F) - 1, F, T, BD> {
     }
 };
 
-// Per-fraction copy parameters, indexed by lane (lane 0 = the tile):
-// numerator, log2 denominator and shared-memory offset of the slot.
+// Copy parameters of window `lane` (0 = the tile, q+1 = fraction q):
+// numerator, log2 denominator and shared-memory offset, computed in
+// registers (no table) from the fold structure: fold h has 2^(h-1)
+// fractions; fold 2 lists 3/4 before 1/4, the other folds ascend.
 template <int T>
-struct WindowTable {
-    int m[32], h[32], off[32];
-    constexpr WindowTable() : m(), h(), off()
-    {
-        m[0] = 1;
-        h[0] = 0;
-        off[0] = 0;
-        for (int q = 0; q < 31; ++q) {
-            m[q + 1] = frac_m(q);
-            h[q + 1] = frac_h(q);
-            off[q + 1] = slot_offset(q, T);
-        }
-    }
-};
-
-// Stage item `i0` of `row` into the stage buffer `sm`: warp 0 issues one
-// bulk copy per lane (lane 0 the tile, lane q+1 fraction q) after lane 0
-// armed `bar` with the total byte count; parts past the row end are
-// zero-filled by all threads.  The caller guarantees the buffer is free.
-template <int F, int T, int BD>
-__device__ __forceinline__ void stage_item(float* sm, uint64_t* bar, const float* __restrict__ row,
-                                           unsigned row_len, unsigned i0, unsigned tid,
-                                           const WindowTable<T>& W)
+__device__ __forceinline__ void window_params(unsigned lane, unsigned& m, unsigned& h,
+                                              unsigned& off)
 {
-    constexpr int NW = nfrac(F) + 1;
-    if (tid < 32) {
-        const unsigned lane = tid;
-        unsigned a4 = 0, len = 0;
-        if (lane < (unsigned)NW) {
-            const unsigned m = (unsigned)W.m[lane], h = (unsigned)W.h[lane];
-            // i0 is a multiple of 128, so i0*m/2^h is a multiple of 4
-            a4 = (unsigned)(((unsigned long long)i0 * m) >> h);
-            const unsigned n = lane == 0 ? (unsigned)T
-                                         : (unsigned)(((((unsigned long long)(T - 1) * m) +
-                                                        (1u << (h - 1))) >> h) + 4u) & ~3u;
-            len = a4 < row_len ? min(n, row_len - a4) : 0u;
-        }
-        const unsigned total = __reduce_add_sync(0xffffffffu, 4u * len);
-        if (lane == 0) mbar_arrive_expect_tx(bar, total);
-        __syncwarp();
-        if (len) bulk_g2s(sm + W.off[lane], row + a4, 4u * len, bar);
+    if (lane == 0) {
+        m = 1;
+        h = 0;
+        off = 0;
+        return;
     }
-    if (i0 + T > row_len) {
-        for (unsigned j = tid; j < (unsigned)T; j += BD)
-            if (i0 + j >= row_len) sm[j] = 0.f;
-#pragma unroll
-        for (int q = 0; q < nfrac(F); ++q) {
-            const unsigned a4 =
-                (unsigned)(((unsigned long long)i0 * (unsigned)frac_m(q)) >> frac_h(q));
-            for (unsigned j = tid; j < (unsigned)slot_floats(q, T); j += BD)
-                if (a4 + j >= row_len) sm[slot_offset(q, T) + j] = 0.f;
-        }
-    }
+    const unsigned q = lane - 1;                 // fraction index
+    h = 32u - __clz(q + 1);                      // floor(log2(q+1)) + 1
+    const unsigned first = (1u << (h - 1)) - 1;  // first fraction of fold h
+    const unsigned r = q - first;                // position inside the fold
+    m = (h == 2) ? (r == 0 ? 3u : 1u) : 2u * r + 1u;
+    // slots of all earlier folds: sum over h' < h of (T*2^(h'-2) + 8*2^(h'-1))
+    off = (unsigned)T;
+    for (unsigned hh = 1; hh < h; ++hh) off += ((unsigned)T << hh >> 2) + (8u << (hh - 1));
+    // earlier fractions of this fold: numerators sum to r^2 (3 for fold 2's second)
+    const unsigned msum = (h == 2) ? (r == 0 ? 0u : 3u) : r * r;
+    off += (((unsigned)T * msum) >> h) + 8u * r;
 }
 
-template <int F, int T, int BD>
+template <int F, int T, int NC>
 __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
                                          const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
                                          unsigned i0, unsigned tid, const PeakParams& pp,
                                          int trial, int4* __restrict__ rec,
                                          unsigned* __restrict__ counter, unsigned cap)
 {
-    float val[T / BD];
+    float val[T / NC];
 #pragma unroll
-    for (int k = 0; k < T / BD; ++k) {
-        val[k] = sm[tid + k * BD];
-        test_and_emit<0>(val[k], pp, i0 + tid + k * BD, trial, rec, counter, cap, tid & 31u);
+    for (int k = 0; k < T / NC; ++k) {
+        val[k] = sm[tid + k * NC];
+        test_and_emit<0>(val[k], pp, i0 + tid + k * NC, trial, rec, counter, cap, tid & 31u);
     }
-    FracStep<0, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
+    FracStep<0, F, T, NC>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
 }
 
-template <int T>
-struct WindowTables {
-    static __device__ const WindowTable<T>& get();
-};
-
-__constant__ WindowTable<512> kWindows512 = WindowTable<512>();
-__constant__ WindowTable<1024> kWindows1024 = WindowTable<1024>();
-template <> __device__ __forceinline__ const WindowTable<512>& WindowTables<512>::get() { return kWindows512; }
-template <> __device__ __forceinline__ const WindowTable<1024>& WindowTables<1024>::get() { return kWindows1024; }
-
-// Persistent CTA: work item w = (row, tile) taken round-robin; two stage
-// buffers form a ring so the TMA engine stages item w+grid while the
-// threads sum item w.  Items alternate between the stages, and the loop
-// is unrolled by two so each stage's base is a compile-time offset.
-template <int F, int T, int BD>
-__global__ void __launch_bounds__(BD, 3) k_harm_tiles(const float* __restrict__ p, size_t ppitch,
-                                                   unsigned row_len, PeakParams pp, int trial0,
-                                                   int rows, unsigned ntiles,
-                                                   int4* __restrict__ rec,
-                                                   unsigned* __restrict__ counter, unsigned cap)
+// Persistent, warp-specialised CTA: warp 0 produces (bulk copies of item
+// w into stage w%S once the consumers released it), warps 1..NC/32
+// consume (sum, test, append), S stages in a ring.  Work items w = (row,
+// tile) are taken round-robin over the grid.  full[s] completes when a
+// stage's bytes have landed; empty[s] when every consumer warp has
+// finished with it.  No CTA-wide barrier is used inside the loop; every
+// wait is bounded and a timeout is reported in counter[1].
+template <int F, int T, int NC, int S>
+__global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restrict__ p,
+                                                           size_t ppitch, unsigned row_len,
+                                                           PeakParams pp, int trial0, int rows,
+                                                           unsigned ntiles,
+                                                           int4* __restrict__ rec,
+                                                           unsigned* __restrict__ counter,
+                                                           unsigned cap)
 {
-    static_assert(T % 128 == 0 && BD % 32 == 0 && T % BD == 0, "tile shape");
+    static_assert(T % 128 == 0 && NC % 32 == 0 && T % NC == 0, "tile shape");
     constexpr int STAGE = harm_smem_floats(F, T);
+    constexpr int NW = nfrac(F) + 1;  // windows (tile + fractions)
+    constexpr unsigned kLimit = 1u << 22;
     extern __shared__ float4 smem4[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t full[S], empty[S];
     float* smem = reinterpret_cast<float*>(smem4);
-    const WindowTable<T>& W = WindowTables<T>::get();
-    const unsigned tid = threadIdx.x;
     const unsigned nitems = ntiles * (unsigned)rows;
-    unsigned w = blockIdx.x;
-    if (w >= nitems) return;
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+    if (blockIdx.x >= nitems) return;
+    const unsigned warp = threadIdx.x / 32, lane = threadIdx.x & 31u;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NC / 32);
+        }
         mbar_init_fence();
     }
-    // item-independent part of every fraction's shared-memory offset
-    unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
-#pragma unroll
-    for (int q = 0; q < nfrac(F); ++q) {
-        const unsigned h = (unsigned)frac_h(q), m = (unsigned)frac_m(q);
-        base[q] = (unsigned)slot_offset(q, T) + ((tid * m + (1u << (h - 1))) >> h);
-    }
     __syncthreads();
-    const unsigned lo = pp.lo;
-#define PSX_ROW(it) (p + (size_t)((it) / ntiles) * ppitch)
-#define PSX_I0(it) (lo + ((it) % ntiles) * (unsigned)T)
-    stage_item<F, T, BD>(smem, &bar[0], PSX_ROW(w), row_len, PSX_I0(w), tid, W);
-    unsigned ph0 = 0u, ph1 = 0u;
     bool ok = true;
-    for (;;) {
-        // ---- item in stage 0
-        unsigned nxt = w + gridDim.x;
-        if (nxt < nitems)
-            stage_item<F, T, BD>(smem + STAGE, &bar[1], PSX_ROW(nxt), row_len, PSX_I0(nxt), tid, W);
-        if (!mbar_wait_bounded(&bar[0], ph0, 1u << 22)) {
-            ok = false;  // reported below; wait once more for the copies in flight
-            mbar_wait_bounded(&bar[0], ph0, 1u << 22);
+    if (warp == 0) {
+        // ---------------- producer
+        unsigned m = 0, h = 0, off = 0;
+        window_params<T>(lane, m, h, off);
+        unsigned j = 0;
+        for (unsigned w = blockIdx.x; w < nitems; w += gridDim.x, ++j) {
+            const unsigned s = j % S;
+            if (j >= (unsigned)S) {  // wait until the consumers released stage s
+                const unsigned ph = ((j / S) - 1) & 1u;
+                if (!mbar_wait_bounded(&empty[s], ph, kLimit)) ok = false;
+            }
+            float* sm = smem + s * STAGE;
+            const float* row = p + (size_t)(w / ntiles) * ppitch;
+            const unsigned i0 = pp.lo + (w % ntiles) * (unsigned)T;
+            unsigned a4 = 0, len = 0;
+            if (lane < (unsigned)NW) {
+                // i0 is a multiple of 128, so i0*m/2^h is a multiple of 4
+                a4 = (unsigned)(((unsigned long long)i0 * m) >> h);
+                const unsigned n =
+                    lane == 0 ? (unsigned)T
+                              : ((unsigned)((((unsigned long long)(T - 1) * m) + (1u << (h - 1))) >> h) + 4u) & ~3u;
+                len = a4 < row_len ? min(n, row_len - a4) : 0u;
+                // past the row end (last tile only): zero-fill this window's slot
+                if (a4 + (lane == 0 ? (unsigned)T : n) > row_len)
+                    for (unsigned k = len; k < (lane == 0 ? (unsigned)T : n); ++k) sm[off + k] = 0.f;
+            }
+            const unsigned total = __reduce_add_sync(0xffffffffu, 4u * len);
+            __syncwarp();
+            if (lane == 0) mbar_arrive_expect_tx(&full[s], total);
+            __syncwarp();
+            if (len) bulk_g2s(sm + off, row + a4, 4u * len, &full[s]);
         }
-        ph0 ^= 1u;
-        sum_item<F, T, BD>(smem, base, PSX_I0(w), tid, pp, trial0 + (int)(w / ntiles), rec,
-                           counter, cap);
-        __syncthreads();  // stage 0 free
-        w = nxt;
-        if (w >= nitems) break;
-        // ---- item in stage 1
-        nxt = w + gridDim.x;
-        if (nxt < nitems)
-            stage_item<F, T, BD>(smem, &bar[0], PSX_ROW(nxt), row_len, PSX_I0(nxt), tid, W);
-        if (!mbar_wait_bounded(&bar[1], ph1, 1u << 22)) {
-            ok = false;  // reported below; wait once more for the copies in flight
-            mbar_wait_bounded(&bar[1], ph1, 1u << 22);
+        // the consumers wait for every stage they use; nothing is left in
+        // flight once they are done, so the producer simply ends here
+    } else {
+        // ---------------- consumers
+        const unsigned tid = threadIdx.x - 32;
+        unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
+#pragma unroll
+        for (int q = 0; q < nfrac(F); ++q) {
+            const unsigned hh = (unsigned)frac_h(q), mm = (unsigned)frac_m(q);
+            base[q] = (unsigned)slot_offset(q, T) + ((tid * mm + (1u << (hh - 1))) >> hh);
         }
-        ph1 ^= 1u;
-        sum_item<F, T, BD>(smem + STAGE, base, PSX_I0(w), tid, pp, trial0 + (int)(w / ntiles),
-                           rec, counter, cap);
-        __syncthreads();  // stage 1 free
-        w = nxt;
-        if (w >= nitems) break;
+        unsigned j = 0;
+        for (unsigned w = blockIdx.x; w < nitems; w += gridDim.x, ++j) {
+            const unsigned s = j % S;
+            const unsigned ph = (j / S) & 1u;
+            if (!mbar_wait_bounded(&full[s], ph, kLimit)) {
+                ok = false;
+                mbar_wait_bounded(&full[s], ph, kLimit);  // let the copies land
+            }
+            const unsigned i0 = pp.lo + (w % ntiles) * (unsigned)T;
+            sum_item<F, T, NC>(smem + s * STAGE, base, i0, tid, pp, trial0 + (int)(w / ntiles),
+                               rec, counter, cap);
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
+        }
     }
-#undef PSX_ROW
-#undef PSX_I0
-    if (!ok && (tid & 31u) == 0) atomicExch(counter + 1, kHarmStagingTimeout);
+    if (!ok && lane == 0) atomicExch(counter + 1, kHarmStagingTimeout);
 }
 
 }  // namespace psx

@@ -98,33 +98,40 @@ __global__ void k_baseline_reset(unsigned* __restrict__ state)
 }
 
 // Fused harmonic sums + threshold + compaction: tile shape and launcher.
-// Persistent grid: kHarmCtasPerSm CTAs per SM (two 2^F-window stages of
-// shared memory each), looping over (trial, tile) items.
+// Persistent grid of kHarmCtasPerSm CTAs per SM, each one producer warp
+// plus kHarmConsumers consumer threads and kHarmStages shared stages.
 constexpr int kHarmTile = 512;
-constexpr int kHarmThreads = 256;
+constexpr int kHarmConsumers = 256;
+constexpr int kHarmStages = 2;
 constexpr int kHarmCtasPerSm = 3;
+
+template <int F>
+constexpr size_t harm_smem_bytes()
+{
+    return (size_t)kHarmStages * sizeof(float) * harm_smem_floats(F, kHarmTile);
+}
 
 template <int F>
 static int launch_harm_f(const float* p, size_t ppitch, unsigned row_len, const PeakParams& pp,
                          int trial0, int rows, int4* rec, unsigned* counter, unsigned cap,
                          cudaStream_t s)
 {
-    constexpr size_t smem = 2 * sizeof(float) * harm_smem_floats(F, kHarmTile);
     const unsigned ntiles = (pp.hi - pp.lo + kHarmTile - 1) / kHarmTile;
     const unsigned items = ntiles * (unsigned)rows;
     const unsigned grid = std::min(items, (unsigned)(sm_count() * kHarmCtasPerSm));
-    k_harm_tiles<F, kHarmTile, kHarmThreads><<<grid, kHarmThreads, smem, s>>>(
-        p, ppitch, row_len, pp, trial0, rows, ntiles, rec, counter, cap);
+    k_harm_tiles<F, kHarmTile, kHarmConsumers, kHarmStages>
+        <<<grid, kHarmConsumers + 32, harm_smem_bytes<F>(), s>>>(p, ppitch, row_len, pp, trial0,
+                                                                 rows, ntiles, rec, counter, cap);
     return launch_status("harmonic-sum kernel");
 }
 
 template <int F>
 static int configure_harm_f()
 {
-    constexpr size_t smem = 2 * sizeof(float) * harm_smem_floats(F, kHarmTile);
-    return cuda_status(cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmThreads>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                       "harmonic-sum kernel attribute");
+    return cuda_status(
+        cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmConsumers, kHarmStages>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)harm_smem_bytes<F>()),
+        "harmonic-sum kernel attribute");
 }
 
 // Opts the kernel for F folds into its dynamic shared memory (once per
