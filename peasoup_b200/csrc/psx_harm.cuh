@@ -138,60 +138,67 @@ __device__ __forceinline__ void emit_hit(bool hit, int trial, int fold, unsigned
     }
 }
 
-template <int F>
-__device__ __forceinline__ float fold_scale(float val);
-// The reference scales the running float sum by a double factor and
-// stores the float-rounded product (src/kernels.cu:46, 53, 62, 75, 96).
-template <> __device__ __forceinline__ float fold_scale<1>(float val) { return val * rsqrt(2.0); }
-template <> __device__ __forceinline__ float fold_scale<2>(float val) { return val * 0.5; }
-template <> __device__ __forceinline__ float fold_scale<3>(float val) { return val * rsqrt(8.0); }
-template <> __device__ __forceinline__ float fold_scale<4>(float val) { return val * 0.25; }
-template <> __device__ __forceinline__ float fold_scale<5>(float val) { return val * rsqrt(32.0); }
+// Fold scales: the reference multiplies the running float sum by a double
+// factor and stores the float-rounded product (src/kernels.cu:46, 53, 62,
+// 75, 96).  For the factors 1/2 and 1/4 the double product is exact, so
+// the float product x*0.5f / x*0.25f is the same correctly rounded value;
+// the other three use the double factors rsqrt(2.0), rsqrt(8.0) and
+// rsqrt(32.0), evaluated once per thread by the same function calls.
+struct FoldScales {
+    double r2, r8, r32;
+    __device__ __forceinline__ FoldScales() : r2(rsqrt(2.0)), r8(rsqrt(8.0)), r32(rsqrt(32.0)) {}
+};
 
-// One warp-level threshold test: the range check and the append only run
-// in warps where some lane crossed the threshold (rare).
 template <int H>
-__device__ __forceinline__ void test_and_emit(float s, const PeakParams& pp, unsigned i,
-                                              int trial, int4* __restrict__ rec,
-                                              unsigned* __restrict__ counter, unsigned cap,
-                                              unsigned lane)
-{
-    const bool over = s > pp.thresh;
-    if (__any_sync(0xffffffffu, over)) {
-        const bool hit = over && (int)i >= pp.start[H] && (int)i < pp.end[H];
-        emit_hit(hit, trial, H, i, s, rec, counter, cap, lane);
-    }
-}
+__device__ __forceinline__ float fold_scale(float val, const FoldScales& c);
+template <> __device__ __forceinline__ float fold_scale<1>(float val, const FoldScales& c) { return val * c.r2; }
+template <> __device__ __forceinline__ float fold_scale<2>(float val, const FoldScales&) { return val * 0.5f; }
+template <> __device__ __forceinline__ float fold_scale<3>(float val, const FoldScales& c) { return val * c.r8; }
+template <> __device__ __forceinline__ float fold_scale<4>(float val, const FoldScales&) { return val * 0.25f; }
+template <> __device__ __forceinline__ float fold_scale<5>(float val, const FoldScales& c) { return val * c.r32; }
 
-// Adds fraction Q to every output of the thread (K = T/BD outputs, BD
-// apart), tests and emits at fold boundaries, recurses to Q+1.
-template <int Q, int F, int T, int BD>
+// Adds fraction Q to every output of the thread (K = T/NC outputs, NC
+// apart).  At a fold boundary: in the fast pass (EMIT false) the fold value
+// only raises the running maximum `mx`; in the exact pass (EMIT true) the
+// fold's search range is applied and hits are appended with one atomic
+// per warp.  Recurses to Q+1.
+template <int Q, int F, int T, int NC, bool EMIT>
 struct FracStep {
     static __device__ __forceinline__ void run(const float* __restrict__ sm,
                                                const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                               float (&val)[T / BD], unsigned i0, unsigned tid,
+                                               float (&val)[T / NC], float (&mx)[T / NC],
+                                               const FoldScales& fs, unsigned i0, unsigned tid,
                                                const PeakParams& pp, int trial,
                                                int4* __restrict__ rec,
                                                unsigned* __restrict__ counter, unsigned cap)
     {
         constexpr int h = frac_h(Q), m = frac_m(Q);
-        constexpr int step = (BD * m) >> h;  // exact: BD is a multiple of 32
+        constexpr int step = (NC * m) >> h;  // exact: NC is a multiple of 32
 #pragma unroll
-        for (int k = 0; k < T / BD; ++k) val[k] += sm[base[Q] + k * step];
+        for (int k = 0; k < T / NC; ++k) val[k] += sm[base[Q] + k * step];
         if (Q == fold_last(h)) {
 #pragma unroll
-            for (int k = 0; k < T / BD; ++k)
-                test_and_emit<h>(fold_scale<h>(val[k]), pp, i0 + tid + k * BD, trial, rec,
-                                 counter, cap, tid & 31u);
+            for (int k = 0; k < T / NC; ++k) {
+                const float s = fold_scale<h>(val[k], fs);
+                if (EMIT) {
+                    const unsigned i = i0 + tid + k * NC;
+                    const bool hit = s > pp.thresh && (int)i >= pp.start[h] && (int)i < pp.end[h];
+                    emit_hit(hit, trial, h, i, s, rec, counter, cap, tid & 31u);
+                } else {
+                    mx[k] = fmaxf(mx[k], s);
+                }
+            }
         }
-        FracStep<Q + 1, F, T, BD>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
+        FracStep<Q + 1, F, T, NC, EMIT>::run(sm, base, val, mx, fs, i0, tid, pp, trial, rec,
+                                             counter, cap);
     }
 };
 
-template <int F, int T, int BD>
-struct FracStep<(1 << F) - 1, F, T, BD> {
+template <int F, int T, int NC, bool EMIT>
+struct FracStep<(1 << F) - 1, F, T, NC, EMIT> {
     static __device__ __forceinline__ void run(const float*, const unsigned (&)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                               float (&)[T / BD], unsigned, unsigned,
+                                               float (&)[T / NC], float (&)[T / NC],
+                                               const FoldScales&, unsigned, unsigned,
                                                const PeakParams&, int, int4*, unsigned*, unsigned)
     {
     }
@@ -224,30 +231,60 @@ __device__ __forceinline__ void window_params(unsigned lane, unsigned& m, unsign
     off += (((unsigned)T * msum) >> h) + 8u * r;
 }
 
+// The exact pass of one item (rare: only warps where some output crosses
+// the threshold): every fold's value again, its search range, and the
+// appends.  Kept out of line so the fast pass's registers are not shared
+// with it.
 template <int F, int T, int NC>
-__device__ __forceinline__ void sum_item(const float* __restrict__ sm,
-                                         const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                         unsigned i0, unsigned tid, const PeakParams& pp,
-                                         int trial, int4* __restrict__ rec,
-                                         unsigned* __restrict__ counter, unsigned cap)
+__device__ __noinline__ void exact_pass(const float* __restrict__ sm,
+                                        const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                        const FoldScales& fs, unsigned i0, unsigned tid,
+                                        const PeakParams& pp, int trial, int4* __restrict__ rec,
+                                        unsigned* __restrict__ counter, unsigned cap)
 {
-    float val[T / NC];
+    float val[T / NC], mx[T / NC];
 #pragma unroll
     for (int k = 0; k < T / NC; ++k) {
         val[k] = sm[tid + k * NC];
-        test_and_emit<0>(val[k], pp, i0 + tid + k * NC, trial, rec, counter, cap, tid & 31u);
+        const unsigned i = i0 + tid + k * NC;
+        const bool hit = val[k] > pp.thresh && (int)i >= pp.start[0] && (int)i < pp.end[0];
+        emit_hit(hit, trial, 0, i, val[k], rec, counter, cap, tid & 31u);
     }
-    FracStep<0, F, T, NC>::run(sm, base, val, i0, tid, pp, trial, rec, counter, cap);
+    FracStep<0, F, T, NC, true>::run(sm, base, val, mx, fs, i0, tid, pp, trial, rec, counter, cap);
+}
+
+// Sums one staged item: a fast pass that tracks each output's largest
+// fold value, then -- only in warps where some output crosses the
+// threshold -- the exact pass.
+template <int F, int T, int NC>
+__device__ __forceinline__ void sum_item(const float* __restrict__ sm,
+                                         const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                         const FoldScales& fs, unsigned i0, unsigned tid,
+                                         const PeakParams& pp, int trial, int4* __restrict__ rec,
+                                         unsigned* __restrict__ counter, unsigned cap)
+{
+    float val[T / NC], mx[T / NC];
+#pragma unroll
+    for (int k = 0; k < T / NC; ++k) {
+        val[k] = sm[tid + k * NC];
+        mx[k] = val[k];
+    }
+    FracStep<0, F, T, NC, false>::run(sm, base, val, mx, fs, i0, tid, pp, trial, rec, counter, cap);
+    bool over = false;
+#pragma unroll
+    for (int k = 0; k < T / NC; ++k) over |= mx[k] > pp.thresh;
+    if (__any_sync(0xffffffffu, over))
+        exact_pass<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
 }
 
 // Persistent, warp-specialised CTA: warp 0 produces (bulk copies of item
-// w into stage w%S once the consumers released it), warps 1..NC/32
-// consume (sum, test, append), S stages in a ring.  Work items w = (row,
-// tile) are taken round-robin over the grid.  full[s] completes when a
-// stage's bytes have landed; empty[s] when every consumer warp has
-// finished with it.  No CTA-wide barrier is used inside the loop; every
-// wait is bounded and a timeout is reported in counter[1].
-template <int F, int T, int NC, int S>
+// w into stage w%2 once the consumers released it), the other NC/32 warps
+// consume (sum, test, append); two stages form a ring.  Work items
+// (row, tile) are taken round-robin over the grid.  full[s] completes when
+// a stage's bytes have landed, empty[s] when every consumer warp is done
+// with it.  No CTA-wide barrier is used in the loop; every wait is bounded
+// and a timeout is reported in counter[1].
+template <int F, int T, int NC>
 __global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restrict__ p,
                                                            size_t ppitch, unsigned row_len,
                                                            PeakParams pp, int trial0, int rows,
@@ -261,13 +298,13 @@ __global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restri
     constexpr int NW = nfrac(F) + 1;  // windows (tile + fractions)
     constexpr unsigned kLimit = 1u << 22;
     extern __shared__ float4 smem4[];
-    __shared__ __align__(8) uint64_t full[S], empty[S];
+    __shared__ __align__(8) uint64_t full[2], empty[2];
     float* smem = reinterpret_cast<float*>(smem4);
     const unsigned nitems = ntiles * (unsigned)rows;
     if (blockIdx.x >= nitems) return;
     const unsigned warp = threadIdx.x / 32, lane = threadIdx.x & 31u;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
+        for (int s = 0; s < 2; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], NC / 32);
         }
@@ -275,20 +312,29 @@ __global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restri
     }
     __syncthreads();
     bool ok = true;
+    // the item sequence of this CTA as (row, tile), advanced without division
+    unsigned row = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+    const unsigned gstep_row = gridDim.x / ntiles, gstep_tile = gridDim.x % ntiles;
+    auto advance = [&]() {
+        row += gstep_row;
+        tile += gstep_tile;
+        if (tile >= ntiles) {
+            tile -= ntiles;
+            ++row;
+        }
+    };
     if (warp == 0) {
         // ---------------- producer
         unsigned m = 0, h = 0, off = 0;
         window_params<T>(lane, m, h, off);
-        unsigned j = 0;
-        for (unsigned w = blockIdx.x; w < nitems; w += gridDim.x, ++j) {
-            const unsigned s = j % S;
-            if (j >= (unsigned)S) {  // wait until the consumers released stage s
-                const unsigned ph = ((j / S) - 1) & 1u;
-                if (!mbar_wait_bounded(&empty[s], ph, kLimit)) ok = false;
+        for (unsigned j = 0; row < (unsigned)rows; ++j, advance()) {
+            const unsigned s = j & 1u;
+            if (j >= 2) {  // wait until the consumers released stage s
+                if (!mbar_wait_bounded(&empty[s], ((j >> 1) - 1) & 1u, kLimit)) ok = false;
             }
             float* sm = smem + s * STAGE;
-            const float* row = p + (size_t)(w / ntiles) * ppitch;
-            const unsigned i0 = pp.lo + (w % ntiles) * (unsigned)T;
+            const float* src = p + (size_t)row * ppitch;
+            const unsigned i0 = pp.lo + tile * (unsigned)T;
             unsigned a4 = 0, len = 0;
             if (lane < (unsigned)NW) {
                 // i0 is a multiple of 128, so i0*m/2^h is a multiple of 4
@@ -297,40 +343,44 @@ __global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restri
                     lane == 0 ? (unsigned)T
                               : ((unsigned)((((unsigned long long)(T - 1) * m) + (1u << (h - 1))) >> h) + 4u) & ~3u;
                 len = a4 < row_len ? min(n, row_len - a4) : 0u;
-                // past the row end (last tile only): zero-fill this window's slot
-                if (a4 + (lane == 0 ? (unsigned)T : n) > row_len)
-                    for (unsigned k = len; k < (lane == 0 ? (unsigned)T : n); ++k) sm[off + k] = 0.f;
+                // past the row end (last tile only): zero-fill the rest of the slot
+                for (unsigned k = len; k < n; ++k) sm[off + k] = 0.f;
             }
             const unsigned total = __reduce_add_sync(0xffffffffu, 4u * len);
             __syncwarp();
             if (lane == 0) mbar_arrive_expect_tx(&full[s], total);
             __syncwarp();
-            if (len) bulk_g2s(sm + off, row + a4, 4u * len, &full[s]);
+            if (len) bulk_g2s(sm + off, src + a4, 4u * len, &full[s]);
         }
-        // the consumers wait for every stage they use; nothing is left in
-        // flight once they are done, so the producer simply ends here
     } else {
         // ---------------- consumers
         const unsigned tid = threadIdx.x - 32;
+        const FoldScales fs;
         unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
 #pragma unroll
         for (int q = 0; q < nfrac(F); ++q) {
             const unsigned hh = (unsigned)frac_h(q), mm = (unsigned)frac_m(q);
             base[q] = (unsigned)slot_offset(q, T) + ((tid * mm + (1u << (hh - 1))) >> hh);
         }
-        unsigned j = 0;
-        for (unsigned w = blockIdx.x; w < nitems; w += gridDim.x, ++j) {
-            const unsigned s = j % S;
-            const unsigned ph = (j / S) & 1u;
-            if (!mbar_wait_bounded(&full[s], ph, kLimit)) {
-                ok = false;
-                mbar_wait_bounded(&full[s], ph, kLimit);  // let the copies land
+        unsigned ph = 0;
+        for (;;) {
+#pragma unroll
+            for (unsigned s = 0; s < 2; ++s) {  // s is a compile-time stage index
+                if (row >= (unsigned)rows) break;
+                if (!mbar_wait_bounded(&full[s], ph, kLimit)) {
+                    ok = false;
+                    mbar_wait_bounded(&full[s], ph, kLimit);  // let the copies land
+                }
+                sum_item<F, T, NC>(smem + s * STAGE, base, fs, pp.lo + tile * (unsigned)T, tid,
+                                   pp, trial0 + (int)row, rec, counter, cap);
+                __syncwarp();
+                if (lane == 0)
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s]))
+                                 : "memory");
+                advance();
             }
-            const unsigned i0 = pp.lo + (w % ntiles) * (unsigned)T;
-            sum_item<F, T, NC>(smem + s * STAGE, base, i0, tid, pp, trial0 + (int)(w / ntiles),
-                               rec, counter, cap);
-            __syncwarp();
-            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s])) : "memory");
+            if (row >= (unsigned)rows) break;
+            ph ^= 1u;
         }
     }
     if (!ok && lane == 0) atomicExch(counter + 1, kHarmStagingTimeout);

@@ -101,7 +101,7 @@ __global__ void k_baseline_reset(unsigned* __restrict__ state)
 // Persistent grid of kHarmCtasPerSm CTAs per SM, each one producer warp
 // plus kHarmConsumers consumer threads and kHarmStages shared stages.
 constexpr int kHarmTile = 512;
-constexpr int kHarmConsumers = 256;
+constexpr int kHarmConsumers = 128;
 constexpr int kHarmStages = 2;
 constexpr int kHarmCtasPerSm = 3;
 
@@ -119,7 +119,7 @@ static int launch_harm_f(const float* p, size_t ppitch, unsigned row_len, const 
     const unsigned ntiles = (pp.hi - pp.lo + kHarmTile - 1) / kHarmTile;
     const unsigned items = ntiles * (unsigned)rows;
     const unsigned grid = std::min(items, (unsigned)(sm_count() * kHarmCtasPerSm));
-    k_harm_tiles<F, kHarmTile, kHarmConsumers, kHarmStages>
+    k_harm_tiles<F, kHarmTile, kHarmConsumers>
         <<<grid, kHarmConsumers + 32, harm_smem_bytes<F>(), s>>>(p, ppitch, row_len, pp, trial0,
                                                                  rows, ntiles, rec, counter, cap);
     return launch_status("harmonic-sum kernel");
@@ -129,7 +129,7 @@ template <int F>
 static int configure_harm_f()
 {
     return cuda_status(
-        cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmConsumers, kHarmStages>,
+        cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmConsumers>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)harm_smem_bytes<F>()),
         "harmonic-sum kernel attribute");
 }
