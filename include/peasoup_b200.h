@@ -174,6 +174,22 @@ int psx_find_peaks(const float* d_spec, int n, int start, float thresh,
                    int* d_idx, float* d_val, int cap, int* h_count,
                    psx_stream_t stream);
 
+/* psx_find_peaks without any device allocation; no counterpart in the
+   reference.  For callers that may not allocate GPU memory during a run
+   (the device's memory is owned by their own pool or another framework,
+   or allocation after start-up is forbidden so that memory use stays
+   fixed).  Same arguments, results and errors as psx_find_peaks; the
+   per-tile counts live in a 256 KiB array compiled into the library,
+   which every GPU that loads the library holds until exit.  Limit:
+   n - start <= 2^28 bins; larger requests fail with PSX_ERR_INVALID.
+   The first call on each device looks up the array's device address with
+   that device current; make that first call before any stream capture.
+   All calls share the array: calls whose GPU work overlaps (different
+   streams or host threads) race and give wrong results. */
+int psx_find_peaks_noalloc(const float* d_spec, int n, int start, float thresh,
+                           int* d_idx, float* d_val, int cap, int* h_count,
+                           psx_stream_t stream);
+
 /* ------------------------------------------------------------------ */
 /* Real transforms (cuFFT)                                             */
 /* ------------------------------------------------------------------ */

@@ -105,6 +105,7 @@ SIGNATURES = {
     "psx_convert_i8_f32": (_i, [_vp, _vp, _sz, _vp]),
     "psx_harmonic_sum": (_i, [_vp, _vp, _sz, _i, _vp]),
     "psx_find_peaks": (_i, [_vp, _i, _i, _f, _vp, _vp, _i, C.POINTER(_i), _vp]),
+    "psx_find_peaks_noalloc": (_i, [_vp, _i, _i, _f, _vp, _vp, _i, C.POINTER(_i), _vp]),
     "psx_fft_plan_create": (_i, [C.POINTER(_vp), _sz, C.c_longlong, _i]),
     "psx_fft_exec": (_i, [_vp, _vp, _vp, _vp]),
     "psx_fft_plan_destroy": (_i, [_vp]),

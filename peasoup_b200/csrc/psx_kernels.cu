@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -948,3 +949,105 @@ int psx_find_peaks(const float* d_spec, int n, int start, float thresh, int* d_i
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- peak finding, no allocation
+// psx_find_peaks_noalloc runs the three compaction kernels of psx_find_peaks
+// with their per-tile counts in a fixed device array instead of memory from
+// cudaMallocAsync.  It serves callers that may not allocate device memory
+// while they search: hosts that have handed the whole of a GPU's memory to
+// their own pool or to another framework, hosts that forbid allocation
+// after start-up so that memory use cannot grow during a run, and code
+// running where an allocation could block or fail at a bad moment.
+//
+// The array g_peak_tile_scratch is compiled into this library: every GPU
+// that loads the library holds its 256 KiB (+ 4 bytes) until the process
+// exits.  It has room for kNoAllocMaxTiles tile counts plus the total, so a
+// call may scan at most kNoAllocMaxTiles * kCompactTile = 2^28 bins
+// (n - start).  All calls on a device share the one array and it keeps the
+// last call's contents; nothing in it needs to start at zero, because
+// k_compact_count writes every tile count a call uses before k_compact_scan
+// reads it.  Calls whose GPU work overlaps (other streams, other host
+// threads) race on the array and give wrong results.
+namespace psx {
+namespace {
+
+constexpr int kNoAllocMaxTiles = 65536;
+constexpr long long kNoAllocMaxBins = (long long)kNoAllocMaxTiles * kCompactTile;
+constexpr int kNoAllocMaxDevices = 64;
+
+// Device-side storage.  In host code this name is only a handle for the
+// runtime's symbol lookup, never a pointer that can be dereferenced or
+// passed to a kernel.
+static __device__ __align__(256) int g_peak_tile_scratch[kNoAllocMaxTiles + 1];
+
+std::mutex g_peak_scratch_mu;
+int* g_peak_scratch_addr[kNoAllocMaxDevices] = {nullptr};
+
+// The device address of g_peak_tile_scratch on the current device, looked
+// up once per device (the first call on each device does it, with that
+// device current) and cached.
+int peak_scratch_address(int** out)
+{
+    int dev = -1;
+    PSX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("find_peaks_noalloc: device ordinal %d outside 0..%d", dev,
+                  kNoAllocMaxDevices - 1);
+        return PSX_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_peak_scratch_mu);
+    if (!g_peak_scratch_addr[dev]) {
+        void* p = nullptr;
+        PSX_CUDA(cudaGetSymbolAddress(&p, g_peak_tile_scratch));
+        if (!p) {
+            set_error("find_peaks_noalloc: no device address for the scratch array");
+            return PSX_ERR_CUDA;
+        }
+        g_peak_scratch_addr[dev] = static_cast<int*>(p);
+    }
+    *out = g_peak_scratch_addr[dev];
+    return PSX_OK;
+}
+
+}  // namespace
+}  // namespace psx
+
+extern "C" int psx_find_peaks_noalloc(const float* d_spec, int n, int start, float thresh,
+                                      int* d_idx, float* d_val, int cap, int* h_count,
+                                      psx_stream_t stream)
+{
+    clear_error();
+    if (!d_spec || !h_count || (cap > 0 && (!d_idx || !d_val))) {
+        set_error("find_peaks_noalloc: bad arguments");
+        return PSX_ERR_INVALID;
+    }
+    if (start < 0) start = 0;
+    *h_count = 0;
+    if (n <= start) return PSX_OK;
+    if ((long long)n - start > kNoAllocMaxBins) {
+        set_error("find_peaks_noalloc: %lld bins to scan, the static scratch holds at most %lld "
+                  "(use psx_find_peaks)", (long long)n - start, kNoAllocMaxBins);
+        return PSX_ERR_INVALID;
+    }
+    int* scratch = nullptr;
+    int rc = peak_scratch_address(&scratch);
+    if (rc != PSX_OK) return rc;
+    cudaStream_t s = cs(stream);
+    const int ntiles = (n - start + kCompactTile - 1) / kCompactTile;
+    k_compact_count<<<ntiles, 256, 0, s>>>(d_spec, start, n, thresh, scratch);
+    k_compact_scan<<<1, 32, 0, s>>>(scratch, ntiles, scratch + ntiles);
+    k_compact_write<<<ntiles, 256, 0, s>>>(d_spec, start, n, thresh, scratch, d_idx, d_val, cap);
+    rc = launch_status("compaction kernels");
+    int total = 0;
+    if (rc == PSX_OK)
+        rc = cuda_status(cudaMemcpyAsync(&total, scratch + ntiles, sizeof(int),
+                                         cudaMemcpyDeviceToHost, s), "find_peaks_noalloc copy");
+    if (rc == PSX_OK) rc = cuda_status(cudaStreamSynchronize(s), "find_peaks_noalloc");
+    if (rc != PSX_OK) return rc;
+    *h_count = total;
+    if (total > cap) {
+        set_error("find_peaks_noalloc: %d values above threshold, buffer holds %d", total, cap);
+        return PSX_ERR_OVERFLOW;
+    }
+    return PSX_OK;
+}
