@@ -175,12 +175,13 @@ def trials_of(plan, dm_list):
     return sum(len(ap.generate_accel_list(float(plan.dms[d]), 0.0)) for d in dm_list)
 
 
-def make_params(plan, mode="batched", batch=0):
+def make_params(plan, mode="batched", batch=0, harm_shape=0):
     from peasoup_b200 import search, synth
     return search.SearchParams(fft_size=N_FFT, tsamp=TSAMP, acc_lo=-ACC, acc_hi=ACC,
                                nharmonics=NFOLDS, cfreq_hz=synth.CFREQ_HZ,
                                ch_bw_hz=synth.CH_BW_HZ, birdie_freqs=plan.birdie_freqs,
-                               birdie_widths=plan.birdie_widths, mode=mode, batch=batch)
+                               birdie_widths=plan.birdie_widths, mode=mode, batch=batch,
+                               harm_shape=harm_shape)
 
 
 # ----------------------------------------------------------------- reference
@@ -283,8 +284,17 @@ def run_psx(args, ws, rank, local):
     row = {d: i for i, d in enumerate(need)}
     log(f"[rank {rank}] synthesised {len(need)} series in {time.perf_counter() - t0:.1f}s")
 
+    # ---- autotuner (untimed): trials per launch group x harmonic-kernel shape
+    tune = None
+    batch, shape = args.batch, 0
+    if not args.batch:
+        t0 = time.perf_counter()
+        tune = search.autotune(make_params(plan, "batched"), batches=(2, 4, 8, 16), reps=2)
+        batch, shape = tune["batch"], tune["harm_shape"]
+        log(f"[rank {rank}] autotune: batch {batch}, harmonic shape {shape} "
+            f"({time.perf_counter() - t0:.1f}s)")
     stream = torch.cuda.Stream()
-    eng = search.AccelSearch(make_params(plan, "batched", args.batch))
+    eng = search.AccelSearch(make_params(plan, "batched", batch, shape))
     eng.set_stream(stream.cuda_stream)
 
     def do_step(dm_list, src):
@@ -315,6 +325,7 @@ def run_psx(args, ws, rank, local):
         barrier(ws)
     dt = e0.elapsed_time(e1) / 1e3
     batch_used = eng.info()["batch"]
+    shape_used = eng.info()["harm_shape"]
     dt_max = max_over_ranks(ws, dt)
     tot_trials = sum_over_ranks(ws, ntr)
     value = tot_trials / dt_max
@@ -447,7 +458,8 @@ def run_psx(args, ws, rank, local):
             "config": {"workload": "survey-2^23: 256 DM trials x 2^23 samples, tsamp 76us, "
                                    "acc -100..100, 5 folds, S/N 9, 20 birdies zapped",
                        "dms_per_step": S, "mode": "batched",
-                       "batch": batch_used,
+                       "batch": batch_used, "harm_shape": shape_used,
+                       "tuned": "autotuner (batch x harmonic shape)" if tune else "fixed",
                        "parallelism": f"dm-sharded x{ws}",
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
             "hbm_roofline_frac": hbm_frac,

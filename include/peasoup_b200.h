@@ -286,7 +286,13 @@ typedef struct {
     int batch;                 /* trials per launch (batched); 0 = tuned */
     int use_fft_callback;      /* batched: fuse the resample into cuFFT */
     int use_graph;             /* batched: capture the trial schedule */
+    int harm_shape;            /* harmonic-kernel tile shape 1..PSX_HARM_SHAPES;
+                                  0 = default (psx_autotune picks one) */
 } psx_search_config;
+
+/* Number of tile shapes of the fused harmonic-sum kernel (tile bins,
+   consumer threads, CTAs per SM, exact pass in or out of line). */
+#define PSX_HARM_SHAPES 5
 
 /* Fills `cfg` with the reference's defaults (include/utils/cmdline.hpp:
    99-191) for a transform of `fft_size` samples of `tsamp` s. */
@@ -336,6 +342,20 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
                      int ndm, int output, psx_candidate* h_out, int* h_nassoc,
                      int* h_trial, int* h_dm, size_t cap, size_t* n_out);
 
+/* Autotuner; no counterpart in the reference (which has one fixed
+   schedule).  Times the batched search of `cfg` on seeded synthetic noise
+   of cfg->fft_size samples for every pair (trials per launch group from
+   h_batches[0..nbatch), harmonic-kernel shape 1..PSX_HARM_SHAPES): one
+   warm-up DM trial, then `reps` DM trials through psx_search_block, timed
+   on the host.  When the DM-0 acceleration list is longer than max_trials
+   the range is narrowed around its middle for the timing.  Candidates whose
+   footprint exceeds 80 % of the free device memory are skipped.  Writes
+   the fastest pair into cfg->batch and cfg->harm_shape; h_ms (may be NULL)
+   receives nbatch * PSX_HARM_SHAPES milliseconds per DM trial, batch-major
+   (-1 for a skipped pair).  Results never depend on the pair chosen. */
+int psx_autotune(psx_search_config* cfg, const int* h_batches, int nbatch,
+                 int reps, int max_trials, double* h_ms);
+
 typedef struct {
     int ntrials;          /* acceleration trials of the last call */
     int nbatches;         /* launch groups of the last call */
@@ -346,6 +366,7 @@ typedef struct {
     int graph;            /* 1 if the trial schedule ran as a CUDA graph */
     int batch;            /* trials per launch used */
     int baseline_passes;  /* mean-removal passes of the last DM (-1: host loop) */
+    int harm_shape;       /* harmonic-kernel tile shape in use */
 } psx_search_info;
 
 int psx_search_last_info(const psx_search* s, psx_search_info* info);

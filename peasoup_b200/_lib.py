@@ -25,6 +25,7 @@ PSX_ERR_BUSY = 8
 
 PSX_FFT_R2C = 0
 PSX_FFT_C2R = 1
+PSX_HARM_SHAPES = 5
 PSX_MODE_PLAIN = 0
 PSX_MODE_BATCHED = 1
 PSX_OUT_TRIAL = 0
@@ -58,14 +59,14 @@ class SearchConfig(C.Structure):
                 ("boundary_5_freq", C.c_float), ("boundary_25_freq", C.c_float),
                 ("birdie_freqs", C.POINTER(C.c_float)), ("birdie_widths", C.POINTER(C.c_float)),
                 ("nbirdies", C.c_size_t), ("mode", C.c_int), ("batch", C.c_int),
-                ("use_fft_callback", C.c_int), ("use_graph", C.c_int)]
+                ("use_fft_callback", C.c_int), ("use_graph", C.c_int), ("harm_shape", C.c_int)]
 
 
 class SearchInfo(C.Structure):
     _fields_ = [("ntrials", C.c_int), ("nbatches", C.c_int), ("kernel_launches", C.c_int),
                 ("fft_launches", C.c_int), ("above_threshold", C.c_longlong),
                 ("fft_callback", C.c_int), ("graph", C.c_int), ("batch", C.c_int),
-                ("baseline_passes", C.c_int)]
+                ("baseline_passes", C.c_int), ("harm_shape", C.c_int)]
 
 
 class SearchProfile(C.Structure):
@@ -126,6 +127,7 @@ SIGNATURES = {
     "psx_search_set_profile": (_i, [_vp, _i]),
     "psx_search_get_profile": (_i, [_vp, C.POINTER(SearchProfile), _i]),
     "psx_search_debug_tap": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "psx_autotune": (_i, [C.POINTER(SearchConfig), _vp, _i, _i, _i, _vp]),
 }
 
 _lib = None

@@ -13,9 +13,15 @@
 // in the reference's summation order.  CTAs are persistent and keep two
 // stages, so the copies of the next item overlap the sums of this one.
 //
-// Threshold crossings are rare: each fold's test is one warp vote, and the
-// search-range check and the append (one atomic per warp and fold) run
-// only in warps where some lane crossed.
+// Each consumer thread owns K = T/NC outputs (NC apart), accumulated in
+// pairs with packed two-lane float adds (add.rn.f32x2: each lane rounds as
+// a scalar add, so the sums are those of the reference's order).
+// Threshold crossings are rare: a fast pass keeps each output's largest
+// fold value, scaled in float, and votes against a threshold lowered by
+// 2^-20 relative (the float scale is within 3*2^-24 of the reference's
+// double-scaled product); only warps where some lane passes the vote run
+// the exact pass (reference scales, search ranges, one atomic per warp and
+// fold).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -28,7 +34,35 @@ struct PeakParams {
     int end[6];
     unsigned lo, hi;  // union of the ranges; lo is rounded down to 128
     float thresh;
+    float vote;       // fast-pass vote level: thresh lowered by 2^-20 relative
 };
+
+// Packed two-lane float arithmetic (sm_100): one instruction for two
+// independent IEEE round-to-nearest operations.
+__device__ __forceinline__ float2 f2add(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rc, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rc;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rc;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rc, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rc;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
 
 // Fraction q (0-based) in the reference's order: fold 1 {1/2}; fold 2
 // {3/4, 1/4}; folds 3..5 {1/2^h, 3/2^h, ...} ascending.
@@ -146,8 +180,18 @@ __device__ __forceinline__ void emit_hit(bool hit, int trial, int fold, unsigned
 // rsqrt(32.0), evaluated once per thread by the same function calls.
 struct FoldScales {
     double r2, r8, r32;
-    __device__ __forceinline__ FoldScales() : r2(rsqrt(2.0)), r8(rsqrt(8.0)), r32(rsqrt(32.0)) {}
+    float f2, f8, f32;  // the same factors rounded to float (fast pass only)
+    __device__ __forceinline__ FoldScales()
+        : r2(rsqrt(2.0)), r8(rsqrt(8.0)), r32(rsqrt(32.0)),
+          f2((float)r2), f8((float)r8), f32((float)r32) {}
 };
+
+// Float scale of fold H for the fast pass's vote.
+template <int H>
+__device__ __forceinline__ float fold_scale_f(const FoldScales& c)
+{
+    return H == 1 ? c.f2 : H == 2 ? 0.5f : H == 3 ? c.f8 : H == 4 ? 0.25f : c.f32;
+}
 
 template <int H>
 __device__ __forceinline__ float fold_scale(float val, const FoldScales& c);
@@ -158,15 +202,17 @@ template <> __device__ __forceinline__ float fold_scale<4>(float val, const Fold
 template <> __device__ __forceinline__ float fold_scale<5>(float val, const FoldScales& c) { return val * c.r32; }
 
 // Adds fraction Q to every output of the thread (K = T/NC outputs, NC
-// apart).  At a fold boundary: in the fast pass (EMIT false) the fold value
-// only raises the running maximum `mx`; in the exact pass (EMIT true) the
-// fold's search range is applied and hits are appended with one atomic
+// apart, accumulated as K/2 packed pairs).  At a fold boundary: in the fast
+// pass (EMIT false) the float-scaled fold value only raises the running
+// maximum `mx`; in the exact pass (EMIT true) the reference's scale and the
+// fold's search range are applied and hits are appended with one atomic
 // per warp.  Recurses to Q+1.
 template <int Q, int F, int T, int NC, bool EMIT>
 struct FracStep {
+    static constexpr int K = T / NC;
     static __device__ __forceinline__ void run(const float* __restrict__ sm,
                                                const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                               float (&val)[T / NC], float (&mx)[T / NC],
+                                               float2 (&acc)[K / 2], float (&mx)[K],
                                                const FoldScales& fs, unsigned i0, unsigned tid,
                                                const PeakParams& pp, int trial,
                                                int4* __restrict__ rec,
@@ -175,21 +221,30 @@ struct FracStep {
         constexpr int h = frac_h(Q), m = frac_m(Q);
         constexpr int step = (NC * m) >> h;  // exact: NC is a multiple of 32
 #pragma unroll
-        for (int k = 0; k < T / NC; ++k) val[k] += sm[base[Q] + k * step];
+        for (int k = 0; k < K / 2; ++k)
+            acc[k] = f2add(acc[k], make_float2(sm[base[Q] + (2 * k) * step],
+                                               sm[base[Q] + (2 * k + 1) * step]));
         if (Q == fold_last(h)) {
+            if (EMIT) {
 #pragma unroll
-            for (int k = 0; k < T / NC; ++k) {
-                const float s = fold_scale<h>(val[k], fs);
-                if (EMIT) {
+                for (int k = 0; k < K; ++k) {
+                    const float v = (k & 1) ? acc[k / 2].y : acc[k / 2].x;
+                    const float s = fold_scale<h>(v, fs);
                     const unsigned i = i0 + tid + k * NC;
                     const bool hit = s > pp.thresh && (int)i >= pp.start[h] && (int)i < pp.end[h];
                     emit_hit(hit, trial, h, i, s, rec, counter, cap, tid & 31u);
-                } else {
-                    mx[k] = fmaxf(mx[k], s);
+                }
+            } else {
+                const float sf = fold_scale_f<h>(fs);
+#pragma unroll
+                for (int k = 0; k < K / 2; ++k) {
+                    const float2 s = f2mul(acc[k], make_float2(sf, sf));
+                    mx[2 * k] = fmaxf(mx[2 * k], s.x);
+                    mx[2 * k + 1] = fmaxf(mx[2 * k + 1], s.y);
                 }
             }
         }
-        FracStep<Q + 1, F, T, NC, EMIT>::run(sm, base, val, mx, fs, i0, tid, pp, trial, rec,
+        FracStep<Q + 1, F, T, NC, EMIT>::run(sm, base, acc, mx, fs, i0, tid, pp, trial, rec,
                                              counter, cap);
     }
 };
@@ -197,7 +252,7 @@ struct FracStep {
 template <int F, int T, int NC, bool EMIT>
 struct FracStep<(1 << F) - 1, F, T, NC, EMIT> {
     static __device__ __forceinline__ void run(const float*, const unsigned (&)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                               float (&)[T / NC], float (&)[T / NC],
+                                               float2 (&)[T / NC / 2], float (&)[T / NC],
                                                const FoldScales&, unsigned, unsigned,
                                                const PeakParams&, int, int4*, unsigned*, unsigned)
     {
@@ -231,50 +286,71 @@ __device__ __forceinline__ void window_params(unsigned lane, unsigned& m, unsign
     off += (((unsigned)T * msum) >> h) + 8u * r;
 }
 
-// The exact pass of one item (rare: only warps where some output crosses
-// the threshold): every fold's value again, its search range, and the
-// appends.  Kept out of line so the fast pass's registers are not shared
-// with it.
+// The exact pass of one item (rare: only warps where some output passes
+// the vote): every fold's value again with the reference's scales, its
+// search range, and the appends.
 template <int F, int T, int NC>
-__device__ __noinline__ void exact_pass(const float* __restrict__ sm,
-                                        const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                        const FoldScales& fs, unsigned i0, unsigned tid,
-                                        const PeakParams& pp, int trial, int4* __restrict__ rec,
-                                        unsigned* __restrict__ counter, unsigned cap)
+__device__ __forceinline__ void exact_body(const float* __restrict__ sm,
+                                           const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                           const FoldScales& fs, unsigned i0, unsigned tid,
+                                           const PeakParams& pp, int trial, int4* __restrict__ rec,
+                                           unsigned* __restrict__ counter, unsigned cap)
 {
-    float val[T / NC], mx[T / NC];
+    constexpr int K = T / NC;
+    float2 acc[K / 2];
+    float mx[K];
 #pragma unroll
-    for (int k = 0; k < T / NC; ++k) {
-        val[k] = sm[tid + k * NC];
+    for (int k = 0; k < K; ++k) {
+        const float v = sm[tid + k * NC];
+        if (k & 1) acc[k / 2].y = v; else acc[k / 2].x = v;
         const unsigned i = i0 + tid + k * NC;
-        const bool hit = val[k] > pp.thresh && (int)i >= pp.start[0] && (int)i < pp.end[0];
-        emit_hit(hit, trial, 0, i, val[k], rec, counter, cap, tid & 31u);
+        const bool hit = v > pp.thresh && (int)i >= pp.start[0] && (int)i < pp.end[0];
+        emit_hit(hit, trial, 0, i, v, rec, counter, cap, tid & 31u);
     }
-    FracStep<0, F, T, NC, true>::run(sm, base, val, mx, fs, i0, tid, pp, trial, rec, counter, cap);
+    FracStep<0, F, T, NC, true>::run(sm, base, acc, mx, fs, i0, tid, pp, trial, rec, counter, cap);
 }
 
-// Sums one staged item: a fast pass that tracks each output's largest
-// fold value, then -- only in warps where some output crosses the
-// threshold -- the exact pass.
+// The same, kept out of line so that the fast pass does not share its
+// registers (a call frame in local memory is the price).
 template <int F, int T, int NC>
+__device__ __noinline__ void exact_pass_ool(const float* __restrict__ sm,
+                                            const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
+                                            const FoldScales& fs, unsigned i0, unsigned tid,
+                                            const PeakParams& pp, int trial,
+                                            int4* __restrict__ rec, unsigned* __restrict__ counter,
+                                            unsigned cap)
+{
+    exact_body<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
+}
+
+// Sums one staged item: the fast pass, then -- only in warps where some
+// output passes the vote -- the exact pass (inline or out of line).
+template <int F, int T, int NC, bool OOL>
 __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
                                          const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
                                          const FoldScales& fs, unsigned i0, unsigned tid,
                                          const PeakParams& pp, int trial, int4* __restrict__ rec,
                                          unsigned* __restrict__ counter, unsigned cap)
 {
-    float val[T / NC], mx[T / NC];
+    constexpr int K = T / NC;
+    float2 acc[K / 2];
+    float mx[K];
 #pragma unroll
-    for (int k = 0; k < T / NC; ++k) {
-        val[k] = sm[tid + k * NC];
-        mx[k] = val[k];
+    for (int k = 0; k < K; ++k) {
+        const float v = sm[tid + k * NC];
+        if (k & 1) acc[k / 2].y = v; else acc[k / 2].x = v;
+        mx[k] = v;
     }
-    FracStep<0, F, T, NC, false>::run(sm, base, val, mx, fs, i0, tid, pp, trial, rec, counter, cap);
+    FracStep<0, F, T, NC, false>::run(sm, base, acc, mx, fs, i0, tid, pp, trial, rec, counter, cap);
     bool over = false;
 #pragma unroll
-    for (int k = 0; k < T / NC; ++k) over |= mx[k] > pp.thresh;
-    if (__any_sync(0xffffffffu, over))
-        exact_pass<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
+    for (int k = 0; k < K; ++k) over |= mx[k] > pp.vote;
+    if (__any_sync(0xffffffffu, over)) {
+        if (OOL)
+            exact_pass_ool<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
+        else
+            exact_body<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
+    }
 }
 
 // Persistent, warp-specialised CTA: warp 0 produces (bulk copies of item
@@ -284,8 +360,8 @@ __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
 // a stage's bytes have landed, empty[s] when every consumer warp is done
 // with it.  No CTA-wide barrier is used in the loop; every wait is bounded
 // and a timeout is reported in counter[1].
-template <int F, int T, int NC>
-__global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restrict__ p,
+template <int F, int T, int NC, int MINB, bool OOL>
+__global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __restrict__ p,
                                                            size_t ppitch, unsigned row_len,
                                                            PeakParams pp, int trial0, int rows,
                                                            unsigned ntiles,
@@ -293,7 +369,7 @@ __global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restri
                                                            unsigned* __restrict__ counter,
                                                            unsigned cap)
 {
-    static_assert(T % 128 == 0 && NC % 32 == 0 && T % NC == 0, "tile shape");
+    static_assert(T % 128 == 0 && NC % 32 == 0 && T % (2 * NC) == 0, "tile shape");
     constexpr int STAGE = harm_smem_floats(F, T);
     constexpr int NW = nfrac(F) + 1;  // windows (tile + fractions)
     constexpr unsigned kLimit = 1u << 22;
@@ -371,8 +447,8 @@ __global__ void __launch_bounds__(NC + 32, 3) k_harm_tiles(const float* __restri
                     ok = false;
                     mbar_wait_bounded(&full[s], ph, kLimit);  // let the copies land
                 }
-                sum_item<F, T, NC>(smem + s * STAGE, base, fs, pp.lo + tile * (unsigned)T, tid,
-                                   pp, trial0 + (int)row, rec, counter, cap);
+                sum_item<F, T, NC, OOL>(smem + s * STAGE, base, fs, pp.lo + tile * (unsigned)T,
+                                        tid, pp, trial0 + (int)row, rec, counter, cap);
                 __syncwarp();
                 if (lane == 0)
                     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s]))

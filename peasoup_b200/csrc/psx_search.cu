@@ -97,45 +97,68 @@ __global__ void k_baseline_reset(unsigned* __restrict__ state)
     state[1] = 0u;
 }
 
-// Fused harmonic sums + threshold + compaction: tile shape and launcher.
-// Persistent grid of kHarmCtasPerSm CTAs per SM, each one producer warp
-// plus kHarmConsumers consumer threads and kHarmStages shared stages.
-constexpr int kHarmTile = 512;
-constexpr int kHarmConsumers = 128;
+// Fused harmonic sums + threshold + compaction: tile shapes and launcher.
+// Persistent grid of MINB CTAs per SM, each one producer warp plus NC
+// consumer threads and kHarmStages shared stages of a T-bin tile and its
+// fractional windows.  The shapes below are the autotuner's choices
+// (psx_search_config::harm_shape); shape 4 is the default.
 constexpr int kHarmStages = 2;
-constexpr int kHarmCtasPerSm = 3;
 
-template <int F>
-constexpr size_t harm_smem_bytes()
-{
-    return (size_t)kHarmStages * sizeof(float) * harm_smem_floats(F, kHarmTile);
-}
+struct HarmShape {
+    int T, NC, minb;
+    bool ool;  // exact pass out of line
+};
+constexpr HarmShape kHarmShapes[] = {
+    {512, 128, 3, true},   // 1
+    {512, 256, 3, true},   // 2
+    {256, 128, 6, true},   // 3
+    {512, 256, 3, false},  // 4
+    {256, 128, 6, false},  // 5
+};
+static_assert(sizeof(kHarmShapes) / sizeof(kHarmShapes[0]) == PSX_HARM_SHAPES, "shape table");
+constexpr int kHarmDefaultShape = 4;
 
-template <int F>
-static int launch_harm_f(const float* p, size_t ppitch, unsigned row_len, const PeakParams& pp,
-                         int trial0, int rows, int4* rec, unsigned* counter, unsigned cap,
-                         cudaStream_t s)
-{
-    const unsigned ntiles = (pp.hi - pp.lo + kHarmTile - 1) / kHarmTile;
-    const unsigned items = ntiles * (unsigned)rows;
-    const unsigned grid = std::min(items, (unsigned)(sm_count() * kHarmCtasPerSm));
-    k_harm_tiles<F, kHarmTile, kHarmConsumers>
-        <<<grid, kHarmConsumers + 32, harm_smem_bytes<F>(), s>>>(p, ppitch, row_len, pp, trial0,
-                                                                 rows, ntiles, rec, counter, cap);
-    return launch_status("harmonic-sum kernel");
-}
+template <int F, int SH>
+struct HarmKernel {
+    static constexpr HarmShape S = kHarmShapes[SH];
+    static constexpr size_t smem_bytes()
+    {
+        return (size_t)kHarmStages * sizeof(float) * harm_smem_floats(F, S.T);
+    }
+    static int configure()
+    {
+        return cuda_status(cudaFuncSetAttribute(k_harm_tiles<F, S.T, S.NC, S.minb, S.ool>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem_bytes()),
+                           "harmonic-sum kernel attribute");
+    }
+    static int launch(const float* p, size_t ppitch, unsigned row_len, const PeakParams& pp,
+                      int trial0, int rows, int4* rec, unsigned* counter, unsigned cap,
+                      cudaStream_t s)
+    {
+        const unsigned ntiles = (pp.hi - pp.lo + S.T - 1) / S.T;
+        const unsigned items = ntiles * (unsigned)rows;
+        const unsigned grid = std::min(items, (unsigned)(sm_count() * S.minb));
+        k_harm_tiles<F, S.T, S.NC, S.minb, S.ool><<<grid, S.NC + 32, smem_bytes(), s>>>(
+            p, ppitch, row_len, pp, trial0, rows, ntiles, rec, counter, cap);
+        return launch_status("harmonic-sum kernel");
+    }
+};
 
 template <int F>
 static int configure_harm_f()
 {
-    return cuda_status(
-        cudaFuncSetAttribute(k_harm_tiles<F, kHarmTile, kHarmConsumers>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)harm_smem_bytes<F>()),
-        "harmonic-sum kernel attribute");
+    int rc = PSX_OK;
+    if (rc == PSX_OK) rc = HarmKernel<F, 0>::configure();
+    if (rc == PSX_OK) rc = HarmKernel<F, 1>::configure();
+    if (rc == PSX_OK) rc = HarmKernel<F, 2>::configure();
+    if (rc == PSX_OK) rc = HarmKernel<F, 3>::configure();
+    if (rc == PSX_OK) rc = HarmKernel<F, 4>::configure();
+    return rc;
 }
 
-// Opts the kernel for F folds into its dynamic shared memory (once per
-// device, before any launch or capture).
+// Opts every shape of the kernel for F folds into its dynamic shared
+// memory (once per device, before any launch or capture).
 static int configure_harm(int F)
 {
     switch (F) {
@@ -148,17 +171,31 @@ static int configure_harm(int F)
     }
 }
 
-static int launch_harm(int F, const float* p, size_t ppitch, unsigned row_len,
+template <int F>
+static int launch_harm_f(int shape, const float* p, size_t ppitch, unsigned row_len,
+                         const PeakParams& pp, int trial0, int rows, int4* rec, unsigned* counter,
+                         unsigned cap, cudaStream_t s)
+{
+    switch (shape) {
+    case 2: return HarmKernel<F, 1>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 3: return HarmKernel<F, 2>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 4: return HarmKernel<F, 3>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 5: return HarmKernel<F, 4>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    default: return HarmKernel<F, 0>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    }
+}
+
+static int launch_harm(int F, int shape, const float* p, size_t ppitch, unsigned row_len,
                        const PeakParams& pp, int trial0, int rows, int4* rec, unsigned* counter,
                        unsigned cap, cudaStream_t s)
 {
     switch (F) {
-    case 0: return launch_harm_f<0>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 1: return launch_harm_f<1>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 2: return launch_harm_f<2>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 3: return launch_harm_f<3>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 4: return launch_harm_f<4>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    default: return launch_harm_f<5>(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 0: return launch_harm_f<0>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 1: return launch_harm_f<1>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 2: return launch_harm_f<2>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 3: return launch_harm_f<3>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 4: return launch_harm_f<4>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    default: return launch_harm_f<5>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
     }
 }
 
@@ -222,6 +259,7 @@ struct psx_search {
     size_t N = 0, B = 0, Bp = 0;
     int F = 0;
     int batch = 1;
+    int harm_shape = 1;
     int device = 0;
     cudaStream_t st = nullptr;   // compute
     cudaStream_t cst = nullptr;  // record copies
@@ -484,7 +522,7 @@ int psx_search::trials_enqueue(Slot& s, int nacc)
         PSX_TRY(launch_status("form kernel"));
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 2], st));
         if (span) {
-            PSX_TRY(launch_harm(F, d_p, Bp, (unsigned)Bp, pk, t0, b, s.d_rec, s.d_count,
+            PSX_TRY(launch_harm(F, harm_shape, d_p, Bp, (unsigned)Bp, pk, t0, b, s.d_rec, s.d_count,
                                 (unsigned)s.rec_cap, st));
             ++s.launches;
         }
@@ -788,6 +826,7 @@ void psx_search_config_defaults(psx_search_config* c, size_t fft_size, float tsa
     c->batch = 0;
     c->use_fft_callback = 0;
     c->use_graph = 1;
+    c->harm_shape = 0;
 }
 
 static int check_config(const psx_search_config* c)
@@ -814,6 +853,10 @@ static int check_config(const psx_search_config* c)
     }
     if (c->batch < 0 || c->batch > 1024) {
         set_error("search: batch must be 0..1024");
+        return PSX_ERR_INVALID;
+    }
+    if (c->harm_shape < 0 || c->harm_shape > PSX_HARM_SHAPES) {
+        set_error("search: harm_shape must be 0..%d", PSX_HARM_SHAPES);
         return PSX_ERR_INVALID;
     }
     if (c->nbirdies && (!c->birdie_freqs || !c->birdie_widths)) {
@@ -874,6 +917,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->Bp = round_up(s->B, 64);
     s->F = cfg->nharmonics;
     s->batch = effective_batch(cfg);
+    s->harm_shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
     unsigned hc = std::thread::hardware_concurrency();
     s->nthreads = (int)std::max(1u, std::min(8u, hc ? hc : 1u));
     // pipeline_multi.cu:126-128: tobs and bin width are floats
@@ -903,6 +947,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->pk.lo = hi > lo ? (lo & ~127u) : 0;
     s->pk.hi = hi > lo ? hi : 0;
     s->pk.thresh = cfg->min_snr;
+    s->pk.vote = cfg->min_snr - std::fabs(cfg->min_snr) * 0x1p-20f;
 
     int rc = PSX_OK;
     auto fail = [&](int code) {
@@ -969,6 +1014,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     if ((rc = cuda_status(cudaStreamSynchronize(s->st), "search create")) != PSX_OK)
         return fail(rc);
     s->info.batch = s->batch;
+    s->info.harm_shape = s->harm_shape;
     s->info.fft_callback = cb ? 1 : 0;
     *out = s;
     return PSX_OK;
@@ -1030,6 +1076,7 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
     s->info = psx_search_info{};
     s->info.batch = bp;
     s->info.fft_callback = cbk;
+    s->info.harm_shape = s->harm_shape;
     s->info.graph = s->batched() && s->cfg.use_graph && !s->profile ? 1 : 0;
     std::vector<psx_candidate> all, out;
     std::vector<int> all_na, all_tr, all_dm, na, tr;

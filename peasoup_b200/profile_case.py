@@ -24,6 +24,7 @@ def main(argv=None) -> int:
     ap.add_argument("--tsamp", type=float, default=76e-6)
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--graph", action="store_true")
+    ap.add_argument("--harm-shape", type=int, default=0)
     a = ap.parse_args(argv)
 
     import torch
@@ -33,7 +34,7 @@ def main(argv=None) -> int:
     p = search.SearchParams(fft_size=a.nsamps, tsamp=a.tsamp, acc_lo=-100.0, acc_hi=100.0,
                             nharmonics=5, cfreq_hz=synth.CFREQ_HZ, ch_bw_hz=synth.CH_BW_HZ,
                             birdie_freqs=plan.birdie_freqs, birdie_widths=plan.birdie_widths,
-                            batch=a.batch, graph=a.graph)
+                            batch=a.batch, graph=a.graph, harm_shape=a.harm_shape)
     s = search.AccelSearch(p)
     s.set_profile(not a.graph)
     for d in range(a.ndm):

@@ -56,6 +56,7 @@ class SearchParams:
     # its own kernel.
     fft_callback: bool = False
     graph: bool = True             # batched: CUDA-graph trial schedule
+    harm_shape: int = 0            # harmonic-kernel tile shape (0 = default)
 
     def to_c(self):
         cfg = SearchConfig()
@@ -74,7 +75,25 @@ class SearchParams:
         cfg.mode = _lib.PSX_MODE_PLAIN if self.mode == "plain" else _lib.PSX_MODE_BATCHED
         cfg.use_fft_callback = int(self.fft_callback)
         cfg.use_graph = int(self.graph)
+        cfg.harm_shape = int(self.harm_shape)
         return cfg, keep
+
+
+def autotune(params: SearchParams, batches=(2, 4, 8, 16), reps: int = 2,
+             max_trials: int = 128) -> dict:
+    """Times every (trials per launch group, harmonic-kernel shape) pair on
+    synthetic noise of params.fft_size samples (psx_autotune) and returns
+    {"batch", "harm_shape", "ms_per_dm": {(batch, shape): ms}}; the choice
+    changes grouping only, never results."""
+    cfg, keep = params.to_c()
+    b = np.ascontiguousarray(batches, np.int32)
+    ms = np.zeros(len(b) * _lib.PSX_HARM_SHAPES, np.float64)
+    check(load().psx_autotune(C.byref(cfg), b.ctypes.data_as(C.c_void_p), len(b), reps,
+                              max_trials, ms.ctypes.data_as(C.c_void_p)), "autotune")
+    del keep
+    table = {(int(bb), sh + 1): float(ms[i * _lib.PSX_HARM_SHAPES + sh])
+             for i, bb in enumerate(b) for sh in range(_lib.PSX_HARM_SHAPES)}
+    return {"batch": int(cfg.batch), "harm_shape": int(cfg.harm_shape), "ms_per_dm": table}
 
 
 def footprint(params: SearchParams) -> int:

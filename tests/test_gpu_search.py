@@ -154,6 +154,55 @@ def test_block_equals_single_dm_calls(S):
     s.close()
 
 
+@pytest.mark.parametrize("nh", [5, 3])
+def test_harmonic_kernel_shapes_identical(S, nh):
+    """Every tile shape of the fused harmonic kernel sums in the same order
+    and must give exactly the same candidates (S/N bits included), with a
+    low threshold so that many bins pass the vote and take the exact pass."""
+    from peasoup_b200 import _lib
+    search, synth = S
+    n, ts = 1 << 17, 64e-6
+    x = synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(2.3e-3, 15.0, 0.04, 0.6)]), 5)
+    outs, hits = [], []
+    for shape in range(1, _lib.PSX_HARM_SHAPES + 1):
+        s = search.AccelSearch(_params(S, n, ts, acc_lo=-60.0, acc_hi=60.0, nharmonics=nh,
+                                       min_snr=4.5, batch=4, harm_shape=shape))
+        c, na, tr = s.search(x, 0.0, 0, per_dm=False)
+        info = s.info()
+        assert info["harm_shape"] == shape
+        outs.append(c)
+        hits.append(info["above_threshold"])
+        s.close()
+    assert hits[0] > 200 and len(outs[0]) > 10
+    assert hits == [hits[0]] * len(hits)
+    for c in outs[1:]:
+        assert np.array_equal(c, outs[0])
+
+
+def test_autotune_picks_a_timed_pair(S):
+    """The autotuner times every (batch, shape) pair it may use and returns
+    the fastest; the tuned engine finds what the default engine finds."""
+    search, synth = S
+    n, ts = 1 << 16, 64e-6
+    p = _params(S, n, ts, acc_lo=-100.0, acc_hi=100.0, nharmonics=4, min_snr=6.0)
+    t = search.autotune(p, batches=(1, 4), reps=1, max_trials=16)
+    assert t["batch"] in (1, 4) and 1 <= t["harm_shape"] <= 5
+    ms = t["ms_per_dm"]
+    assert len(ms) == 10 and all(v > 0 for v in ms.values())
+    assert ms[(t["batch"], t["harm_shape"])] == min(ms.values())
+    x = synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(3.3e-3, 30.0, 0.05, 0.8)]), 8)
+    import dataclasses
+    tuned = search.AccelSearch(dataclasses.replace(p, batch=t["batch"],
+                                                   harm_shape=t["harm_shape"]))
+    default = search.AccelSearch(p)
+    a, b = tuned.search(x)[0], default.search(x)[0]
+    assert len(a) > 0 and np.array_equal(a, b)
+    tuned.close()
+    default.close()
+
+
 def test_repeatable_and_graph_replay(S):
     search, synth = S
     n, ts = 1 << 16, 64e-6
