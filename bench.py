@@ -18,7 +18,10 @@ Printed: one JSON line.  `value` = DM x acceleration trials per second of
 the batched path with the series resident in HBM; `e2e` = the same through
 the C ABI (psx_search_block) from pinned host buffers (host->device copies
 inside the timed region, candidates copied back); `plain` = the one-trial-
-per-launch path on a sample of the same workload; `roofline` = the
+per-launch path on a sample of the same workload; `served` = the served
+workload (Poisson arrivals of uneven segmented searches through the C++
+server, p50/p95/p99 latency from arrival and from admission, each request
+also run alone for the ratios); `roofline` = the
 dominant stage's achieved HBM bytes/s against the measured copy bandwidth;
 `cpu_baseline` = the FP64 CPU oracle on a bounded sample.
 
@@ -49,6 +52,10 @@ TSAMP = 76e-6
 ACC = 100.0
 NFOLDS = 5
 NDM = 256
+SERVED_REQUESTS = 32
+SERVED_TRIAL_BUDGET = 2000
+SERVED_SLOTS = 2
+SERVED_BUDGET = 150_000_000_000
 
 
 def log(*a):
@@ -266,6 +273,106 @@ def cpu_baseline(plan, block_row, dm):
     return per_trial, per_dm, t1 + t3
 
 
+
+# ----------------------------------------------------------------- served
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
+
+
+def _served_series(r, seed):
+    """One request's block on the device: white N(0,1) noise plus one
+    injected accelerated pulse train per DM trial (seeded)."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.randn((r.ndm, r.fft_size), device="cuda", generator=g)
+    n = torch.arange(r.fft_size, device="cuda", dtype=torch.float64)
+    rng = np.random.default_rng(seed)
+    for d in range(r.ndm):
+        f0 = float(np.exp(rng.uniform(np.log(2.0), np.log(500.0))))
+        a = float(rng.uniform(-0.8, 0.8)) * r.acc_half
+        k = a * r.tsamp / (2.0 * 299792458.0)
+        ph = torch.frac(f0 * r.tsamp * (n - k * n * (n - r.fft_size)))
+        x[d] += (0.3 * torch.exp(-0.5 * ((ph - 0.5) / 0.02) ** 2)).float()
+    return x
+
+
+def run_served(nreq, rank, log_prefix):
+    """The served workload (Poisson arrivals, uneven requests) through the
+    C++ server, then every request alone on a one-slot server: latency
+    from arrival and from admission, throughput, and the ratios to the
+    isolated runs."""
+    import threading as th
+    import torch
+    from peasoup_b200 import serve
+    reqs = serve.served_stream(nreq, seed=1, rate=4.0, trial_budget=SERVED_TRIAL_BUDGET)
+    params = [serve.request_params(r) for r in reqs]
+
+    def one_pass(max_active, paced):
+        srv = serve.Server(SERVED_BUDGET, max_active=max_active)
+        res = [None] * len(reqs)
+        tickets = [None] * len(reqs)
+        ready = [th.Event() for _ in reqs]
+
+        def collect():
+            for i in range(len(reqs)):
+                ready[i].wait()
+                res[i] = srv.wait(tickets[i])[3]
+
+        ct = th.Thread(target=collect)
+        ct.start()
+        t_start = srv.clock()
+        arrivals = []
+        for i, r in enumerate(reqs):
+            x = _served_series(r, 1000 + i)
+            torch.cuda.current_stream().synchronize()   # this stream only
+            if paced:
+                delay = t_start + r.arrival - srv.clock()
+                if delay > 0:
+                    time.sleep(delay)
+                arrivals.append(t_start + r.arrival)
+            tickets[i] = srv.submit(params[i], x, np.arange(r.ndm, dtype=np.float32) * 0.5)
+            if not paced:
+                arrivals.append(srv.clock())
+                ready[i].set()
+                while res[i] is None:   # alone: one request on the device at a time
+                    time.sleep(0.001)
+            else:
+                ready[i].set()
+            del x
+        ct.join()
+        srv.close()
+        return res, arrivals
+
+    mixed, arr = one_pass(SERVED_SLOTS, True)
+    alone, _ = one_pass(1, False)
+    trials = sum(s["ntrials"] for s in mixed)
+    lat_arr = [1e3 * (s["t_done"] - a) for s, a in zip(mixed, arr)]
+    lat_adm = [1e3 * (s["t_done"] - s["t_admit"]) for s in mixed]
+    iso = [1e3 * (s["t_done"] - s["t_admit"]) for s in alone]
+    span = max(s["t_done"] for s in mixed) - min(arr)
+    served_tps = trials / span
+    isolated_tps = trials / (sum(iso) / 1e3)
+    ratio = [a / b for a, b in zip(lat_adm, iso)]
+    failed = sum(1 for s in mixed + alone if s["status"] != 0)
+    return {
+        "requests": len(reqs), "failed": failed, "arrival_rate_per_s": 4.0,
+        "trials": int(trials), "trials_per_s": served_tps,
+        "latency_from_arrival_ms": {"p50": _pct(lat_arr, 50), "p95": _pct(lat_arr, 95),
+                                    "p99": _pct(lat_arr, 99)},
+        "latency_from_admission_ms": {"p50": _pct(lat_adm, 50), "p95": _pct(lat_adm, 95),
+                                      "p99": _pct(lat_adm, 99)},
+        "isolated_ms": {"p50": _pct(iso, 50), "p99": _pct(iso, 99)},
+        "p99_admitted_over_p99_isolated": _pct(lat_adm, 99) / _pct(iso, 99),
+        "per_request_ratio_p99": _pct(ratio, 99),
+        "throughput_over_isolated_back_to_back": served_tps / isolated_tps,
+        "max_active": SERVED_SLOTS, "hbm_budget_gb": SERVED_BUDGET / 1e9,
+        "engines_reused": int(sum(s["engine_reused"] for s in mixed)),
+        "workload": (f"{len(reqs)} requests, Poisson 4/s (seed 1), fft_size in 2^20..2^25 "
+                     f"incl. 3*2^k, DM count log-uniform 16..512 cut to <= "
+                     f"{SERVED_TRIAL_BUDGET} 2^23-equivalent trials per request, acc "
+                     f"half-range 10..300, 3..5 folds, white noise + one pulsar per DM"),
+    }
+
 # ----------------------------------------------------------------- main arm
 def run_psx(args, ws, rank, local):
     import torch
@@ -448,6 +555,13 @@ def run_psx(args, ws, rank, local):
                           f"{per_dm:.2f}s per DM prologue, extrapolated to "
                           f"{avg_trials:.1f} trials per DM")}
     eng.close()
+    served = None
+    if rank == 0 and ws == 1 and args.served > 0:
+        del block
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        served = run_served(args.served, rank, "served")
+        log(f"[rank {rank}] served workload in {time.perf_counter() - t0:.1f}s")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": ws,
@@ -463,7 +577,8 @@ def run_psx(args, ws, rank, local):
                        "parallelism": f"dm-sharded x{ws}",
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
             "hbm_roofline_frac": hbm_frac,
-            "plain": plain, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "plain": plain, "e2e": e2e, "served": served, "roofline": roofline,
+            "cpu_baseline": cpu,
             "clocks": clocks, "gpu_launches": launches, "candidates": ncand,
             "trials": int(tot_trials),
         }
@@ -482,6 +597,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--served", type=int, default=SERVED_REQUESTS,
+                    help="requests of the served workload (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_init()

@@ -367,6 +367,8 @@ typedef struct {
     int batch;            /* trials per launch used */
     int baseline_passes;  /* mean-removal passes of the last DM (-1: host loop) */
     int harm_shape;       /* harmonic-kernel tile shape in use */
+    int capture_fallbacks; /* schedules launched directly because their
+                              graph capture was invalidated */
 } psx_search_info;
 
 int psx_search_last_info(const psx_search* s, psx_search_info* info);
@@ -395,6 +397,75 @@ int psx_search_get_profile(psx_search* s, psx_search_profile* out, int reset);
    (N/2+1 floats), recomputed on the device.  Any pointer may be NULL. */
 int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
                          float* h_tim_r, float* h_pspec, float* h_norm2);
+
+/* Reuses an instance for another request with the same transform length,
+   folds, mode, batch, harmonic shape and callback setting (the things its
+   buffers and plans depend on): acceleration range, tsamp, thresholds,
+   frequency limits and birdies may all change.  Waits for the instance's
+   queued work first.  No counterpart in the reference (whose Worker builds
+   its transforms once per process, src/pipeline_multi.cu:114-149). */
+int psx_search_retarget(psx_search* s, const psx_search_config* cfg);
+
+/* ------------------------------------------------------------------ */
+/* Served loop; no counterpart in the reference, which searches one     */
+/* observation per process                                              */
+/* ------------------------------------------------------------------ */
+
+typedef struct psx_server psx_server;
+
+typedef struct {
+    int device;         /* CUDA device of every search instance */
+    size_t hbm_budget;  /* device bytes the server may hold in instances
+                           (busy and pooled), by psx_search_footprint */
+    int max_active;     /* requests searched at once (1..64), one host thread
+                           and one instance each; their GPU work overlaps */
+    int max_queue;      /* pending requests before submit refuses */
+} psx_server_config;
+
+typedef struct {
+    double t_submit;    /* seconds on the server clock (psx_server_clock) */
+    double t_admit;     /* when a slot and the memory were granted */
+    double t_done;      /* when its candidates were ready */
+    size_t footprint;   /* bytes newly charged at admission (0 if reused) */
+    long long ntrials;  /* acceleration trials searched */
+    int ndm;            /* DM trials */
+    int status;         /* PSX_OK or the failure */
+    int engine_reused;  /* 1 if a pooled instance was retargeted */
+} psx_request_stats;
+
+/* Starts max_active worker threads on `device`. */
+int psx_server_create(const psx_server_config* cfg, psx_server** out);
+/* Fails requests not yet admitted (PSX_ERR_BUSY), lets admitted ones
+   finish, and frees every instance. */
+int psx_server_destroy(psx_server* srv);
+/* Seconds since the server was created. */
+double psx_server_clock(psx_server* srv);
+
+/* Queues a search of ndm DM trials: series[d] holds nsamps floats (device
+   or host memory per series_on_device) and must stay valid until the
+   request completes; the config (birdies included) is copied.  Requests
+   are admitted first in, first out, when a worker is free and the new
+   instance they need fits the budget (a pooled instance with the same
+   shape is reused).  PSX_ERR_BUSY: queue full; PSX_ERR_ALLOC: larger than
+   the whole budget. */
+int psx_server_submit(psx_server* srv, const psx_search_config* cfg,
+                      const float* const* series, size_t nsamps,
+                      int series_on_device, const float* dms,
+                      const int* dm_idx, int ndm, long long* ticket);
+
+/* Waits up to timeout_s seconds (< 0: no limit) for a request and copies
+   its per-DM acceleration-distilled candidates in DM order (the output of
+   psx_search_block with PSX_OUT_DM), their association counts and DM
+   positions (h_nassoc, h_dm and stats may be NULL).  PSX_ERR_BUSY: still
+   running; PSX_ERR_OVERFLOW: *n_out is the need, call again.  The ticket
+   is released once its result (or failure) has been returned. */
+int psx_server_wait(psx_server* srv, long long ticket, double timeout_s,
+                    psx_candidate* h_out, int* h_nassoc, int* h_dm,
+                    size_t cap, size_t* n_out, psx_request_stats* stats);
+
+/* Bytes held, requests running, waiting, and pooled idle instances. */
+int psx_server_status(psx_server* srv, size_t* used_bytes, int* active,
+                      int* pending, int* pooled);
 
 #ifdef __cplusplus
 }

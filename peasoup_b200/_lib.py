@@ -66,7 +66,8 @@ class SearchInfo(C.Structure):
     _fields_ = [("ntrials", C.c_int), ("nbatches", C.c_int), ("kernel_launches", C.c_int),
                 ("fft_launches", C.c_int), ("above_threshold", C.c_longlong),
                 ("fft_callback", C.c_int), ("graph", C.c_int), ("batch", C.c_int),
-                ("baseline_passes", C.c_int), ("harm_shape", C.c_int)]
+                ("baseline_passes", C.c_int), ("harm_shape", C.c_int),
+                ("capture_fallbacks", C.c_int)]
 
 
 class SearchProfile(C.Structure):
@@ -74,6 +75,17 @@ class SearchProfile(C.Structure):
                 ("fft_ms", C.c_double), ("form_ms", C.c_double), ("harm_ms", C.c_double),
                 ("groups", C.c_longlong), ("trials", C.c_longlong), ("dms", C.c_longlong),
                 ("event_errors", C.c_longlong), ("last_event_error", C.c_int)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_active", C.c_int),
+                ("max_queue", C.c_int)]
+
+
+class RequestStats(C.Structure):
+    _fields_ = [("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("footprint", C.c_size_t), ("ntrials", C.c_longlong), ("ndm", C.c_int),
+                ("status", C.c_int), ("engine_reused", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -128,6 +140,16 @@ SIGNATURES = {
     "psx_search_get_profile": (_i, [_vp, C.POINTER(SearchProfile), _i]),
     "psx_search_debug_tap": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "psx_autotune": (_i, [C.POINTER(SearchConfig), _vp, _i, _i, _i, _vp]),
+    "psx_search_retarget": (_i, [_vp, C.POINTER(SearchConfig)]),
+    "psx_server_create": (_i, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
+    "psx_server_destroy": (_i, [_vp]),
+    "psx_server_clock": (C.c_double, [_vp]),
+    "psx_server_submit": (_i, [_vp, C.POINTER(SearchConfig), _vp, _sz, _i, _vp, _vp, _i,
+                               C.POINTER(C.c_longlong)]),
+    "psx_server_wait": (_i, [_vp, C.c_longlong, C.c_double, _vp, _vp, _vp, _sz, C.POINTER(_sz),
+                             C.POINTER(RequestStats)]),
+    "psx_server_status": (_i, [_vp, C.POINTER(_sz), C.POINTER(_i), C.POINTER(_i),
+                               C.POINTER(_i)]),
 }
 
 _lib = None

@@ -281,6 +281,7 @@ struct psx_search {
     float* d_mean = nullptr;
     float* d_bf = nullptr;
     float* d_bw = nullptr;
+    size_t bird_cap = 0;  // entries d_bf / d_bw hold
     double* d_kbatch = nullptr;
     float* h_mean = nullptr;
 
@@ -288,6 +289,7 @@ struct psx_search {
     FftPlan r2c1, c2r1;
     std::map<int, FftPlan*> r2cb;
     std::map<long long, GraphEntry> graphs;
+    std::map<long long, int> capture_failures;
 
     int last_slot = 0;
     bool profile = false;
@@ -556,6 +558,7 @@ int psx_search::run_trials(Slot& s, int nacc)
     if (!graph) return trials_enqueue(s, nacc);
     const long long key = ((long long)nacc << 2) | ((&s == &slot[1]) ? 2 : 0) | (s.profiled ? 1 : 0);
     auto it = graphs.find(key);
+    if (it == graphs.end() && capture_failures[key] >= 2) return trials_enqueue(s, nacc);
     if (it == graphs.end()) {
         // plans must exist before capture (creation allocates)
         for (int b = batch; b >= 1; b >>= 1) {
@@ -567,11 +570,20 @@ int psx_search::run_trials(Slot& s, int nacc)
         int rc = trials_enqueue(s, nacc);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(st, &g);
-        if (rc != PSX_OK) {
+        if (rc != PSX_OK || e != cudaSuccess) {
+            // A capture can be invalidated from outside this instance (in a
+            // multi-threaded host, e.g. by a kernel module loaded on first
+            // use while the capture is open).  Nothing captured has run:
+            // launch the same schedule directly and try capturing next time.
             if (g) cudaGraphDestroy(g);
-            return rc;
+            (void)cudaGetLastError();  // capture errors are not sticky
+            clear_error();
+            s.launches = l0;
+            s.ffts = f0;
+            ++info.capture_fallbacks;
+            ++capture_failures[key];  // after two, this schedule is not captured again
+            return trials_enqueue(s, nacc);
         }
-        PSX_CUDA(e);
         GraphEntry ge;
         e = cudaGraphInstantiate(&ge.exec, g, 0);
         cudaGraphDestroy(g);
@@ -897,15 +909,16 @@ size_t psx_search_footprint(const psx_search_config* c)
     return bytes;
 }
 
-int psx_search_create(const psx_search_config* cfg, psx_search** out)
+// Host-side state of an instance derived from its configuration: the
+// birdie list, transform sizes, tobs and bin width (floats, as at
+// pipeline_multi.cu:126-128), the search ranges of every fold
+// (peakfinder.hpp:123-128) and the fast-pass vote level.  Shared by
+// psx_search_create and psx_search_retarget.
+static void host_setup(psx_search* s, const psx_search_config* cfg)
 {
-    clear_error();
-    if (!out) return PSX_ERR_INVALID;
-    *out = nullptr;
-    PSX_TRY(check_config(cfg));
-    psx_search* s = new (std::nothrow) psx_search;
-    if (!s) return PSX_ERR_ALLOC;
     s->cfg = *cfg;
+    s->bf.clear();
+    s->bw.clear();
     if (cfg->nbirdies) {
         s->bf.assign(cfg->birdie_freqs, cfg->birdie_freqs + cfg->nbirdies);
         s->bw.assign(cfg->birdie_widths, cfg->birdie_widths + cfg->nbirdies);
@@ -948,6 +961,17 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->pk.hi = hi > lo ? hi : 0;
     s->pk.thresh = cfg->min_snr;
     s->pk.vote = cfg->min_snr - std::fabs(cfg->min_snr) * 0x1p-20f;
+}
+
+int psx_search_create(const psx_search_config* cfg, psx_search** out)
+{
+    clear_error();
+    if (!out) return PSX_ERR_INVALID;
+    *out = nullptr;
+    PSX_TRY(check_config(cfg));
+    psx_search* s = new (std::nothrow) psx_search;
+    if (!s) return PSX_ERR_ALLOC;
+    host_setup(s, cfg);
 
     int rc = PSX_OK;
     auto fail = [&](int code) {
@@ -985,6 +1009,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     if (!s->bf.empty()) {
         ALLOC(s->d_bf, sizeof(float) * s->bf.size());
         ALLOC(s->d_bw, sizeof(float) * s->bw.size());
+        s->bird_cap = s->bf.size();
     }
 #undef ALLOC
     if (cudaMallocHost(&s->h_mean, sizeof(float) * 4) != cudaSuccess) return fail(PSX_ERR_ALLOC);
@@ -1025,6 +1050,47 @@ int psx_search_destroy(psx_search* s)
     clear_error();
     if (!s) return PSX_OK;
     delete s;
+    return PSX_OK;
+}
+
+int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
+{
+    clear_error();
+    if (!s) {
+        set_error("search_retarget: null instance");
+        return PSX_ERR_INVALID;
+    }
+    PSX_TRY(check_config(cfg));
+    const int shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
+    const bool cb = cfg->mode == PSX_MODE_BATCHED && cfg->use_fft_callback;
+    if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
+        effective_batch(cfg) != s->batch || shape != s->harm_shape || cb != s->callback()) {
+        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape and callback "
+                  "must match the instance");
+        return PSX_ERR_INVALID;
+    }
+    PSX_CUDA(cudaSetDevice(s->device));
+    // work queued with the old parameters finishes first
+    PSX_CUDA(cudaStreamSynchronize(s->st));
+    PSX_CUDA(cudaStreamSynchronize(s->cst));
+    host_setup(s, cfg);
+    if (s->bf.size() > s->bird_cap) {
+        cudaFree(s->d_bf);
+        cudaFree(s->d_bw);
+        s->d_bf = s->d_bw = nullptr;
+        s->bird_cap = 0;
+        PSX_CUDA(cudaMalloc((void**)&s->d_bf, sizeof(float) * s->bf.size()));
+        PSX_CUDA(cudaMalloc((void**)&s->d_bw, sizeof(float) * s->bw.size()));
+        s->bird_cap = s->bf.size();
+    }
+    if (!s->bf.empty()) {
+        PSX_CUDA(cudaMemcpy(s->d_bf, s->bf.data(), sizeof(float) * s->bf.size(),
+                            cudaMemcpyHostToDevice));
+        PSX_CUDA(cudaMemcpy(s->d_bw, s->bw.data(), sizeof(float) * s->bw.size(),
+                            cudaMemcpyHostToDevice));
+    }
+    // captured schedules hold the old search ranges by value
+    s->drop_graphs();
     return PSX_OK;
 }
 

@@ -97,3 +97,17 @@ def test_zaplist_parsing(psx):
         os.unlink(path)
     assert psx.psx_read_zaplist(b"/nonexistent/zaplist", None, None, 0,
                                 C.byref(C.c_size_t())) == _lib.PSX_ERR_IO
+
+
+def test_server_needs_a_device(psx):
+    """Without a CUDA device the server refuses to start (no CPU fallback)."""
+    import ctypes as C
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from peasoup_b200._lib import PSX_ERR_CUDA, ServerConfig
+    cfg = ServerConfig(device=0, hbm_budget=1 << 30, max_active=2, max_queue=8)
+    h = C.c_void_p()
+    assert psx.psx_server_create(C.byref(cfg), C.byref(h)) == PSX_ERR_CUDA
+    bad = ServerConfig(device=0, hbm_budget=0, max_active=0, max_queue=0)
+    assert psx.psx_server_create(C.byref(bad), C.byref(h)) == 1

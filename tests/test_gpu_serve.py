@@ -1,0 +1,122 @@
+"""The served loop (psx_server, C++): requests of uneven transform length,
+DM count and acceleration range admitted as they arrive and searched
+concurrently.  Each result must be exactly what the same request gives
+alone, on a fresh search instance, and on a retargeted pooled instance."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1 << 16, 3 << 15, 1 << 17, 1 << 16, 3 << 16, 1 << 17]
+
+
+@pytest.fixture(scope="module")
+def M(cuda, psx):
+    from peasoup_b200 import search, serve, synth
+    return search, serve, synth
+
+
+def _requests(M):
+    search, serve, synth = M
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i, n in enumerate(SIZES):
+        ndm = 2 + i % 3
+        ts = 64e-6
+        xs = np.stack([synth.make_series_np(synth.SeriesSpec(
+            nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(float(rng.uniform(2e-3, 9e-3)),
+                                                      float(rng.uniform(-40, 40)), 0.05, 0.7)]),
+            100 * i + d) for d in range(ndm)])
+        acc = float(rng.uniform(20, 120))
+        p = search.SearchParams(fft_size=n, tsamp=ts, acc_lo=-acc, acc_hi=acc,
+                                nharmonics=3 + i % 3, min_snr=6.0, cfreq_hz=synth.CFREQ_HZ,
+                                ch_bw_hz=synth.CH_BW_HZ)
+        dms = (0.5 * np.arange(ndm)).astype(np.float32)
+        reqs.append((p, xs, dms))
+    return reqs
+
+
+def _alone(M, p, xs, dms):
+    search = M[0]
+    s = search.AccelSearch(p)
+    c, na, tr, dm = s.search_block(xs, dms)
+    s.close()
+    return c, na, dm
+
+
+def test_mixed_equals_alone(M):
+    search, serve, synth = M
+    import torch
+    reqs = _requests(M)
+    srv = serve.Server(40 << 30, max_active=3)
+    # half of the requests from device memory, half from host memory
+    tickets = []
+    for i, (p, xs, dms) in enumerate(reqs):
+        src = torch.from_numpy(xs).cuda() if i % 2 else xs
+        tickets.append(srv.submit(p, src, dms))
+    got = [srv.wait(t) for t in tickets]
+    st = srv.status()
+    assert st["active"] == 0 and st["pending"] == 0 and st["pooled"] >= 1
+    srv.close()
+    for (p, xs, dms), (c, na, dm, stats) in zip(reqs, got):
+        assert stats["status"] == 0 and stats["ndm"] == len(dms) and stats["ntrials"] > 0
+        assert stats["t_submit"] <= stats["t_admit"] <= stats["t_done"]
+        ac, ana, adm = _alone(M, p, xs, dms)
+        assert len(c) > 0
+        assert np.array_equal(c, ac) and np.array_equal(na, ana) and np.array_equal(dm, adm)
+
+
+def test_pooled_instance_is_retargeted(M):
+    """Two requests with the same instance shape but different acceleration
+    ranges, tsamp-derived limits and birdies: the second reuses the pooled
+    instance and must still equal a fresh instance's result."""
+    search, serve, synth = M
+    import dataclasses
+    reqs = _requests(M)
+    p, xs, dms = reqs[0]
+    p2 = dataclasses.replace(p, acc_lo=-75.0, acc_hi=60.0, min_snr=5.5, max_freq=900.0,
+                             birdie_freqs=np.array([50.0, 120.0], np.float32),
+                             birdie_widths=np.array([0.3, 0.5], np.float32))
+    srv = serve.Server(40 << 30, max_active=1)
+    c1, _, _, s1 = srv.wait(srv.submit(p, xs, dms))
+    c2, na2, dm2, s2 = srv.wait(srv.submit(p2, xs, dms))
+    srv.close()
+    assert s1["engine_reused"] == 0 and s1["footprint"] > 0
+    assert s2["engine_reused"] == 1 and s2["footprint"] == 0
+    a2, ana2, adm2 = _alone(M, p2, xs, dms)
+    assert np.array_equal(c2, a2) and np.array_equal(na2, ana2)
+    assert np.array_equal(c1, _alone(M, p, xs, dms)[0])
+
+
+def test_admission_limits(M):
+    search, serve, synth = M
+    from peasoup_b200 import _lib
+    from peasoup_b200._lib import PsxError
+    reqs = _requests(M)
+    p, xs, dms = reqs[2]
+    need = search.footprint(p)
+    # larger than the whole budget: refused at submission
+    srv = serve.Server(need // 2, max_active=1)
+    with pytest.raises(PsxError) as e:
+        srv.submit(p, xs, dms)
+    assert e.value.status == _lib.PSX_ERR_ALLOC
+    srv.close()
+    # one slot, a queue of one: a burst of four must see the queue full
+    srv = serve.Server(need * 2, max_active=1, max_queue=1)
+    ok, busy = [], 0
+    for _ in range(4):
+        try:
+            ok.append(srv.submit(p, xs, dms))
+        except PsxError as ex:
+            assert ex.status == _lib.PSX_ERR_BUSY
+            busy += 1
+    assert busy >= 1 and len(ok) >= 1
+    first = None
+    for t in ok:
+        c, na, dm, st = srv.wait(t)
+        assert st["status"] == 0
+        first = c if first is None else first
+        assert np.array_equal(c, first)
+    srv.close()
