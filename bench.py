@@ -373,6 +373,194 @@ def run_served(nreq, rank, log_prefix):
                      f"half-range 10..300, 3..5 folds, white noise + one pulsar per DM"),
     }
 
+
+# ----------------------------------------------------------------- configs 3, 5
+def _pulse_block_torch(ndm, n, ts, seed, pulsar=(5.7e-3, 12.0, 0.05, 0.3), sigma=1.0):
+    """White N(0, sigma^2) noise plus one accelerated Gaussian pulse train
+    per row (the small benchmark's statistics), made on the GPU."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    out = torch.empty((ndm, n), dtype=torch.float32, device="cuda")
+    i = torch.arange(n, device="cuda", dtype=torch.float64)
+    P, acc, duty, amp = pulsar
+    k = acc * ts / (2.0 * 299792458.0)
+    phi = (i - k * i * (i - n)) * (ts / P)
+    dd = phi - torch.round(phi)
+    sig = duty / (2.0 * np.sqrt(2.0 * np.log(2.0)))
+    pulse = (amp * sigma * torch.exp(-0.5 * (dd / sig) ** 2)).float()
+    del i, phi, dd
+    for r in range(ndm):
+        out[r] = sigma * torch.randn(n, generator=g, device="cuda") + pulse
+    return out
+
+
+def _timed_block(eng, rows, dms, stream, chunk):
+    """Searches rows in chunks through psx_search_block; CUDA-event time on
+    the engine's stream.  Returns (seconds, candidate arrays per chunk)."""
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = []
+    for c0 in range(0, len(rows), chunk):
+        idx = np.arange(c0, min(len(rows), c0 + chunk))
+        outs.append(eng.search_block([rows[i] for i in idx], dms[idx], idx.astype(np.int32))[0])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, outs
+
+
+def run_config3(args):
+    """2048 DM trials x 2^22 samples of the small benchmark's statistics,
+    acc +-50, 4 folds, S/N 7: batched (autotuned) over every DM trial, plain
+    on a sample, and the candidate sets of the sampled DM trials compared."""
+    import torch
+    from peasoup_b200 import search, synth
+    from peasoup_b200.build import build
+    from peasoup_b200.transforms import AccelerationPlan
+    build()
+    n, ts, ndm = 1 << 22, 64e-6, args.ndm or 2048
+    t0 = time.perf_counter()
+    block = _pulse_block_torch(ndm, n, ts, seed=3)
+    torch.cuda.synchronize()
+    log(f"config 3: synthesised {ndm} series in {time.perf_counter() - t0:.1f}s")
+    dms = (0.5 * np.arange(ndm)).astype(np.float32)
+
+    def params(mode, batch=0, shape=0):
+        return search.SearchParams(fft_size=n, tsamp=ts, acc_lo=-50.0, acc_hi=50.0,
+                                   nharmonics=4, min_snr=7.0, cfreq_hz=synth.CFREQ_HZ,
+                                   ch_bw_hz=synth.CH_BW_HZ, mode=mode, batch=batch,
+                                   harm_shape=shape)
+    tune = search.autotune(params("batched"), batches=(2, 4, 8, 16), reps=4)
+    ap = AccelerationPlan(-50.0, 50.0, 1.10, 64e-6, n, ts, synth.CFREQ_HZ, synth.CH_BW_HZ)
+    ntr = [len(ap.generate_accel_list(float(d), 0.0)) for d in dms]
+    stream = torch.cuda.Stream()
+    eng = search.AccelSearch(params("batched", tune["batch"], tune["harm_shape"]))
+    eng.set_stream(stream.cuda_stream)
+    rows = [block[i] for i in range(ndm)]
+    _timed_block(eng, rows[:16], dms[:16], stream, 16)          # warm-up
+    with ClockSampler(0) as clk:
+        tb, outs_b = _timed_block(eng, rows, dms, stream, 64)
+    clocks = clk.summary()
+    nsample = min(ndm, args.plain_sample)
+    sel = np.linspace(0, ndm - 1, nsample).astype(int)
+    engp = search.AccelSearch(params("plain"))
+    engp.set_stream(stream.cuda_stream)
+    _timed_block(engp, [rows[i] for i in sel[:2]], dms[sel[:2]], stream, 2)
+    tp, outs_p = _timed_block(engp, [rows[i] for i in sel], dms[sel], stream, 64)
+    # candidate sets of the sampled DM trials: plain vs batched
+    cb = np.concatenate(outs_b)
+    cp = np.concatenate(outs_p)
+    bsel = cb[np.isin(cb["dm_idx"], sel)]
+    cp_fixed = cp.copy()
+    cp_fixed["dm_idx"] = sel[cp["dm_idx"]]          # plain ran on a subset: map back
+    cp_fixed["dm"] = dms[cp_fixed["dm_idx"]]
+    key = lambda c: (int(c["dm_idx"]), float(c["acc"]), int(c["nh"]), float(c["freq"]))
+    kb = {key(c): float(c["snr"]) for c in bsel}
+    kp = {key(c): float(c["snr"]) for c in cp_fixed}
+    same = set(kb) == set(kp)
+    worst = max([abs(kb[k] - kp[k]) / max(abs(kp[k]), 1e-30) for k in set(kb) & set(kp)] or [0])
+    tot_b = sum(ntr)
+    tot_p = sum(ntr[i] for i in sel)
+    vb, vp = tot_b / tb, tot_p / tp
+    eng.close()
+    engp.close()
+    print(json.dumps({
+        "metric": "DM x accel trials/s, config 3 (2048 DM x 2^22)", "config_id": 3,
+        "value": vb, "unit": "trials/s", "higher_is_better": True,
+        "batched": {"value": vb, "seconds": tb, "dm_trials": ndm, "trials": tot_b,
+                    "batch": tune["batch"], "harm_shape": tune["harm_shape"]},
+        "plain": {"value": vp, "seconds": tp, "dm_trials": int(nsample), "trials": tot_p},
+        "batched_over_plain": vb / vp,
+        "candidate_sets_equal_on_plain_sample": bool(same),
+        "candidates_compared": len(kp), "snr_worst_rel": worst,
+        "hbm_roofline_frac": (ndm * 24.0 * n + tot_b * 12.0 * n) / tb / (peaks()[0] * 1e9),
+        "clocks": clocks,
+        "workload": "2048 DM x 2^22, tsamp 64us, white N(0,1) + P=5.7ms 5% duty 0.3 sigma "
+                    "pulsar at +12 m/s^2 in every row, acc -50..50 (15 trials at DM 0), "
+                    "4 folds, S/N 7, no zap list; series resident on the GPU",
+    }), flush=True)
+    return 0
+
+
+def run_config5(args):
+    """2^27 samples, 64 DM trials, acc +-500 (123,653 trials at DM 0), 5
+    folds: a fixed subset timed and extrapolated.  Per-trial and per-DM
+    costs come from two subsets of different trial counts on the same DM
+    trials (narrowed acceleration ranges; the cost of a trial does not depend
+    on its acceleration)."""
+    import torch
+    from peasoup_b200 import search, synth
+    from peasoup_b200.build import build
+    from peasoup_b200.transforms import AccelerationPlan
+    build()
+    n, ts, ndm = 1 << 27, 64e-6, 64
+    nuse = args.ndm or 4
+    plan = synth.survey_plan(ndm=ndm, nsamps=n, tsamp=ts, seed=5, npulsars=3, nbirdies=0)
+    rng = np.random.default_rng(5)
+    for p in plan.pulsars:
+        p.accel = float(rng.uniform(-400.0, 400.0))
+    dsel = list(range(nuse))
+    t0 = time.perf_counter()
+    block = synth.survey_block_torch(plan, dm_indices=dsel, chunk=1)
+    torch.cuda.synchronize()
+    log(f"config 5: synthesised {nuse} series of 2^27 in {time.perf_counter() - t0:.1f}s")
+    ap = AccelerationPlan(-500.0, 500.0, 1.10, 64e-6, n, ts, synth.CFREQ_HZ, synth.CH_BW_HZ)
+    full = [len(ap.generate_accel_list(float(d), 0.0)) for d in plan.dms]
+
+    def params(mode, half, batch=0, shape=0):
+        return search.SearchParams(fft_size=n, tsamp=ts, acc_lo=-half, acc_hi=half,
+                                   nharmonics=5, min_snr=9.0, cfreq_hz=synth.CFREQ_HZ,
+                                   ch_bw_hz=synth.CH_BW_HZ, mode=mode, batch=batch,
+                                   harm_shape=shape)
+
+    def ntrials(half, dlist):
+        a = AccelerationPlan(-half, half, 1.10, 64e-6, n, ts, synth.CFREQ_HZ, synth.CH_BW_HZ)
+        return sum(len(a.generate_accel_list(float(plan.dms[d]), 0.0)) for d in dlist)
+
+    tune = search.autotune(params("batched", 500.0), batches=(2, 4, 8, 16), reps=1,
+                           max_trials=64)
+    stream = torch.cuda.Stream()
+    rows = [block[i] for i in range(nuse)]
+    res = {}
+    for mode, halves in (("batched", (0.5, 2.0)), ("plain", (0.25, 1.0))):
+        fit = []
+        for half in halves:
+            eng = search.AccelSearch(params(mode, half, tune["batch"] if mode == "batched" else 0,
+                                            tune["harm_shape"]))
+            eng.set_stream(stream.cuda_stream)
+            _timed_block(eng, rows[:1], plan.dms[:1], stream, 1)   # warm-up
+            sec, _ = _timed_block(eng, rows, plan.dms[dsel], stream, nuse)
+            fit.append((ntrials(half, dsel), sec))
+            eng.close()
+        (n1, s1), (n2, s2) = fit
+        per_trial = (s2 - s1) / (n2 - n1)
+        per_dm = max(0.0, (s1 - n1 * per_trial) / nuse)
+        tot = sum(full)
+        est = ndm * per_dm + tot * per_trial
+        res[mode] = {"value": tot / est, "per_trial_us": 1e6 * per_trial,
+                     "per_dm_ms": 1e3 * per_dm, "subset": [{"trials": a, "seconds": b}
+                                                           for a, b in fit]}
+    print(json.dumps({
+        "metric": "DM x accel trials/s, config 5 (2^27, 64 DM, acc +-500), extrapolated",
+        "config_id": 5, "value": res["batched"]["value"], "unit": "trials/s",
+        "higher_is_better": True, "batched": res["batched"], "plain": res["plain"],
+        "batched_over_plain": res["batched"]["value"] / res["plain"]["value"],
+        "trials_full": int(sum(full)), "trials_dm0": full[0],
+        "batch": tune["batch"], "harm_shape": tune["harm_shape"],
+        "hbm_roofline_frac": ((24.0 * n * ndm + 12.0 * n * sum(full)) /
+                              (ndm * res["batched"]["per_dm_ms"] / 1e3 +
+                               sum(full) * res["batched"]["per_trial_us"] / 1e6) /
+                              (peaks()[0] * 1e9)),
+        "workload": f"2^27 x tsamp 64us, survey-shape red noise + 3 binary pulsars "
+                    f"(|a| <= 400), 64 DM trials (0.5 steps), acc -500..500, 5 folds, S/N 9; "
+                    f"timed on {nuse} DM trials with narrowed acceleration ranges "
+                    f"(batched +-0.5 and +-2, plain +-0.25 and +-1 m/s^2) and extrapolated "
+                    f"to the full {sum(full)} trials",
+    }), flush=True)
+    return 0
+
 # ----------------------------------------------------------------- main arm
 def run_psx(args, ws, rank, local):
     import torch
@@ -599,12 +787,22 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--served", type=int, default=SERVED_REQUESTS,
                     help="requests of the served workload (0: skip)")
+    ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
+                    help="2: the headline survey workload; 3 and 5: the other throughput "
+                         "configurations (one JSON line each)")
+    ap.add_argument("--ndm", type=int, default=0, help="configs 3/5: DM trials to time")
+    ap.add_argument("--plain-sample", type=int, default=128,
+                    help="config 3: DM trials searched by the plain path")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_init()
     try:
         if args.impl == "reference":
             rc = run_reference(args, ws, rank)
+        elif args.config == 3:
+            rc = run_config3(args)
+        elif args.config == 5:
+            rc = run_config5(args)
         else:
             rc = run_psx(args, ws, rank, local)
     finally:
