@@ -395,7 +395,144 @@ struct InterbinSrc {
     }
 };
 
+// Block sum of (a, b) pairs into partials[blockIdx.x] (fixed order).
+template <int NT>
+__device__ __forceinline__ void block_partials(double s, double s2, double2* __restrict__ partials)
+{
+    for (int o = 16; o; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    __shared__ double sh[2][NT / 32];
+    const int w = threadIdx.x / 32;
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][w] = s;
+        sh[1][w] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < NT / 32; ++i) {
+            a += sh[0][i];
+            b += sh[1][i];
+        }
+        partials[blockIdx.x] = make_double2(a, b);
+    }
+}
+
+__device__ __forceinline__ void acc4(float4 v, double& s, double& s2)
+{
+    const double a = v.x, b = v.y, c = v.z, d = v.w;
+    s += (a + b) + (c + d);
+    s2 += (a * a + b * b) + (c * c + d * d);
+}
+
+constexpr int kVecThreads = 512;
+
+// Partial sums of x and x^2 over [0, n) with 128-bit loads (x 16-byte
+// aligned); the n % 4 tail is added by block 0.
+__global__ void __launch_bounds__(kVecThreads) k_partials_v4(const float* __restrict__ x, size_t n,
+                                                             double2* __restrict__ partials)
+{
+    double s = 0.0, s2 = 0.0;
+    const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride)
+        acc4(x4[q], s, s2);
+    if (blockIdx.x == 0 && threadIdx.x < n - 4 * n4) {
+        const double v = x[4 * n4 + threadIdx.x];
+        s += v;
+        s2 += v * v;
+    }
+    block_partials<kVecThreads>(s, s2, partials);
+}
+
+// One pass of the baseline loop after the mean is known: x -= *mean and,
+// while state[0] says the loop goes on, the partial sums of the new x.  A
+// zero mean (an inactive pass, k_baseline_step writes 0) leaves x as it is
+// and the kernel returns at once.
+__global__ void __launch_bounds__(kVecThreads) k_sub_partials_v4(float* __restrict__ x, size_t n,
+                                                                 const float* __restrict__ mean,
+                                                                 double2* __restrict__ partials,
+                                                                 const unsigned* __restrict__ state)
+{
+    const float m = *mean;
+    if (m == 0.0f) return;
+    const bool sum = state[0] != 0u;
+    double s = 0.0, s2 = 0.0;
+    const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+    float4* x4 = reinterpret_cast<float4*>(x);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+        float4 v = x4[q];
+        v.x -= m;
+        v.y -= m;
+        v.z -= m;
+        v.w -= m;
+        x4[q] = v;
+        if (sum) acc4(v, s, s2);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < n - 4 * n4) {
+        const float v = x[4 * n4 + threadIdx.x] - m;
+        x[4 * n4 + threadIdx.x] = v;
+        s += (double)v;
+        s2 += (double)v * v;
+    }
+    if (sum) block_partials<kVecThreads>(s, s2, partials);
+}
+
+// Partial sums of the interbinned amplitude of the complex spectrum X over
+// bins [0, nbins): two bins per thread from one 128-bit load, the previous
+// bin's pair from a 64-bit load; the odd last bin is added by block 0.
+__global__ void __launch_bounds__(kVecThreads) k_interbin_partials_v4(const float* __restrict__ X,
+                                                                      size_t nbins,
+                                                                      double2* __restrict__ partials)
+{
+    double s = 0.0, s2 = 0.0;
+    const size_t npairs = nbins / 2, stride = (size_t)gridDim.x * blockDim.x;
+    const float4* X4 = reinterpret_cast<const float4*>(X);
+    const float2* X2 = reinterpret_cast<const float2*>(X);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += stride) {
+        const float4 v = X4[q];
+        const float2 l = q ? X2[2 * q - 1] : make_float2(0.f, 0.f);
+        const double a = interbin(v.x, v.y, l.x, l.y);
+        const double b = interbin(v.z, v.w, v.x, v.y);
+        s += a + b;
+        s2 += a * a + b * b;
+    }
+    if ((nbins & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const size_t k = nbins - 1;
+        const float2 l = k ? X2[k - 1] : make_float2(0.f, 0.f);
+        const double a = interbin(X[2 * k], X[2 * k + 1], l.x, l.y);
+        s += a;
+        s2 += a * a;
+    }
+    block_partials<kVecThreads>(s, s2, partials);
+}
+
 int reduction_blocks() { return sm_count() * 2; }
+
+int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, cudaStream_t s)
+{
+    k_partials_v4<<<reduction_blocks(), kVecThreads, 0, s>>>(d_x, n, d_partials);
+    return launch_status("partial sums kernel");
+}
+
+int launch_sub_partials_v4(float* d_x, size_t n, const float* d_mean, double2* d_partials,
+                           const unsigned* d_state, cudaStream_t s)
+{
+    k_sub_partials_v4<<<reduction_blocks(), kVecThreads, 0, s>>>(d_x, n, d_mean, d_partials,
+                                                                 d_state);
+    return launch_status("baseline subtract kernel");
+}
+
+int launch_interbin_stats_v4(const float* d_X, size_t nbins, double2* d_partials, double* d_sums,
+                             float* d_stat, float scale, cudaStream_t s)
+{
+    const int nb = reduction_blocks();
+    k_interbin_partials_v4<<<nb, kVecThreads, 0, s>>>(d_X, nbins, d_partials);
+    k_finish_stats<<<1, 32, 0, s>>>(d_partials, nb, (double)nbins, d_sums, d_stat, scale);
+    return launch_status("interbin statistics kernels");
+}
 
 int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_t s)
 {

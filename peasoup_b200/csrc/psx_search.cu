@@ -439,13 +439,16 @@ int psx_search::prologue(Slot& s)
     // src/kernels.cu:463-479)
     const int nb = reduction_blocks();
     if (!s.host_baseline) {
+        // sums of the series, then per pass: the mean (k_baseline_step)
+        // and one fused subtract + re-sum; passes after convergence return
+        // at once
         k_baseline_reset<<<1, 1, 0, st>>>(s.d_count + 2);
-        ++s.launches;
+        PSX_TRY(launch_partials_v4(d_tim, ncopy, d_part, st));
+        s.launches += 2;
         for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
-            PSX_TRY(launch_partials(d_tim, ncopy, d_part, st));
             k_baseline_step<<<1, 32, 0, st>>>(d_part, nb, (double)ncopy, d_mean, s.d_count + 2);
-            PSX_TRY(launch_sub_scalar(d_tim, ncopy, d_mean, st));
-            s.launches += 3;
+            PSX_TRY(launch_sub_partials_v4(d_tim, ncopy, d_mean, d_part, s.d_count + 2, st));
+            s.launches += 2;
         }
     } else {
         int count = 0;
@@ -478,7 +481,7 @@ int psx_search::prologue(Slot& s)
         ++s.launches;
     }
     // interbin statistics (pipeline_multi.cu:230-234) -> mean*N, std*N
-    PSX_TRY(launch_stats(d_X, true, 0, B, d_part, d_sums, d_stat, (float)N, st));
+    PSX_TRY(launch_interbin_stats_v4(d_X, B, d_part, d_sums, d_stat, (float)N, st));
     s.launches += 2;
     PSX_TRY(c2r1.exec(d_X, d_tim, st));
     ++s.ffts;

@@ -40,6 +40,18 @@ int launch_fill(float* d_x, size_t n, float value, cudaStream_t s);
 // Per-block partial sums of x and x^2 over [0, n) (reduction_blocks() of them).
 int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_t s);
 
+// The same with 128-bit loads (d_x 16-byte aligned).
+int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, cudaStream_t s);
+
+// One baseline pass: x -= *d_mean (nothing when it is 0) and, while
+// d_state[0] is set, the partial sums of the new x.
+int launch_sub_partials_v4(float* d_x, size_t n, const float* d_mean, double2* d_partials,
+                           const unsigned* d_state, cudaStream_t s);
+
+// launch_stats(interbinned, first = 0) with 128-bit loads (d_X 16-byte aligned).
+int launch_interbin_stats_v4(const float* d_X, size_t nbins, double2* d_partials, double* d_sums,
+                             float* d_stat, float scale, cudaStream_t s);
+
 // x[i] -= *d_v.
 int launch_sub_scalar(float* d_x, size_t n, const float* d_v, cudaStream_t s);
 
