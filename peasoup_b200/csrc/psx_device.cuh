@@ -124,4 +124,26 @@ __device__ __forceinline__ unsigned frac_index(unsigned i, unsigned m)
     return (unsigned)(((unsigned long long)i * m + (1u << (H - 1))) >> H);
 }
 
+// Sum of `nparts` partials by one warp in a fixed order (lane j adds
+// partials j, j+32, ... in turn, then a fixed shuffle tree): deterministic,
+// and ~30x shorter than one thread walking the array.  Every lane of the
+// warp must call it; all receive the totals.
+__device__ __forceinline__ void warp_sum_partials(const double2* __restrict__ partials,
+                                                  int nparts, double& a, double& b)
+{
+    const int lane = threadIdx.x & 31;
+    double sa = 0.0, sb = 0.0;
+    for (int i = lane; i < nparts; i += 32) {
+        const double2 v = partials[i];
+        sa += v.x;
+        sb += v.y;
+    }
+    for (int o = 16; o; o >>= 1) {
+        sa += __shfl_down_sync(0xffffffffu, sa, o);
+        sb += __shfl_down_sync(0xffffffffu, sb, o);
+    }
+    a = __shfl_sync(0xffffffffu, sa, 0);
+    b = __shfl_sync(0xffffffffu, sb, 0);
+}
+
 }  // namespace psx

@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(256) k_sum_partials(Src src, size_t first, siz
     }
 }
 
-// Adds `nparts` partials in fixed order; writes the totals to sums[0..1]
+// Adds `nparts` partials (one warp, fixed order); writes the totals to sums[0..1]
 // and, when stat != nullptr, the reference's float statistics
 // {mean, rms, std, mean*scale, std*scale} computed exactly as its host
 // code does (stats.hpp:160-173 and src/kernels.cu:443,458), without
@@ -359,12 +359,10 @@ __global__ void __launch_bounds__(256) k_sum_partials(Src src, size_t first, siz
 __global__ void k_finish_stats(const double2* __restrict__ partials, int nparts, double count,
                                double* __restrict__ sums, float* __restrict__ stat, float scale)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double a = 0.0, b = 0.0;
-    for (int i = 0; i < nparts; ++i) {
-        a += partials[i].x;
-        b += partials[i].y;
-    }
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    double a, b;
+    warp_sum_partials(partials, nparts, a, b);
+    if (threadIdx.x != 0) return;
     sums[0] = a;
     sums[1] = b;
     if (stat) {
@@ -430,19 +428,33 @@ __device__ __forceinline__ void acc4(float4 v, double& s, double& s2)
 constexpr int kVecThreads = 512;
 
 // Partial sums of x and x^2 over [0, n) with 128-bit loads (x 16-byte
-// aligned); the n % 4 tail is added by block 0.
+// aligned); the n % 4 tail is added by block 0.  With `copy` set, x is also
+// written there (16-byte aligned), fusing the copy of a series into its
+// first pass; with `state` set, block 0 starts the baseline loop state
+// (state[0] = 1 active, state[1] = 0 passes).
 __global__ void __launch_bounds__(kVecThreads) k_partials_v4(const float* __restrict__ x, size_t n,
-                                                             double2* __restrict__ partials)
+                                                             double2* __restrict__ partials,
+                                                             float* __restrict__ copy,
+                                                             unsigned* __restrict__ state)
 {
+    if (state && blockIdx.x == 0 && threadIdx.x == 0) {
+        state[0] = 1u;
+        state[1] = 0u;
+    }
     double s = 0.0, s2 = 0.0;
     const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
     const float4* x4 = reinterpret_cast<const float4*>(x);
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride)
-        acc4(x4[q], s, s2);
+    float4* c4 = reinterpret_cast<float4*>(copy);
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += stride) {
+        const float4 v = x4[q];
+        if (copy) c4[q] = v;
+        acc4(v, s, s2);
+    }
     if (blockIdx.x == 0 && threadIdx.x < n - 4 * n4) {
-        const double v = x[4 * n4 + threadIdx.x];
-        s += v;
-        s2 += v * v;
+        const float v = x[4 * n4 + threadIdx.x];
+        if (copy) copy[4 * n4 + threadIdx.x] = v;
+        s += (double)v;
+        s2 += (double)v * v;
     }
     block_partials<kVecThreads>(s, s2, partials);
 }
@@ -511,9 +523,10 @@ __global__ void __launch_bounds__(kVecThreads) k_interbin_partials_v4(const floa
 
 int reduction_blocks() { return sm_count() * 2; }
 
-int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, cudaStream_t s)
+int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, float* d_copy,
+                       unsigned* d_state, cudaStream_t s)
 {
-    k_partials_v4<<<reduction_blocks(), kVecThreads, 0, s>>>(d_x, n, d_partials);
+    k_partials_v4<<<reduction_blocks(), kVecThreads, 0, s>>>(d_x, n, d_partials, d_copy, d_state);
     return launch_status("partial sums kernel");
 }
 

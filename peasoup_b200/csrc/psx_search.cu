@@ -78,9 +78,10 @@ __global__ void __launch_bounds__(256) k_form_norm(const float* __restrict__ X, 
 __global__ void k_baseline_step(const double2* __restrict__ partials, int nparts, double count,
                                 float* __restrict__ mean_out, unsigned* __restrict__ state)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double a = 0.0;
-    for (int i = 0; i < nparts; ++i) a += partials[i].x;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    double a, b;
+    warp_sum_partials(partials, nparts, a, b);
+    if (threadIdx.x != 0) return;
     const float mean = __fdiv_rn((float)a, (float)count);
     if (state[0]) {
         *mean_out = mean;
@@ -89,12 +90,6 @@ __global__ void k_baseline_step(const double2* __restrict__ partials, int nparts
     } else {
         *mean_out = 0.0f;
     }
-}
-
-__global__ void k_baseline_reset(unsigned* __restrict__ state)
-{
-    state[0] = 1u;
-    state[1] = 0u;
 }
 
 // Fused harmonic sums + threshold + compaction: tile shapes and launcher.
@@ -433,8 +428,13 @@ int psx_search::ensure_events(Slot& s, int groups)
 int psx_search::prologue(Slot& s)
 {
     const size_t ncopy = std::min(s.nsamps, N);
-    PSX_CUDA(cudaMemcpyAsync(d_tim, s.series, sizeof(float) * ncopy,
-                             s.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    // a device series 16-byte aligned is copied by the first baseline pass
+    const bool fused_copy =
+        s.on_device && !s.host_baseline && (reinterpret_cast<uintptr_t>(s.series) & 15u) == 0;
+    if (!fused_copy)
+        PSX_CUDA(cudaMemcpyAsync(d_tim, s.series, sizeof(float) * ncopy,
+                                 s.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 st));
     // baseline removal over the copied samples (timeseries.hpp:282-287,
     // src/kernels.cu:463-479)
     const int nb = reduction_blocks();
@@ -442,9 +442,11 @@ int psx_search::prologue(Slot& s)
         // sums of the series, then per pass: the mean (k_baseline_step)
         // and one fused subtract + re-sum; passes after convergence return
         // at once
-        k_baseline_reset<<<1, 1, 0, st>>>(s.d_count + 2);
-        PSX_TRY(launch_partials_v4(d_tim, ncopy, d_part, st));
-        s.launches += 2;
+        if (fused_copy)
+            PSX_TRY(launch_partials_v4(s.series, ncopy, d_part, d_tim, s.d_count + 2, st));
+        else
+            PSX_TRY(launch_partials_v4(d_tim, ncopy, d_part, nullptr, s.d_count + 2, st));
+        ++s.launches;
         for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
             k_baseline_step<<<1, 32, 0, st>>>(d_part, nb, (double)ncopy, d_mean, s.d_count + 2);
             PSX_TRY(launch_sub_partials_v4(d_tim, ncopy, d_mean, d_part, s.d_count + 2, st));

@@ -40,8 +40,10 @@ int launch_fill(float* d_x, size_t n, float value, cudaStream_t s);
 // Per-block partial sums of x and x^2 over [0, n) (reduction_blocks() of them).
 int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_t s);
 
-// The same with 128-bit loads (d_x 16-byte aligned).
-int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, cudaStream_t s);
+// The same with 128-bit loads (d_x 16-byte aligned); with d_copy set, x is
+// also copied there; with d_state set, the baseline loop state is started.
+int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, float* d_copy,
+                       unsigned* d_state, cudaStream_t s);
 
 // One baseline pass: x -= *d_mean (nothing when it is 0) and, while
 // d_state[0] is set, the partial sums of the new x.
