@@ -250,29 +250,61 @@ def run_reference(args, ws, rank):
 
 
 # ----------------------------------------------------------------- CPU baseline
+def _oracle_params(plan, dm, lo, hi):
+    from peasoup_b200 import synth
+    return dict(fft_size=N_FFT, tsamp=TSAMP, dm=float(dm), acc_lo=lo, acc_hi=hi,
+                nharmonics=NFOLDS, cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ,
+                birdie_freqs=np.asarray(plan.birdie_freqs), birdie_widths=np.asarray(plan.birdie_widths))
+
+
+def _oracle_init():
+    from oracle import oracle as O
+    O.lib()
+
+
+def _oracle_job(job):
+    """One oracle DM search (run in a spawned worker); its own elapsed time."""
+    x, kw = job
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    O.search_dm(x, O.SearchParams(**kw))
+    return time.perf_counter() - t0
+
+
+def _cpu_workers():
+    """Host threads for the parallel sample: every core, bounded by memory
+    (about 1.5 GB per FP64 2^23 search) and by 32."""
+    n = os.cpu_count() or 1
+    try:
+        with open("/proc/meminfo") as f:
+            avail = next(int(l.split()[1]) for l in f if l.startswith("MemAvailable")) * 1024
+        n = min(n, max(1, int(avail // 1.5e9)))
+    except (OSError, StopIteration, ValueError):
+        pass
+    return max(1, min(n, 32))
+
+
 def cpu_baseline(plan, block_row, dm):
     """FP64 oracle on a bounded sample: one DM trial with 1 and with 3
-    acceleration trials; per-trial and per-DM costs are separated and the
-    throughput extrapolated to the workload's trials per DM."""
-    from oracle import oracle as O
-    from peasoup_b200 import synth
-    x = block_row
-
-    def run(lo, hi):
-        p = O.SearchParams(fft_size=N_FFT, tsamp=TSAMP, dm=float(dm), acc_lo=lo, acc_hi=hi,
-                           nharmonics=NFOLDS, cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ,
-                           birdie_freqs=plan.birdie_freqs, birdie_widths=plan.birdie_widths)
-        t0 = time.perf_counter()
-        O.search_dm(x, p)
-        return time.perf_counter() - t0
-
-    t1 = run(0.0, 0.0)
-    t3 = run(-1.0, 1.0)      # {-1, 0, 1}: three trials
+    acceleration trials on one core separates the per-trial and per-DM
+    costs; the 3-trial search run on every worker at once (spawned
+    processes, one per core) gives the parallel efficiency.  Throughput is
+    extrapolated to the workload's trials per DM."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    x = np.ascontiguousarray(block_row, np.float32)
+    t1 = _oracle_job((x, _oracle_params(plan, dm, 0.0, 0.0)))
+    t3 = _oracle_job((x, _oracle_params(plan, dm, -1.0, 1.0)))   # {-1, 0, 1}: three trials
     per_trial = max(1e-9, (t3 - t1) / 2.0)
     per_dm = max(0.0, t1 - per_trial)
-    return per_trial, per_dm, t1 + t3
-
-
+    cores = _cpu_workers()
+    par = [t3]
+    if cores > 1:
+        with ProcessPoolExecutor(cores, mp_context=mp.get_context("spawn"),
+                                 initializer=_oracle_init) as ex:
+            par = list(ex.map(_oracle_job, [(x, _oracle_params(plan, dm, -1.0, 1.0))] * cores))
+    eff = t3 / (sum(par) / len(par))
+    return per_trial, per_dm, cores, eff, t1 + t3 + max(par)
 
 # ----------------------------------------------------------------- served
 def _pct(v, q):
@@ -734,14 +766,17 @@ def run_psx(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu:
         d0 = timed[0][0]
         x = block[row[d0]].cpu().numpy()
-        per_trial, per_dm, spent = cpu_baseline(plan, x, plan.dms[d0])
+        per_trial, per_dm, cores, eff, spent = cpu_baseline(plan, x, plan.dms[d0])
         avg_trials = ntr / max(1, sum(len(st) for st in timed))
-        cpu_v = avg_trials / (per_dm + avg_trials * per_trial)
-        cpu = {"value": cpu_v, "unit": "trials/s", "cores": 1, "kind": "port",
-               "sample": (f"FP64 oracle, one 2^23 DM trial with 1 and with 3 acceleration "
-                          f"trials ({spent:.1f}s): {per_trial:.2f}s per trial, "
-                          f"{per_dm:.2f}s per DM prologue, extrapolated to "
-                          f"{avg_trials:.1f} trials per DM")}
+        cpu_v = cores * eff * avg_trials / (per_dm + avg_trials * per_trial)
+        cpu = {"value": cpu_v, "unit": "trials/s", "cores": cores, "kind": "port",
+               "sample": (f"FP64 oracle (the project's C restatement; no FFTW in the image), "
+                          f"one 2^23 DM trial with 1 and with 3 acceleration trials on one "
+                          f"core: {per_trial:.2f}s per trial, {per_dm:.2f}s per DM prologue; "
+                          f"the 3-trial search on {cores} spawned processes at once ran at "
+                          f"{eff:.2f} of the one-core speed; extrapolated to "
+                          f"{avg_trials:.1f} trials per DM over {cores} cores "
+                          f"({spent:.1f}s of sampling)")}
     eng.close()
     served = None
     if rank == 0 and ws == 1 and args.served > 0:
