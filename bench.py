@@ -621,7 +621,9 @@ def run_psx(args, ws, rank, local):
         log(f"[rank {rank}] autotune: batch {batch}, harmonic shape {shape} "
             f"({time.perf_counter() - t0:.1f}s)")
     stream = torch.cuda.Stream()
-    eng = search.AccelSearch(make_params(plan, "batched", batch, shape))
+    pr = make_params(plan, "batched", batch, shape)
+    pr.graph = not args.no_graph
+    eng = search.AccelSearch(pr)
     eng.set_stream(stream.cuda_stream)
 
     def do_step(dm_list, src):
@@ -796,6 +798,7 @@ def run_psx(args, ws, rank, local):
                                    "acc -100..100, 5 folds, S/N 9, 20 birdies zapped",
                        "dms_per_step": S, "mode": "batched",
                        "batch": batch_used, "harm_shape": shape_used,
+                       "graphs": not args.no_graph,
                        "tuned": "autotuner (batch x harmonic shape)" if tune else "fixed",
                        "parallelism": f"dm-sharded x{ws}",
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
@@ -820,6 +823,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch the trial schedules directly instead of as CUDA graphs")
     ap.add_argument("--served", type=int, default=SERVED_REQUESTS,
                     help="requests of the served workload (0: skip)")
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],

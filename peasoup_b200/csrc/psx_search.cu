@@ -226,7 +226,22 @@ struct Slot {
     size_t ktab_cap = 0;
     cudaEvent_t done = nullptr;
     cudaEvent_t copied = nullptr;
-    std::vector<cudaEvent_t> ev;  // profiling: 2 + 4 per launch group
+    std::vector<cudaEvent_t> ev;  // profiling: prologue start/end, trials start, 4 per launch group
+    // The DM's resident dereddened series and the prologue's scratch, one
+    // set per slot: the prologue of the next DM runs on this slot's own
+    // stream while the previous DM's trials run on the compute stream.
+    float* d_tim = nullptr;
+    float* d_Xp = nullptr;    // prologue spectrum (Bp complex)
+    float* d_pp = nullptr;    // prologue amplitudes (Bp floats)
+    void* d_med = nullptr;
+    double2* d_part = nullptr;
+    double* d_sums = nullptr;
+    float* d_stat = nullptr;  // interbin statistics: [3] mean*N, [4] std*N
+    float* d_mean = nullptr;
+    FftPlan* r2c = nullptr;   // batch-1 plans of the prologue
+    FftPlan* c2r = nullptr;
+    cudaStream_t pst = nullptr;
+    cudaEvent_t ready = nullptr;  // prologue complete (on pst)
     // job
     std::vector<float> accs;
     const float* series = nullptr;
@@ -265,15 +280,9 @@ struct psx_search {
     PeakParams pk{};
     float factor[6] = {0, 0, 0, 0, 0, 0};
 
-    float* d_tim = nullptr;
     float* d_tr = nullptr;
     float* d_X = nullptr;
     float* d_p = nullptr;
-    void* d_med = nullptr;
-    double2* d_part = nullptr;
-    double* d_sums = nullptr;
-    float* d_stat = nullptr;
-    float* d_mean = nullptr;
     float* d_bf = nullptr;
     float* d_bw = nullptr;
     size_t bird_cap = 0;  // entries d_bf / d_bw hold
@@ -281,7 +290,8 @@ struct psx_search {
     float* h_mean = nullptr;
 
     Slot slot[2];
-    FftPlan r2c1, c2r1;
+    FftPlan r2c1;                      // plain-mode trials and the debug tap
+    cudaEvent_t call_start = nullptr;  // compute-stream position at a call's start
     std::map<int, FftPlan*> r2cb;
     std::map<long long, GraphEntry> graphs;
     std::map<long long, int> capture_failures;
@@ -308,16 +318,13 @@ struct psx_search {
         for (auto& p : r2cb) delete p.second;
         r2cb.clear();
         r2c1.destroy();
-        c2r1.destroy();
-        void* dev[] = {d_tim, d_tr, d_X, d_p, d_med, d_part, d_sums, d_stat, d_mean, d_bf, d_bw,
-                       d_kbatch};
+        void* dev[] = {d_tr, d_X, d_p, d_bf, d_bw, d_kbatch};
         for (void* q : dev)
             if (q) cudaFree(q);
-        d_tim = d_tr = d_X = d_p = d_stat = d_mean = d_bf = d_bw = nullptr;
-        d_med = nullptr;
-        d_part = nullptr;
-        d_sums = nullptr;
+        d_tr = d_X = d_p = d_bf = d_bw = nullptr;
         d_kbatch = nullptr;
+        if (call_start) cudaEventDestroy(call_start);
+        call_start = nullptr;
         if (h_mean) cudaFreeHost(h_mean);
         h_mean = nullptr;
         for (Slot& s : slot) {
@@ -330,6 +337,15 @@ struct psx_search {
             if (s.done) cudaEventDestroy(s.done);
             if (s.copied) cudaEventDestroy(s.copied);
             for (cudaEvent_t e : s.ev) cudaEventDestroy(e);
+            if (s.pst) cudaStreamSynchronize(s.pst);
+            void* sdev[] = {s.d_tim, s.d_Xp, s.d_pp, s.d_med, s.d_part, s.d_sums, s.d_stat,
+                            s.d_mean};
+            for (void* q : sdev)
+                if (q) cudaFree(q);
+            delete s.r2c;
+            delete s.c2r;
+            if (s.ready) cudaEventDestroy(s.ready);
+            if (s.pst) cudaStreamDestroy(s.pst);
             s = Slot();
         }
         if (cst) cudaStreamDestroy(cst);
@@ -368,7 +384,7 @@ int psx_search::get_plan(int b, FftPlan** out)
     FftPlan* p = new (std::nothrow) FftPlan;
     if (!p) return PSX_ERR_ALLOC;
     int rc = p->create(N, b, PSX_FFT_R2C, N, Bp, callback());
-    if (rc == PSX_OK && callback()) rc = p->set_resample(d_tim, d_kbatch, st);
+    if (rc == PSX_OK && callback()) rc = p->set_resample(slot[0].d_tim, d_kbatch, st);
     if (rc != PSX_OK) {
         delete p;
         return rc;
@@ -415,7 +431,7 @@ int psx_search::grow_ktab(Slot& s, size_t need)
 
 int psx_search::ensure_events(Slot& s, int groups)
 {
-    const size_t need = 2 + 4 * (size_t)groups;
+    const size_t need = 3 + 4 * (size_t)groups;
     while (s.ev.size() < need) {
         cudaEvent_t e;
         PSX_CUDA(cudaEventCreate(&e));
@@ -424,17 +440,25 @@ int psx_search::ensure_events(Slot& s, int groups)
     return PSX_OK;
 }
 
-// src/pipeline_multi.cu:170-238 for one series, all on the compute stream.
+// src/pipeline_multi.cu:170-238 for one series, on the slot's own stream.
+// It starts once the caller's work queued before this call (call_start)
+// and the slot's previous DM (whose trials read s.d_tim) are done, and
+// records s.ready; the trials wait for s.ready on the compute stream.  So
+// the prologue of DM d+1 runs alongside the trials of DM d.
 int psx_search::prologue(Slot& s)
 {
+    cudaStream_t ps = s.pst;
+    PSX_CUDA(cudaStreamWaitEvent(ps, call_start, 0));
+    PSX_CUDA(cudaStreamWaitEvent(ps, s.done, 0));
+    if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[0], ps));
     const size_t ncopy = std::min(s.nsamps, N);
     // a device series 16-byte aligned is copied by the first baseline pass
     const bool fused_copy =
         s.on_device && !s.host_baseline && (reinterpret_cast<uintptr_t>(s.series) & 15u) == 0;
     if (!fused_copy)
-        PSX_CUDA(cudaMemcpyAsync(d_tim, s.series, sizeof(float) * ncopy,
+        PSX_CUDA(cudaMemcpyAsync(s.d_tim, s.series, sizeof(float) * ncopy,
                                  s.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                 st));
+                                 ps));
     // baseline removal over the copied samples (timeseries.hpp:282-287,
     // src/kernels.cu:463-479)
     const int nb = reduction_blocks();
@@ -443,50 +467,53 @@ int psx_search::prologue(Slot& s)
         // and one fused subtract + re-sum; passes after convergence return
         // at once
         if (fused_copy)
-            PSX_TRY(launch_partials_v4(s.series, ncopy, d_part, d_tim, s.d_count + 2, st));
+            PSX_TRY(launch_partials_v4(s.series, ncopy, s.d_part, s.d_tim, s.d_count + 2, ps));
         else
-            PSX_TRY(launch_partials_v4(d_tim, ncopy, d_part, nullptr, s.d_count + 2, st));
+            PSX_TRY(launch_partials_v4(s.d_tim, ncopy, s.d_part, nullptr, s.d_count + 2, ps));
         ++s.launches;
         for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
-            k_baseline_step<<<1, 32, 0, st>>>(d_part, nb, (double)ncopy, d_mean, s.d_count + 2);
-            PSX_TRY(launch_sub_partials_v4(d_tim, ncopy, d_mean, d_part, s.d_count + 2, st));
+            k_baseline_step<<<1, 32, 0, ps>>>(s.d_part, nb, (double)ncopy, s.d_mean,
+                                               s.d_count + 2);
+            PSX_TRY(launch_sub_partials_v4(s.d_tim, ncopy, s.d_mean, s.d_part, s.d_count + 2, ps));
             s.launches += 2;
         }
     } else {
         int count = 0;
         float mean = 0.f;
         do {
-            PSX_TRY(remove_baseline_pass(d_tim, ncopy, d_part, d_sums, d_mean, st));
+            PSX_TRY(remove_baseline_pass(s.d_tim, ncopy, s.d_part, s.d_sums, s.d_mean, ps));
             s.launches += 4;
-            PSX_CUDA(cudaMemcpyAsync(h_mean, d_mean, sizeof(float), cudaMemcpyDeviceToHost, st));
-            PSX_CUDA(cudaStreamSynchronize(st));
+            PSX_CUDA(cudaMemcpyAsync(h_mean, s.d_mean, sizeof(float), cudaMemcpyDeviceToHost, ps));
+            PSX_CUDA(cudaStreamSynchronize(ps));
             mean = *h_mean;
             if (count++ > 100) break;
         } while (std::fabs(mean) > 5e-7 * (double)ncopy);
     }
     // zero padding (pipeline_multi.cu:179-187)
     if (ncopy < N) {
-        PSX_TRY(launch_fill(d_tim + ncopy, N - ncopy, 0.f, st));
+        PSX_TRY(launch_fill(s.d_tim + ncopy, N - ncopy, 0.f, ps));
         ++s.launches;
     }
-    PSX_TRY(r2c1.exec(d_tim, d_X, st));
+    PSX_TRY(s.r2c->exec(s.d_tim, s.d_Xp, ps));
     ++s.ffts;
-    // amplitude spectrum into the first row of d_p (spectrumformer.hpp:16-22)
-    PSX_TRY(psx_form_power_series(d_X, d_p, B, 0, reinterpret_cast<psx_stream_t>(st)));
+    // amplitude spectrum (spectrumformer.hpp:16-22)
+    PSX_TRY(psx_form_power_series(s.d_Xp, s.d_pp, B, 0, reinterpret_cast<psx_stream_t>(ps)));
     ++s.launches;
     // running median and division (dereddener.hpp:41-66)
-    PSX_TRY(launch_running_median(d_p, B, bin_width, cfg.boundary_5_freq, cfg.boundary_25_freq,
-                                  nullptr, d_X, d_med, st));
+    PSX_TRY(launch_running_median(s.d_pp, B, bin_width, cfg.boundary_5_freq,
+                                  cfg.boundary_25_freq, nullptr, s.d_Xp, s.d_med, ps));
     s.launches += 4;
     if (!bf.empty()) {
-        PSX_TRY(launch_zap(d_X, d_bf, d_bw, bin_width_f, bf.size(), B, st));
+        PSX_TRY(launch_zap(s.d_Xp, d_bf, d_bw, bin_width_f, bf.size(), B, ps));
         ++s.launches;
     }
     // interbin statistics (pipeline_multi.cu:230-234) -> mean*N, std*N
-    PSX_TRY(launch_interbin_stats_v4(d_X, B, d_part, d_sums, d_stat, (float)N, st));
+    PSX_TRY(launch_interbin_stats_v4(s.d_Xp, B, s.d_part, s.d_sums, s.d_stat, (float)N, ps));
     s.launches += 2;
-    PSX_TRY(c2r1.exec(d_X, d_tim, st));
+    PSX_TRY(s.c2r->exec(s.d_Xp, s.d_tim, ps));
     ++s.ffts;
+    if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[1], ps));
+    PSX_CUDA(cudaEventRecord(s.ready, ps));
     return PSX_OK;
 }
 
@@ -495,6 +522,7 @@ int psx_search::prologue(Slot& s)
 int psx_search::trials_enqueue(Slot& s, int nacc)
 {
     PSX_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned) * 2, st));
+    if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2], st));
     const unsigned T = 256;
     const unsigned span = pk.hi > pk.lo ? pk.hi - pk.lo : 0;
     int t0 = 0, g = 0;
@@ -506,34 +534,35 @@ int psx_search::trials_enqueue(Slot& s, int nacc)
             FftPlan* plan = nullptr;
             PSX_TRY(get_plan(b, &plan));
             if (callback()) {
+                PSX_TRY(plan->set_resample(s.d_tim, d_kbatch, st));
                 PSX_CUDA(cudaMemcpyAsync(d_kbatch, s.d_ktab + t0, sizeof(double) * b,
                                          cudaMemcpyDeviceToDevice, st));
             } else {
-                PSX_TRY(launch_resample(d_tim, d_tr, N, s.d_ktab + t0, 0.0, b, N, false, st));
+                PSX_TRY(launch_resample(s.d_tim, d_tr, N, s.d_ktab + t0, 0.0, b, N, false, st));
                 ++s.launches;
             }
-            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g], st));
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], st));
             PSX_TRY(plan->exec(d_tr, d_X, st));
             ++s.ffts;
         } else {
-            PSX_TRY(launch_resample(d_tim, d_tr, N, s.d_ktab + t0, 0.0, 1, N, false, st));
+            PSX_TRY(launch_resample(s.d_tim, d_tr, N, s.d_ktab + t0, 0.0, 1, N, false, st));
             ++s.launches;
-            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g], st));
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], st));
             PSX_TRY(r2c1.exec(d_tr, d_X, st));
             ++s.ffts;
         }
-        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 1], st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 1], st));
         dim3 gf(grid_for(B / 2 + 1, T, 4), (unsigned)b);
-        k_form_norm<<<gf, T, 0, st>>>(d_X, 2 * Bp, d_p, Bp, (unsigned)B, d_stat);
+        k_form_norm<<<gf, T, 0, st>>>(d_X, 2 * Bp, d_p, Bp, (unsigned)B, s.d_stat);
         ++s.launches;
         PSX_TRY(launch_status("form kernel"));
-        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 2], st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 2], st));
         if (span) {
             PSX_TRY(launch_harm(F, harm_shape, d_p, Bp, (unsigned)Bp, pk, t0, b, s.d_rec, s.d_count,
                                 (unsigned)s.rec_cap, st));
             ++s.launches;
         }
-        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2 + 4 * g + 3], st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 3], st));
         t0 += b;
         ++g;
     }
@@ -625,12 +654,9 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
     const int nacc = (int)s.accs.size();
     PSX_TRY(grow_ktab(s, (size_t)nacc));
     for (int t = 0; t < nacc; ++t) s.h_ktab[t] = accel_fact(s.accs[t], c.tsamp);
-    if (s.profiled) {
-        PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
-        PSX_CUDA(cudaEventRecord(s.ev[0], st));
-    }
+    if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
     PSX_TRY(prologue(s));
-    if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[1], st));
+    PSX_CUDA(cudaStreamWaitEvent(st, s.ready, 0));
     PSX_CUDA(cudaMemcpyAsync(s.d_ktab, s.h_ktab, sizeof(double) * nacc, cudaMemcpyHostToDevice, st));
     PSX_TRY(run_trials(s, nacc));
     PSX_CUDA(cudaMemcpyAsync(s.h_count, s.d_count, sizeof(unsigned) * 4, cudaMemcpyDeviceToHost, st));
@@ -653,8 +679,8 @@ void psx_search::read_profile(Slot& s)
     };
     span(s.ev[0], s.ev[1], prof.prologue_ms);
     for (int g = 0; g < s.groups; ++g) {
-        cudaEvent_t prev = g == 0 ? s.ev[1] : s.ev[2 + 4 * (g - 1) + 3];
-        cudaEvent_t* e = &s.ev[2 + 4 * g];
+        cudaEvent_t prev = g == 0 ? s.ev[2] : s.ev[3 + 4 * (g - 1) + 3];
+        cudaEvent_t* e = &s.ev[3 + 4 * g];
         span(prev, e[0], prof.resample_ms);
         span(e[0], e[1], prof.fft_ms);
         span(e[1], e[2], prof.form_ms);
@@ -903,14 +929,15 @@ size_t psx_search_footprint(const psx_search_config* c)
     const size_t b = (size_t)effective_batch(c);
     const bool cb = c->mode == PSX_MODE_BATCHED && c->use_fft_callback;
     size_t bytes = 0;
-    bytes += sizeof(float) * N;                       // resident dereddened series
+    bytes += 2 * sizeof(float) * (N + 3 * Bp);        // per slot: series, prologue spectra
+    bytes += 2 * median_scratch_bytes(B);
     bytes += sizeof(float) * N * (cb ? 1 : b);        // resampled series
     bytes += sizeof(float) * 2 * Bp * b;              // complex spectra
     bytes += sizeof(float) * Bp * b;                  // normalised spectra
-    bytes += median_scratch_bytes(B);
     bytes += 2 * sizeof(int4) * ((size_t)1 << 20);    // two initial record slots
-    // cuFFT work areas: about one transform's worth per batched plan size
-    bytes += sizeof(float) * 2 * Bp * (2 * b + 2);
+    // cuFFT work areas: about one transform's worth per batched plan size,
+    // plus the batch-1 plans of the two slots' prologues and the plain path
+    bytes += sizeof(float) * 2 * Bp * (2 * b + 6);
     return bytes;
 }
 
@@ -1000,17 +1027,21 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     if ((rc = cuda_status(cudaMalloc((void**)&(ptr), (bytes)), "cudaMalloc")) != \
         PSX_OK)                                                                  \
         return fail(rc == PSX_ERR_CUDA ? PSX_ERR_ALLOC : rc);
-    ALLOC(s->d_tim, sizeof(float) * N);
     ALLOC(s->d_tr, sizeof(float) * N * (cb ? 1 : b));
     ALLOC(s->d_X, sizeof(float) * 2 * Bp * b);
     ALLOC(s->d_p, sizeof(float) * Bp * b);
-    ALLOC(s->d_med, median_scratch_bytes(s->B));
-    ALLOC(s->d_part, sizeof(double2) * nb);
-    ALLOC(s->d_sums, sizeof(double) * 2);
-    ALLOC(s->d_stat, sizeof(float) * 8);
-    ALLOC(s->d_mean, sizeof(float) * 2);
     ALLOC(s->d_kbatch, sizeof(double) * b);
-    for (Slot& sl : s->slot) ALLOC(sl.d_count, sizeof(unsigned) * 4);
+    for (Slot& sl : s->slot) {
+        ALLOC(sl.d_count, sizeof(unsigned) * 4);
+        ALLOC(sl.d_tim, sizeof(float) * N);
+        ALLOC(sl.d_Xp, sizeof(float) * 2 * Bp);
+        ALLOC(sl.d_pp, sizeof(float) * Bp);
+        ALLOC(sl.d_med, median_scratch_bytes(s->B));
+        ALLOC(sl.d_part, sizeof(double2) * nb);
+        ALLOC(sl.d_sums, sizeof(double) * 2);
+        ALLOC(sl.d_stat, sizeof(float) * 8);
+        ALLOC(sl.d_mean, sizeof(float) * 2);
+    }
     if (!s->bf.empty()) {
         ALLOC(s->d_bf, sizeof(float) * s->bf.size());
         ALLOC(s->d_bw, sizeof(float) * s->bw.size());
@@ -1022,8 +1053,17 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
         if (cudaMallocHost(&sl.h_count, sizeof(unsigned) * 4) != cudaSuccess)
             return fail(PSX_ERR_ALLOC);
         if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.ready, cudaEventDisableTiming) != cudaSuccess)
             return fail(PSX_ERR_CUDA);
+        if ((rc = cuda_status(cudaStreamCreateWithFlags(&sl.pst, cudaStreamNonBlocking),
+                              "cudaStreamCreate")) != PSX_OK)
+            return fail(rc);
+        sl.r2c = new (std::nothrow) FftPlan;
+        sl.c2r = new (std::nothrow) FftPlan;
+        if (!sl.r2c || !sl.c2r) return fail(PSX_ERR_ALLOC);
+        if ((rc = sl.r2c->create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
+        if ((rc = sl.c2r->create(N, 1, PSX_FFT_C2R, 0, 0, false)) != PSX_OK) return fail(rc);
         if ((rc = s->grow_records(sl, (size_t)1 << 20)) != PSX_OK) return fail(rc);
         if ((rc = s->grow_ktab(sl, 1024)) != PSX_OK) return fail(rc);
     }
@@ -1035,8 +1075,13 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     cudaMemsetAsync(s->d_X, 0, sizeof(float) * 2 * Bp * b, s->st);
     cudaMemsetAsync(s->d_p, 0, sizeof(float) * Bp * b, s->st);
     cudaMemsetAsync(s->d_kbatch, 0, sizeof(double) * b, s->st);
+    for (Slot& sl : s->slot) {
+        cudaMemsetAsync(sl.d_Xp, 0, sizeof(float) * 2 * Bp, s->st);
+        cudaMemsetAsync(sl.d_pp, 0, sizeof(float) * Bp, s->st);
+    }
+    if (cudaEventCreateWithFlags(&s->call_start, cudaEventDisableTiming) != cudaSuccess)
+        return fail(PSX_ERR_CUDA);
     if ((rc = s->r2c1.create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
-    if ((rc = s->c2r1.create(N, 1, PSX_FFT_C2R, 0, 0, false)) != PSX_OK) return fail(rc);
     if (s->batched()) {
         FftPlan* p = nullptr;
         if ((rc = s->get_plan(s->batch, &p)) != PSX_OK) return fail(rc);
@@ -1078,6 +1123,7 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     // work queued with the old parameters finishes first
     PSX_CUDA(cudaStreamSynchronize(s->st));
     PSX_CUDA(cudaStreamSynchronize(s->cst));
+    for (Slot& sl : s->slot) PSX_CUDA(cudaStreamSynchronize(sl.pst));
     host_setup(s, cfg);
     if (s->bf.size() > s->bird_cap) {
         cudaFree(s->d_bf);
@@ -1151,6 +1197,8 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
     s->info.graph = s->batched() && s->cfg.use_graph && !s->profile ? 1 : 0;
     std::vector<psx_candidate> all, out;
     std::vector<int> all_na, all_tr, all_dm, na, tr;
+    // prologues wait for the caller's work queued on the compute stream so far
+    PSX_CUDA(cudaEventRecord(s->call_start, s->st));
     int rc = s->enqueue(s->slot[0], series[0], nsamps, series_on_device != 0, dms[0],
                         dm_idx ? dm_idx[0] : 0);
     for (int d = 0; d < ndm && rc == PSX_OK; ++d) {
@@ -1210,17 +1258,17 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
     Slot& sl = s->slot[s->last_slot];
     const std::vector<float>& accs = sl.accs;
     if (h_tim_dered)
-        PSX_CUDA(cudaMemcpyAsync(h_tim_dered, s->d_tim, sizeof(float) * s->N,
+        PSX_CUDA(cudaMemcpyAsync(h_tim_dered, sl.d_tim, sizeof(float) * s->N,
                                  cudaMemcpyDeviceToHost, s->st));
     if (h_norm2)
-        PSX_CUDA(cudaMemcpyAsync(h_norm2, s->d_stat + 3, sizeof(float) * 2, cudaMemcpyDeviceToHost,
+        PSX_CUDA(cudaMemcpyAsync(h_norm2, sl.d_stat + 3, sizeof(float) * 2, cudaMemcpyDeviceToHost,
                                  s->st));
     if (h_tim_r || h_pspec) {
         if (trial < 0 || trial >= (int)accs.size()) {
             set_error("debug_tap: trial %d out of range", trial);
             return PSX_ERR_INVALID;
         }
-        PSX_TRY(launch_resample(s->d_tim, s->d_tr, s->N, nullptr,
+        PSX_TRY(launch_resample(sl.d_tim, s->d_tr, s->N, nullptr,
                                 accel_fact(accs[trial], s->cfg.tsamp), 1, s->N, false, s->st));
         if (h_tim_r)
             PSX_CUDA(cudaMemcpyAsync(h_tim_r, s->d_tr, sizeof(float) * s->N,
@@ -1229,7 +1277,7 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
             PSX_TRY(s->r2c1.exec(s->d_tr, s->d_X, s->st));
             dim3 gf(grid_for(s->B / 2 + 1, 256, 4), 1);
             k_form_norm<<<gf, 256, 0, s->st>>>(s->d_X, 2 * s->Bp, s->d_p, s->Bp, (unsigned)s->B,
-                                               s->d_stat);
+                                               sl.d_stat);
             PSX_TRY(launch_status("debug tap"));
             PSX_CUDA(cudaMemcpyAsync(h_pspec, s->d_p, sizeof(float) * s->B,
                                      cudaMemcpyDeviceToHost, s->st));
