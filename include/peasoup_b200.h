@@ -255,6 +255,86 @@ size_t psx_distill(int kind, psx_candidate* cands, size_t n, float tol,
                    int fractional, int* h_nassoc);
 
 /* ------------------------------------------------------------------ */
+/* Candidate forests: the association trees of the distillers           */
+/* ------------------------------------------------------------------ */
+
+/* A candidate forest is `nodes` in depth-first order with sizes[i] = the
+   number of nodes in the subtree node i roots (itself included); roots are
+   the nodes that start a top-level subtree.  It is the reference's
+   Candidate::assoc tree (include/data_types/candidates.hpp:19-86) laid out
+   as Candidate::collect_candidates walks it, so a root's subtree is the
+   run of records candidates.peasoup holds for that candidate, and
+   sizes[root] - 1 is its Candidate::count_assoc(). */
+
+/* Distillation of the roots of a forest, keeping trees: BaseDistiller::
+   distill (include/transforms/distiller.hpp:25-57) with the three
+   conditions as in psx_distill; with keep_related each survivor's subtree
+   is its own followed by every absorbed candidate's (in the reference's
+   append order, repeated where it appends more than once).  Survivors come
+   out in descending S/N.  *n_out = nodes written (the need, with
+   PSX_ERR_OVERFLOW), *n_roots = survivors (may be NULL).  Replaces the
+   global DMDistiller / HarmonicDistiller(keep_related) of
+   src/pipeline_multi.cu:406-407, 547-548. */
+int psx_distill_forest(int kind, const psx_candidate* nodes, const int* sizes,
+                       size_t n_nodes, float tol, float max_harm, float tobs,
+                       int keep_related, int fractional, psx_candidate* h_out,
+                       int* h_out_sizes, size_t cap, size_t* n_out,
+                       size_t* n_roots);
+
+typedef struct {
+    int is_physical;       /* 1/freq > channel DM smearing at the DM */
+    int is_adjacent;       /* an association one DM trial away, or none off-DM */
+    float ddm_count_ratio; /* share of associations within the DM width */
+    float ddm_snr_ratio;   /* share of their S/N */
+    int nassoc;            /* Candidate::count_assoc() */
+} psx_candidate_score;
+
+/* CandidateScorer(tsamp, cfreq, foff, bw)::score for every root, from its
+   direct associations (include/transforms/scorer.hpp:8-87; frequencies in
+   MHz as the reference passes them, src/pipeline_multi.cu:550-552). */
+int psx_score_forest(const psx_candidate* nodes, const int* sizes,
+                     size_t n_nodes, float tsamp, float cfreq, float foff,
+                     float bw, psx_candidate_score* h_scores, size_t cap,
+                     size_t* n_roots);
+
+/* candidates.peasoup: per root an int record count and its subtree's
+   24-byte records (CandidateFileWriter::write_binary, include/utils/
+   output_stats.hpp:270-298; no FOLD blocks: folding is not part of this
+   library).  h_offsets (may be NULL) receives each root's byte offset. */
+int psx_write_candidates(const char* path, const psx_candidate* nodes,
+                         const int* sizes, size_t n_nodes, long long* h_offsets,
+                         size_t cap, size_t* n_roots);
+
+/* overview.xml (OutputFileWriter, include/utils/output_stats.hpp:20-210),
+   built section by section and written in the reference's XML layout
+   (include/utils/xml_util.hpp).  Sections whose values come from outside
+   this library (header_parameters, search_parameters,
+   segment_parameters, execution_times) are added as name/value pairs,
+   values already formatted. */
+typedef struct psx_overview psx_overview;
+int psx_overview_create(psx_overview** out);
+void psx_overview_destroy(psx_overview* o);
+int psx_overview_add_section(psx_overview* o, const char* section,
+                             const char* const* keys, const char* const* values,
+                             size_t n);
+int psx_overview_add_misc_info(psx_overview* o, long long unix_time);
+int psx_overview_add_dm_list(psx_overview* o, const float* dms, size_t n);
+int psx_overview_add_acc_list(psx_overview* o, const float* accs, size_t n,
+                              float cdm);
+int psx_overview_add_device_info(psx_overview* o, int runtime_version,
+                                 int driver_version, const int* ids,
+                                 const char* const* names, const int* major,
+                                 const int* minor, size_t n);
+int psx_overview_add_candidates(psx_overview* o, const psx_candidate* nodes,
+                                const int* sizes, size_t n_nodes,
+                                const psx_candidate_score* scores,
+                                const long long* byte_offsets);
+/* Writes the document to `path` (may be NULL) and/or copies it into h_text
+   (cap bytes, NUL-terminated; may be NULL); *n_text = its length. */
+int psx_overview_write(psx_overview* o, const char* path, char* h_text,
+                       size_t cap, size_t* n_text);
+
+/* ------------------------------------------------------------------ */
 /* Per-DM acceleration search (the fused hot path)                     */
 /* ------------------------------------------------------------------ */
 
@@ -313,8 +393,11 @@ int psx_search_set_stream(psx_search* s, psx_stream_t stream);
 
 enum {
     PSX_OUT_TRIAL = 0,  /* per-trial harmonic-distilled candidates */
-    PSX_OUT_DM = 1      /* plus the per-DM acceleration distillation:
+    PSX_OUT_DM = 1,     /* plus the per-DM acceleration distillation:
                            the reference Worker's dm_trial_cands */
+    PSX_OUT_DM_FOREST = 2 /* the same survivors with their association
+                             trees: a candidate forest (see psx_distill_forest)
+                             whose subtree sizes go to h_nassoc */
 };
 
 /* Searches one dedispersed series: the body of the reference's DM loop,

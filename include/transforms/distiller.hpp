@@ -1,9 +1,13 @@
 // distiller.hpp -- candidate distillers of the drop-in API (reference
 // include/transforms/distiller.hpp:16-196).  distill() sorts the input by
 // descending S/N in place, as the reference does, and returns the
-// survivors; with keep_related each survivor carries its association
-// count in `assoc` (as placeholder entries).
+// survivors; with keep_related each survivor carries its association tree
+// in `assoc` (the absorbed candidates with their own trees, in the
+// reference's append order), computed by psx_distill_forest.
 #pragma once
+#include <algorithm>
+#include <stdexcept>
+#include <string>
 #include <vector>
 #include "data_types/candidates.hpp"
 #include "peasoup_b200.h"
@@ -22,20 +26,25 @@ public:
     virtual ~BaseDistiller() {}
     std::vector<Candidate> distill(std::vector<Candidate>& cands)
     {
-        std::vector<psx_candidate> pod(cands.size());
-        for (size_t i = 0; i < cands.size(); ++i) pod[i] = cands[i].pod();
-        std::vector<int> na(cands.size());
-        const size_t keep = pod.empty() ? 0
-                                        : psx_distill(kind, pod.data(), pod.size(), tol, max_harm,
-                                                      tobs, keep_related, fractional, na.data());
-        std::vector<Candidate> out;
-        out.reserve(keep);
-        for (size_t i = 0; i < keep; ++i) {
-            Candidate c(pod[i]);
-            c.assoc.resize((size_t)na[i]);
-            out.push_back(c);
+        std::vector<psx_candidate> nodes, out;
+        std::vector<int> sizes, out_sizes;
+        to_forest(cands, nodes, sizes);
+        size_t n = 0;
+        int rc = psx_distill_forest(kind, nodes.data(), sizes.data(), nodes.size(), tol, max_harm,
+                                    tobs, keep_related, fractional, nullptr, nullptr, 0, &n,
+                                    nullptr);
+        if (rc == PSX_ERR_OVERFLOW || rc == PSX_OK) {
+            out.resize(n);
+            out_sizes.resize(n);
+            rc = psx_distill_forest(kind, nodes.data(), sizes.data(), nodes.size(), tol, max_harm,
+                                    tobs, keep_related, fractional, out.data(), out_sizes.data(),
+                                    n, &n, nullptr);
         }
-        return out;
+        if (rc != PSX_OK) throw std::runtime_error(std::string("distill: ") + psx_last_error());
+        // the reference sorts its input by descending S/N in place
+        std::sort(cands.begin(), cands.end(),
+                  [](const Candidate& a, const Candidate& b) { return a.snr > b.snr; });
+        return from_forest(out.data(), out_sizes.data(), n);
     }
 };
 

@@ -425,6 +425,16 @@ def ref_host():
         L.ref_distill.restype = C.c_size_t
         L.ref_distill.argtypes = [C.c_int, C.c_void_p, C.c_size_t, C.c_float, C.c_float,
                                   C.c_float, C.c_int, C.c_int, C.c_void_p, _ip]
+        vp, sz, f = C.c_void_p, C.c_size_t, C.c_float
+        L.ref_distill_forest.restype = sz
+        L.ref_distill_forest.argtypes = [C.c_int, vp, vp, sz, f, f, f, C.c_int, C.c_int, vp, vp,
+                                         sz]
+        L.ref_score_forest.restype = sz
+        L.ref_score_forest.argtypes = [vp, vp, sz, f, f, f, f, vp]
+        L.ref_write_binary.restype = sz
+        L.ref_write_binary.argtypes = [C.c_char_p, C.c_char_p, vp, vp, sz, vp]
+        L.ref_overview_text.restype = sz
+        L.ref_overview_text.argtypes = [vp, sz, vp, sz, f, vp, vp, sz, vp, f, f, f, f, vp, sz]
         _ref_host = L
     return _ref_host
 
@@ -445,6 +455,68 @@ def ref_distill(kind: int, cands, tol=1e-4, max_harm=16.0, tobs=0.0, keep_relate
     n = ref_host().ref_distill(kind, arr.ctypes.data, arr.size, tol, max_harm, tobs,
                                int(keep_related), int(fractional), out.ctypes.data, na)
     return out[:n], na[:n]
+
+
+SCORE_DTYPE = np.dtype([("is_physical", "<i4"), ("is_adjacent", "<i4"),
+                        ("ddm_count_ratio", "<f4"), ("ddm_snr_ratio", "<f4"),
+                        ("nassoc", "<i4")])
+
+
+def ref_distill_forest(kind, nodes, sizes, tol=1e-4, max_harm=16.0, tobs=0.0,
+                       keep_related=True, fractional=False):
+    """The reference's distillers on candidate trees (a forest: nodes in
+    depth-first order with subtree sizes); returns the survivors' forest."""
+    a = np.ascontiguousarray(nodes, CAND_DTYPE)
+    sz = np.ascontiguousarray(sizes, np.int32)
+    L = ref_host()
+    args = (kind, a.ctypes.data, sz.ctypes.data, a.size, tol, max_harm, tobs,
+            int(keep_related), int(fractional))
+    n = L.ref_distill_forest(*args, None, None, 0)
+    out = np.zeros(max(1, n), CAND_DTYPE)
+    osz = np.zeros(max(1, n), np.int32)
+    L.ref_distill_forest(*args, out.ctypes.data, osz.ctypes.data, out.size)
+    return out[:n], osz[:n]
+
+
+def _nroots(sizes):
+    i, k = 0, 0
+    while i < len(sizes):
+        i += int(sizes[i])
+        k += 1
+    return k
+
+
+def ref_score_forest(nodes, sizes, tsamp, cfreq, foff, bw):
+    a = np.ascontiguousarray(nodes, CAND_DTYPE)
+    sz = np.ascontiguousarray(sizes, np.int32)
+    out = np.zeros(max(1, _nroots(sz)), SCORE_DTYPE)
+    n = ref_host().ref_score_forest(a.ctypes.data, sz.ctypes.data, a.size, tsamp, cfreq, foff, bw,
+                                    out.ctypes.data)
+    return out[:n]
+
+
+def ref_write_binary(directory, filename, nodes, sizes):
+    a = np.ascontiguousarray(nodes, CAND_DTYPE)
+    sz = np.ascontiguousarray(sizes, np.int32)
+    off = np.zeros(max(1, _nroots(sz)), np.int64)
+    n = ref_host().ref_write_binary(directory.encode(), filename.encode(), a.ctypes.data,
+                                    sz.ctypes.data, a.size, off.ctypes.data)
+    return off[:n]
+
+
+def ref_overview_text(dms, accs, cdm, nodes, sizes, offsets, tsamp, cfreq, foff, bw) -> str:
+    d = np.ascontiguousarray(dms, np.float32)
+    ac = np.ascontiguousarray(accs, np.float32)
+    a = np.ascontiguousarray(nodes, CAND_DTYPE)
+    sz = np.ascontiguousarray(sizes, np.int32)
+    off = np.ascontiguousarray(offsets, np.int64)
+    L = ref_host()
+    args = (d.ctypes.data, d.size, ac.ctypes.data, ac.size, cdm, a.ctypes.data, sz.ctypes.data,
+            a.size, off.ctypes.data, tsamp, cfreq, foff, bw)
+    n = L.ref_overview_text(*args, None, 0)
+    buf = C.create_string_buffer(n + 1)
+    L.ref_overview_text(*args, buf, n + 1)
+    return buf.value.decode("latin-1")
 
 
 class _RefArgs(C.Structure):

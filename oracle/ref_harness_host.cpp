@@ -1,18 +1,27 @@
 /*
  * ref_harness_host.cpp -- drives the reference's own host-side classes of
  * the search path that need no GPU: AccelerationPlan
- * (include/utils/utils.hpp:143-233) and the candidate distillers
- * (include/transforms/distiller.hpp).  Compiled with g++ from the reference
+ * (include/utils/utils.hpp:143-233), the candidate distillers
+ * (include/transforms/distiller.hpp), CandidateScorer
+ * (include/transforms/scorer.hpp) and the output writers
+ * (include/utils/output_stats.hpp).  Candidate trees cross this boundary as
+ * forests: nodes in depth-first order with subtree sizes.  Compiled with g++ from the reference
  * headers where they lie, into oracle/_ref/; runs on any CPU.
  *
  * TEST INFRASTRUCTURE ONLY: used to pin the oracle and the product's host
  * logic; never linked by the product.
  */
+#include <cuda_runtime.h>
 #include <cstring>
+#include <string>
 #include <vector>
 #include <utils/utils.hpp>
+#include <utils/exceptions.hpp>
 #include <data_types/candidates.hpp>
+#include <data_types/filterbank.hpp>
 #include <transforms/distiller.hpp>
+#include <transforms/scorer.hpp>
+#include <utils/output_stats.hpp>
 
 extern "C" {
 
@@ -67,6 +76,122 @@ size_t ref_distill(int kind, const ref_candidate* in, size_t n, float tol, float
         if (nassoc) nassoc[i] = r[i].count_assoc();
     }
     return r.size();
+}
+
+/* ---- candidate forests <-> Candidate trees ---- */
+static Candidate tree_at(const ref_candidate* nodes, const int* sizes, size_t& i)
+{
+    Candidate c(nodes[i].dm, nodes[i].dm_idx, nodes[i].acc, nodes[i].nh, nodes[i].snr,
+                nodes[i].freq);
+    const size_t end = i + (size_t)sizes[i];
+    ++i;
+    while (i < end) {
+        Candidate child = tree_at(nodes, sizes, i);
+        c.append(child);
+    }
+    return c;
+}
+
+static std::vector<Candidate> trees(const ref_candidate* nodes, const int* sizes, size_t n)
+{
+    std::vector<Candidate> out;
+    size_t i = 0;
+    while (i < n) out.push_back(tree_at(nodes, sizes, i));
+    return out;
+}
+
+static void flatten(Candidate& c, std::vector<ref_candidate>& out, std::vector<int>& sizes)
+{
+    const size_t at = out.size();
+    out.push_back(ref_candidate{c.dm, c.dm_idx, c.acc, c.nh, c.snr, c.freq});
+    sizes.push_back(0);
+    for (size_t k = 0; k < c.assoc.size(); ++k) flatten(c.assoc[k], out, sizes);
+    sizes[at] = (int)(out.size() - at);
+}
+
+/* The distillers on trees; writes the survivors' trees as a forest and
+   returns its node count (or the need when larger than cap). */
+size_t ref_distill_forest(int kind, const ref_candidate* nodes, const int* sizes, size_t n,
+                          float tol, float max_harm, float tobs, int keep_related,
+                          int fractional, ref_candidate* out, int* out_sizes, size_t cap)
+{
+    std::vector<Candidate> c = trees(nodes, sizes, n);
+    std::vector<Candidate> r;
+    if (kind == 0) {
+        HarmonicDistiller d(tol, max_harm, keep_related != 0, fractional != 0);
+        r = d.distill(c);
+    } else if (kind == 1) {
+        AccelerationDistiller d(tobs, tol, keep_related != 0);
+        r = d.distill(c);
+    } else {
+        DMDistiller d(tol, keep_related != 0);
+        r = d.distill(c);
+    }
+    std::vector<ref_candidate> f;
+    std::vector<int> fs;
+    for (size_t i = 0; i < r.size(); ++i) flatten(r[i], f, fs);
+    if (f.size() <= cap) {
+        std::memcpy(out, f.data(), sizeof(ref_candidate) * f.size());
+        std::memcpy(out_sizes, fs.data(), sizeof(int) * fs.size());
+    }
+    return f.size();
+}
+
+typedef struct {
+    int is_physical, is_adjacent;
+    float ddm_count_ratio, ddm_snr_ratio;
+    int nassoc;
+} ref_score;
+
+static void score(std::vector<Candidate>& c, float tsamp, float cfreq, float foff, float bw)
+{
+    CandidateScorer sc(tsamp, cfreq, foff, bw);
+    sc.score_all(c);
+}
+
+/* CandidateScorer::score_all on the forest's roots. */
+size_t ref_score_forest(const ref_candidate* nodes, const int* sizes, size_t n, float tsamp,
+                        float cfreq, float foff, float bw, ref_score* out)
+{
+    std::vector<Candidate> c = trees(nodes, sizes, n);
+    score(c, tsamp, cfreq, foff, bw);
+    for (size_t i = 0; i < c.size(); ++i)
+        out[i] = ref_score{c[i].is_physical ? 1 : 0, c[i].is_adjacent ? 1 : 0,
+                           c[i].ddm_count_ratio, c[i].ddm_snr_ratio, c[i].count_assoc()};
+    return c.size();
+}
+
+/* CandidateFileWriter(dir).write_binary(trees, filename); byte offsets of
+   every root. */
+size_t ref_write_binary(const char* dir, const char* filename, const ref_candidate* nodes,
+                        const int* sizes, size_t n, long long* offsets)
+{
+    std::vector<Candidate> c = trees(nodes, sizes, n);
+    CandidateFileWriter w(dir);
+    w.write_binary(c, filename);
+    for (size_t i = 0; i < c.size(); ++i) offsets[i] = w.byte_mapping[(unsigned)i];
+    return c.size();
+}
+
+/* OutputFileWriter with the DM list, the acceleration list and the scored
+   candidates (byte offsets given), as text; returns its length. */
+size_t ref_overview_text(const float* dms, size_t ndm, const float* accs, size_t nacc, float cdm,
+                         const ref_candidate* nodes, const int* sizes, size_t n,
+                         const long long* offsets, float tsamp, float cfreq, float foff,
+                         float bw, char* out, size_t cap)
+{
+    std::vector<Candidate> c = trees(nodes, sizes, n);
+    score(c, tsamp, cfreq, foff, bw);
+    OutputFileWriter w;
+    std::vector<float> d(dms, dms + ndm), a(accs, accs + nacc);
+    w.add_dm_list(d);
+    w.add_acc_list(a, cdm);
+    std::map<unsigned, long int> bm;
+    for (size_t i = 0; i < c.size(); ++i) bm[(unsigned)i] = (long int)offsets[i];
+    w.add_candidates(c, bm);
+    const std::string t = w.to_string();
+    if (t.size() + 1 <= cap) std::memcpy(out, t.c_str(), t.size() + 1);
+    return t.size();
 }
 
 }  // extern "C"

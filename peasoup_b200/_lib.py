@@ -30,6 +30,7 @@ PSX_MODE_PLAIN = 0
 PSX_MODE_BATCHED = 1
 PSX_OUT_TRIAL = 0
 PSX_OUT_DM = 1
+PSX_OUT_DM_FOREST = 2
 PSX_DISTILL_HARMONIC = 0
 PSX_DISTILL_ACCEL = 1
 PSX_DISTILL_DM = 2
@@ -75,6 +76,12 @@ class SearchProfile(C.Structure):
                 ("fft_ms", C.c_double), ("form_ms", C.c_double), ("harm_ms", C.c_double),
                 ("groups", C.c_longlong), ("trials", C.c_longlong), ("dms", C.c_longlong),
                 ("event_errors", C.c_longlong), ("last_event_error", C.c_int)]
+
+
+class CandidateScore(C.Structure):
+    _fields_ = [("is_physical", C.c_int), ("is_adjacent", C.c_int),
+                ("ddm_count_ratio", C.c_float), ("ddm_snr_ratio", C.c_float),
+                ("nassoc", C.c_int)]
 
 
 class ServerConfig(C.Structure):
@@ -141,6 +148,19 @@ SIGNATURES = {
     "psx_search_debug_tap": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "psx_autotune": (_i, [C.POINTER(SearchConfig), _vp, _i, _i, _i, _vp]),
     "psx_search_retarget": (_i, [_vp, C.POINTER(SearchConfig)]),
+    "psx_distill_forest": (_i, [_i, _vp, _vp, _sz, _f, _f, _f, _i, _i, _vp, _vp, _sz,
+                                C.POINTER(_sz), C.POINTER(_sz)]),
+    "psx_score_forest": (_i, [_vp, _vp, _sz, _f, _f, _f, _f, _vp, _sz, C.POINTER(_sz)]),
+    "psx_write_candidates": (_i, [C.c_char_p, _vp, _vp, _sz, _vp, _sz, C.POINTER(_sz)]),
+    "psx_overview_create": (_i, [C.POINTER(_vp)]),
+    "psx_overview_destroy": (None, [_vp]),
+    "psx_overview_add_section": (_i, [_vp, C.c_char_p, _vp, _vp, _sz]),
+    "psx_overview_add_misc_info": (_i, [_vp, C.c_longlong]),
+    "psx_overview_add_dm_list": (_i, [_vp, _vp, _sz]),
+    "psx_overview_add_acc_list": (_i, [_vp, _vp, _sz, _f]),
+    "psx_overview_add_device_info": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _sz]),
+    "psx_overview_add_candidates": (_i, [_vp, _vp, _vp, _sz, _vp, _vp]),
+    "psx_overview_write": (_i, [_vp, C.c_char_p, _vp, _sz, C.POINTER(_sz)]),
     "psx_server_create": (_i, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
     "psx_server_destroy": (_i, [_vp]),
     "psx_server_clock": (C.c_double, [_vp]),

@@ -129,7 +129,9 @@ size_t distill(int kind, psx_candidate* c, size_t n, float tol, float max_harm, 
     std::sort(c, c + n, SnrGreater());
     std::vector<char> uniq(n, 1);
     std::vector<int> na(n, 0);
-    const double upper = 1 + (double)tol, lower = 1 - (double)tol;
+    // `1 + tolerance` with a float tolerance is a float sum in the reference
+    // (distiller.hpp:76-77, 164-165), widened to double afterwards
+    const double upper = (double)(1.0f + tol), lower = (double)(1.0f - tol);
     const double tobs_over_c = (double)tobs / 299792458.0;
     for (size_t i = 0; i < n; ++i) {
         if (!uniq[i]) continue;

@@ -780,7 +780,33 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
             out.push_back(c);
             trial_of.push_back(t);
         }
-    if (output == PSX_OUT_DM && !out.empty()) {
+    if (output == PSX_OUT_DM_FOREST && !out.empty()) {
+        // AccelerationDistiller(tobs, freq_tol, keep_related) keeping trees
+        // (pipeline_multi.cu:149, 294): the trial survivors are leaves
+        std::vector<int> ones(out.size(), 1);
+        std::vector<psx_candidate> f(out.size() * 2);
+        std::vector<int> fs(f.size());
+        size_t nn = 0;
+        int rc = psx_distill_forest(PSX_DISTILL_ACCEL, out.data(), ones.data(), out.size(),
+                                    cfg.freq_tol, cfg.max_harm, tobs, 1, 1, f.data(), fs.data(),
+                                    f.size(), &nn, nullptr);
+        if (rc == PSX_ERR_OVERFLOW) {
+            f.resize(nn);
+            fs.resize(nn);
+            rc = psx_distill_forest(PSX_DISTILL_ACCEL, out.data(), ones.data(), out.size(),
+                                    cfg.freq_tol, cfg.max_harm, tobs, 1, 1, f.data(), fs.data(),
+                                    f.size(), &nn, nullptr);
+        }
+        f.resize(nn);
+        fs.resize(nn);
+        trial_of.assign(nn, -1);
+        for (size_t k = 0; k < nn; ++k) {
+            auto it = std::lower_bound(s.accs.begin(), s.accs.end(), f[k].acc);
+            if (it != s.accs.end() && *it == f[k].acc) trial_of[k] = (int)(it - s.accs.begin());
+        }
+        out.swap(f);
+        nassoc.swap(fs);
+    } else if (output == PSX_OUT_DM && !out.empty()) {
         std::vector<psx_candidate> c = out;
         nassoc.assign(c.size(), 0);
         const size_t keep = distill(PSX_DISTILL_ACCEL, c.data(), c.size(), cfg.freq_tol,
@@ -1178,7 +1204,7 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
 {
     clear_error();
     if (!s || !series || !dms || !n_out || ndm <= 0 || nsamps == 0 ||
-        (output != PSX_OUT_TRIAL && output != PSX_OUT_DM)) {
+        (output != PSX_OUT_TRIAL && output != PSX_OUT_DM && output != PSX_OUT_DM_FOREST)) {
         set_error("search: bad arguments");
         return PSX_ERR_INVALID;
     }

@@ -148,7 +148,8 @@ class AccelSearch:
             ptr = C.c_void_p(a.ctypes.data)
             n = a.size if nsamps is None else nsamps
             keep = a
-        out_mode = _lib.PSX_OUT_DM if per_dm else _lib.PSX_OUT_TRIAL
+        out_mode = (_lib.PSX_OUT_DM_FOREST if per_dm == "forest" else
+                    _lib.PSX_OUT_DM if per_dm else _lib.PSX_OUT_TRIAL)
         nout = C.c_size_t()
         L = load()
         while True:
@@ -167,11 +168,14 @@ class AccelSearch:
         k = nout.value
         return self._out[:k].copy(), self._na[:k].copy(), self._tr[:k].copy()
 
-    def search_block(self, series, dms, dm_idx=None, per_dm: bool = True):
+    def search_block(self, series, dms, dm_idx=None, per_dm=True):
         """Search a block of DM trials (a sequence of host arrays, a 2-D
         array, or a sequence / 2-D CUDA tensor), overlapping the host-side
         clustering of one DM with the GPU search of the next.  Returns
-        (candidates, nassoc, trial_index, dm_position)."""
+        (candidates, nassoc, trial_index, dm_position).  per_dm="forest"
+        returns each DM's acceleration-distilled candidates with their
+        association trees: a candidate forest whose subtree sizes take the
+        place of nassoc (see peasoup_b200.output)."""
         rows = [series[i] for i in range(len(series))]
         n = len(rows)
         on_dev = int(hasattr(rows[0], "is_cuda") and rows[0].is_cuda)
@@ -186,7 +190,8 @@ class AccelSearch:
             nsamps = arrs[0].size
         dm_arr = np.ascontiguousarray(dms, np.float32)
         idx_arr = np.ascontiguousarray(np.arange(n) if dm_idx is None else dm_idx, np.int32)
-        out_mode = _lib.PSX_OUT_DM if per_dm else _lib.PSX_OUT_TRIAL
+        out_mode = (_lib.PSX_OUT_DM_FOREST if per_dm == "forest" else
+                    _lib.PSX_OUT_DM if per_dm else _lib.PSX_OUT_TRIAL)
         nout = C.c_size_t()
         L = load()
         while True:

@@ -180,6 +180,34 @@ def test_harmonic_kernel_shapes_identical(S, nh):
         assert np.array_equal(c, outs[0])
 
 
+def test_dm_forest_output(S, ref_host):
+    """PSX_OUT_DM_FOREST: the per-DM survivors of PSX_OUT_DM with their
+    association trees, equal to the reference's AccelerationDistiller
+    (keep_related) run on the engine's own per-trial lists."""
+    from peasoup_b200 import output
+    search, synth = S
+    n, ts = 1 << 16, 64e-6
+    xs = np.stack([synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(3e-3 * (d + 1), 15.0 * d, 0.05, 0.9)]), 20 + d)
+        for d in range(3)])
+    dms = np.array([0.0, 1.0, 2.0], np.float32)
+    p = _params(S, n, ts, acc_lo=-80.0, acc_hi=80.0, nharmonics=4, min_snr=6.0, batch=4)
+    s = search.AccelSearch(p)
+    c_dm, na, _, dpos = s.search_block(xs, dms)
+    f_nodes, f_sizes, _, f_pos = s.search_block(xs, dms, per_dm="forest")
+    c_tr, _, _, tpos = s.search_block(xs, dms, per_dm=False)
+    s.close()
+    r = output.roots(f_sizes)
+    assert np.array_equal(f_nodes[r], c_dm) and np.array_equal(f_sizes[r] - 1, na)
+    assert (f_sizes > 1).any()
+    tobs = float(np.float32(n * ts))
+    for d in range(3):
+        got_n, got_s = f_nodes[f_pos == d], f_sizes[f_pos == d]
+        want = ref_host.ref_distill_forest(1, *output.leaves(c_tr[tpos == d]), tol=p.freq_tol,
+                                           tobs=tobs, keep_related=True, fractional=True)
+        assert np.array_equal(got_n, want[0]) and np.array_equal(got_s, want[1])
+
+
 def test_autotune_picks_a_timed_pair(S):
     """The autotuner times every (batch, shape) pair it may use and returns
     the fastest; the tuned engine finds what the default engine finds."""
