@@ -656,6 +656,31 @@ def ref_find_candidates(spec, bin_width, nh, thresh, min_freq, max_freq, min_gap
     return snr[:n.value].copy(), freq[:n.value].copy()
 
 
+def ref_worker_search_forest(series2d, tsamp, dms, fft_size, p: SearchParams,
+                             zapfile: str = ""):
+    """The same run as ref_worker_search; the per-DM candidates with their
+    association trees, as a forest (nodes, subtree sizes)."""
+    s = np.ascontiguousarray(series2d, np.float32)
+    ndm, nsamps = s.shape
+    a = _RefArgs(p.cdm, p.acc_lo, p.acc_hi, p.acc_tol, p.acc_pulse_width * 1e6, p.cfreq,
+                 p.ch_bw, p.nharmonics, p.min_snr, p.min_freq, p.max_freq,
+                 int(p.max_harm), p.freq_tol, zapfile.encode())
+    cap = 1 << 20
+    out = np.zeros(cap, CAND_DTYPE)
+    sz = np.zeros(cap, np.int32)
+    n = C.c_size_t()
+    L = ref_gpu()
+    L.ref_worker_search_forest.restype = C.c_int
+    _chk(L.ref_worker_search_forest(s.reshape(-1).ctypes.data_as(C.c_void_p), C.c_size_t(ndm),
+                                    C.c_size_t(nsamps), C.c_float(tsamp),
+                                    np.ascontiguousarray(dms, np.float32).ctypes.data_as(
+                                        C.c_void_p), C.c_size_t(fft_size), C.byref(a),
+                                    out.ctypes.data_as(C.c_void_p), sz.ctypes.data_as(C.c_void_p),
+                                    C.c_size_t(cap), C.byref(n)),
+         "worker_search_forest")
+    return out[:n.value].copy(), sz[:n.value].copy()
+
+
 def ref_worker_search(series2d, tsamp, dms, fft_size, p: SearchParams, zapfile: str = ""):
     """The reference's unmodified Worker::start over a block of DM trials;
     returns its per-DM acceleration-distilled candidates and their

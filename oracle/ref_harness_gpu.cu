@@ -278,9 +278,19 @@ typedef struct {
    (pipeline_multi.cu:412-421, 523-535).  Writes the per-DM
    acceleration-distilled candidates and, for each, its count of associated
    candidates (Candidate::count_assoc). */
-int ref_worker_search(const float* series, size_t ndm, size_t nsamps, float tsamp,
-                      const float* dms, size_t fft_size, const ref_search_args* a,
-                      ref_candidate* out, int* nassoc, size_t cap, size_t* n_out)
+static void flatten_tree(Candidate& c, std::vector<ref_candidate>& out, std::vector<int>& sizes)
+{
+    const size_t at = out.size();
+    out.push_back(ref_candidate{c.dm, c.dm_idx, c.acc, c.nh, c.snr, c.freq});
+    sizes.push_back(0);
+    for (size_t k = 0; k < c.assoc.size(); ++k) flatten_tree(c.assoc[k], out, sizes);
+    sizes[at] = (int)(out.size() - at);
+}
+
+static int worker_search(const float* series, size_t ndm, size_t nsamps, float tsamp,
+                         const float* dms, size_t fft_size, const ref_search_args* a,
+                         ref_candidate* out, int* nassoc, int* sizes_out, size_t cap,
+                         size_t* n_out)
 {
     return guarded([&] {
         DispersionTrials<float> trials(tsamp);
@@ -310,12 +320,42 @@ int ref_worker_search(const float* series, size_t ndm, size_t nsamps, float tsam
         Worker w(trials, dispenser, plan, args, (unsigned)fft_size, 0);
         w.start();
         std::vector<Candidate>& c = w.dm_trial_cands.cands;
+        if (sizes_out) {
+            // the candidates with their association trees, as a forest
+            std::vector<ref_candidate> f;
+            std::vector<int> fs;
+            for (size_t i = 0; i < c.size(); ++i) flatten_tree(c[i], f, fs);
+            *n_out = f.size();
+            for (size_t i = 0; i < f.size() && i < cap; ++i) {
+                out[i] = f[i];
+                sizes_out[i] = fs[i];
+            }
+            return;
+        }
         *n_out = c.size();
         for (size_t i = 0; i < c.size() && i < cap; ++i) {
             out[i] = ref_candidate{c[i].dm, c[i].dm_idx, c[i].acc, c[i].nh, c[i].snr, c[i].freq};
             if (nassoc) nassoc[i] = c[i].count_assoc();
         }
     });
+}
+
+int ref_worker_search(const float* series, size_t ndm, size_t nsamps, float tsamp,
+                      const float* dms, size_t fft_size, const ref_search_args* a,
+                      ref_candidate* out, int* nassoc, size_t cap, size_t* n_out)
+{
+    return worker_search(series, ndm, nsamps, tsamp, dms, fft_size, a, out, nassoc, nullptr, cap,
+                         n_out);
+}
+
+/* The same run; its per-DM candidates with their association trees as a
+   forest (nodes depth first, subtree sizes). */
+int ref_worker_search_forest(const float* series, size_t ndm, size_t nsamps, float tsamp,
+                             const float* dms, size_t fft_size, const ref_search_args* a,
+                             ref_candidate* out, int* sizes, size_t cap, size_t* n_out)
+{
+    return worker_search(series, ndm, nsamps, tsamp, dms, fft_size, a, out, nullptr, sizes, cap,
+                         n_out);
 }
 
 }  // extern "C"
