@@ -623,6 +623,7 @@ def run_psx(args, ws, rank, local):
     stream = torch.cuda.Stream()
     pr = make_params(plan, "batched", batch, shape)
     pr.graph = not args.no_graph
+    pr.lanes = args.lanes
     eng = search.AccelSearch(pr)
     eng.set_stream(stream.cuda_stream)
 
@@ -798,7 +799,7 @@ def run_psx(args, ws, rank, local):
                                    "acc -100..100, 5 folds, S/N 9, 20 birdies zapped",
                        "dms_per_step": S, "mode": "batched",
                        "batch": batch_used, "harm_shape": shape_used,
-                       "graphs": not args.no_graph,
+                       "graphs": not args.no_graph, "lanes": args.lanes or 1,
                        "tuned": "autotuner (batch x harmonic shape)" if tune else "fixed",
                        "parallelism": f"dm-sharded x{ws}",
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
@@ -823,6 +824,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0,
+                    help="streams the launch groups alternate over (0: the engine's default)")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch the trial schedules directly instead of as CUDA graphs")
     ap.add_argument("--served", type=int, default=SERVED_REQUESTS,

@@ -368,6 +368,10 @@ typedef struct {
     int use_graph;             /* batched: capture the trial schedule */
     int harm_shape;            /* harmonic-kernel tile shape 1..PSX_HARM_SHAPES;
                                   0 = default (psx_autotune picks one) */
+    int lanes;                 /* batched: launch groups alternate over this
+                                  many streams with their own buffers, so one
+                                  group's harmonic sums overlap the next one's
+                                  transform (1 or 2; 0 = 1) */
 } psx_search_config;
 
 /* Number of tile shapes of the fused harmonic-sum kernel (tile bins,

@@ -270,9 +270,12 @@ struct psx_search {
     int F = 0;
     int batch = 1;
     int harm_shape = 1;
+    int lanes = 1;               // streams the launch groups alternate over
     int device = 0;
-    cudaStream_t st = nullptr;   // compute
+    cudaStream_t st = nullptr;   // compute (lane 0)
+    cudaStream_t st2 = nullptr;  // lane 1
     cudaStream_t cst = nullptr;  // record copies
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool own_stream = false;
     double bin_width = 0.0;
     float bin_width_f = 0.f;
@@ -280,6 +283,11 @@ struct psx_search {
     PeakParams pk{};
     float factor[6] = {0, 0, 0, 0, 0, 0};
 
+    // trial buffers of each lane (lane 0 also serves the plain path and the
+    // debug tap); d_tr/d_X/d_p alias lane 0
+    float* d_trl[2] = {nullptr, nullptr};
+    float* d_Xl[2] = {nullptr, nullptr};
+    float* d_pl[2] = {nullptr, nullptr};
     float* d_tr = nullptr;
     float* d_X = nullptr;
     float* d_p = nullptr;
@@ -292,7 +300,7 @@ struct psx_search {
     Slot slot[2];
     FftPlan r2c1;                      // plain-mode trials and the debug tap
     cudaEvent_t call_start = nullptr;  // compute-stream position at a call's start
-    std::map<int, FftPlan*> r2cb;
+    std::map<int, FftPlan*> r2cb[2];  // batched plans per lane, by batch
     std::map<long long, GraphEntry> graphs;
     std::map<long long, int> capture_failures;
 
@@ -315,13 +323,21 @@ struct psx_search {
         if (st) cudaStreamSynchronize(st);
         if (cst) cudaStreamSynchronize(cst);
         drop_graphs();
-        for (auto& p : r2cb) delete p.second;
-        r2cb.clear();
+        if (st2) cudaStreamSynchronize(st2);
+        for (auto& m : r2cb) {
+            for (auto& p : m) delete p.second;
+            m.clear();
+        }
         r2c1.destroy();
-        void* dev[] = {d_tr, d_X, d_p, d_bf, d_bw, d_kbatch};
+        void* dev[] = {d_trl[0], d_Xl[0], d_pl[0], d_trl[1], d_Xl[1], d_pl[1], d_bf, d_bw,
+                       d_kbatch};
         for (void* q : dev)
             if (q) cudaFree(q);
+        for (int l = 0; l < 2; ++l) d_trl[l] = d_Xl[l] = d_pl[l] = nullptr;
         d_tr = d_X = d_p = d_bf = d_bw = nullptr;
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        ev_fork = ev_join = nullptr;
         d_kbatch = nullptr;
         if (call_start) cudaEventDestroy(call_start);
         call_start = nullptr;
@@ -350,6 +366,8 @@ struct psx_search {
         }
         if (cst) cudaStreamDestroy(cst);
         cst = nullptr;
+        if (st2) cudaStreamDestroy(st2);
+        st2 = nullptr;
         if (own_stream && st) cudaStreamDestroy(st);
         st = nullptr;
         own_stream = false;
@@ -358,7 +376,7 @@ struct psx_search {
     bool batched() const { return cfg.mode == PSX_MODE_BATCHED; }
     bool callback() const { return batched() && cfg.use_fft_callback; }
 
-    int get_plan(int b, FftPlan** out);
+    int get_plan(int b, FftPlan** out, int lane = 0);
     int grow_records(Slot& s, size_t need);
     int grow_ktab(Slot& s, size_t need);
     int ensure_events(Slot& s, int groups);
@@ -374,10 +392,10 @@ struct psx_search {
     void read_profile(Slot& s);
 };
 
-int psx_search::get_plan(int b, FftPlan** out)
+int psx_search::get_plan(int b, FftPlan** out, int lane)
 {
-    auto it = r2cb.find(b);
-    if (it != r2cb.end()) {
+    auto it = r2cb[lane].find(b);
+    if (it != r2cb[lane].end()) {
         *out = it->second;
         return PSX_OK;
     }
@@ -389,7 +407,7 @@ int psx_search::get_plan(int b, FftPlan** out)
         delete p;
         return rc;
     }
-    r2cb[b] = p;
+    r2cb[lane][b] = p;
     *out = p;
     return PSX_OK;
 }
@@ -525,46 +543,63 @@ int psx_search::trials_enqueue(Slot& s, int nacc)
     if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2], st));
     const unsigned T = 256;
     const unsigned span = pk.hi > pk.lo ? pk.hi - pk.lo : 0;
+    // launch groups alternate over the lanes; lane 1 starts after the
+    // counter reset and lane 0 waits for lane 1 at the end (fork / join,
+    // also inside a graph capture)
+    const int L = batched() ? lanes : 1;
+    if (L > 1) {
+        PSX_CUDA(cudaEventRecord(ev_fork, st));
+        PSX_CUDA(cudaStreamWaitEvent(st2, ev_fork, 0));
+    }
     int t0 = 0, g = 0;
     while (t0 < nacc) {
+        const int lane = g % L;
+        cudaStream_t ls = lane ? st2 : st;
+        float* tr = d_trl[lane];
+        float* X = d_Xl[lane];
+        float* pp = d_pl[lane];
         int b = 1;
         if (batched()) {
             b = batch;
             while (b > nacc - t0) b >>= 1;
             FftPlan* plan = nullptr;
-            PSX_TRY(get_plan(b, &plan));
+            PSX_TRY(get_plan(b, &plan, lane));
             if (callback()) {
-                PSX_TRY(plan->set_resample(s.d_tim, d_kbatch, st));
+                PSX_TRY(plan->set_resample(s.d_tim, d_kbatch, ls));
                 PSX_CUDA(cudaMemcpyAsync(d_kbatch, s.d_ktab + t0, sizeof(double) * b,
-                                         cudaMemcpyDeviceToDevice, st));
+                                         cudaMemcpyDeviceToDevice, ls));
             } else {
-                PSX_TRY(launch_resample(s.d_tim, d_tr, N, s.d_ktab + t0, 0.0, b, N, false, st));
+                PSX_TRY(launch_resample(s.d_tim, tr, N, s.d_ktab + t0, 0.0, b, N, false, ls));
                 ++s.launches;
             }
-            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], st));
-            PSX_TRY(plan->exec(d_tr, d_X, st));
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], ls));
+            PSX_TRY(plan->exec(tr, X, ls));
             ++s.ffts;
         } else {
-            PSX_TRY(launch_resample(s.d_tim, d_tr, N, s.d_ktab + t0, 0.0, 1, N, false, st));
+            PSX_TRY(launch_resample(s.d_tim, tr, N, s.d_ktab + t0, 0.0, 1, N, false, ls));
             ++s.launches;
-            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], st));
-            PSX_TRY(r2c1.exec(d_tr, d_X, st));
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], ls));
+            PSX_TRY(r2c1.exec(tr, X, ls));
             ++s.ffts;
         }
-        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 1], st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 1], ls));
         dim3 gf(grid_for(B / 2 + 1, T, 4), (unsigned)b);
-        k_form_norm<<<gf, T, 0, st>>>(d_X, 2 * Bp, d_p, Bp, (unsigned)B, s.d_stat);
+        k_form_norm<<<gf, T, 0, ls>>>(X, 2 * Bp, pp, Bp, (unsigned)B, s.d_stat);
         ++s.launches;
         PSX_TRY(launch_status("form kernel"));
-        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 2], st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 2], ls));
         if (span) {
-            PSX_TRY(launch_harm(F, harm_shape, d_p, Bp, (unsigned)Bp, pk, t0, b, s.d_rec, s.d_count,
-                                (unsigned)s.rec_cap, st));
+            PSX_TRY(launch_harm(F, harm_shape, pp, Bp, (unsigned)Bp, pk, t0, b, s.d_rec,
+                                s.d_count, (unsigned)s.rec_cap, ls));
             ++s.launches;
         }
-        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 3], st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 3], ls));
         t0 += b;
         ++g;
+    }
+    if (L > 1) {
+        PSX_CUDA(cudaEventRecord(ev_join, st2));
+        PSX_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     }
     s.groups = g;
     return PSX_OK;
@@ -595,10 +630,11 @@ int psx_search::run_trials(Slot& s, int nacc)
     if (it == graphs.end() && capture_failures[key] >= 2) return trials_enqueue(s, nacc);
     if (it == graphs.end()) {
         // plans must exist before capture (creation allocates)
-        for (int b = batch; b >= 1; b >>= 1) {
-            FftPlan* p = nullptr;
-            PSX_TRY(get_plan(b, &p));
-        }
+        for (int l = 0; l < lanes; ++l)
+            for (int b = batch; b >= 1; b >>= 1) {
+                FftPlan* p = nullptr;
+                PSX_TRY(get_plan(b, &p, l));
+            }
         const int l0 = s.launches, f0 = s.ffts;
         PSX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int rc = trials_enqueue(s, nacc);
@@ -679,7 +715,9 @@ void psx_search::read_profile(Slot& s)
     };
     span(s.ev[0], s.ev[1], prof.prologue_ms);
     for (int g = 0; g < s.groups; ++g) {
-        cudaEvent_t prev = g == 0 ? s.ev[2] : s.ev[3 + 4 * (g - 1) + 3];
+        // the previous group of the same lane (or the start of the trials)
+        const int L = batched() ? lanes : 1;
+        cudaEvent_t prev = g < L ? s.ev[2] : s.ev[3 + 4 * (g - L) + 3];
         cudaEvent_t* e = &s.ev[3 + 4 * g];
         span(prev, e[0], prof.resample_ms);
         span(e[0], e[1], prof.fft_ms);
@@ -896,6 +934,7 @@ void psx_search_config_defaults(psx_search_config* c, size_t fft_size, float tsa
     c->use_fft_callback = 0;
     c->use_graph = 1;
     c->harm_shape = 0;
+    c->lanes = 0;
 }
 
 static int check_config(const psx_search_config* c)
@@ -924,6 +963,10 @@ static int check_config(const psx_search_config* c)
         set_error("search: batch must be 0..1024");
         return PSX_ERR_INVALID;
     }
+    if (c->lanes < 0 || c->lanes > 2) {
+        set_error("search: lanes must be 0..2");
+        return PSX_ERR_INVALID;
+    }
     if (c->harm_shape < 0 || c->harm_shape > PSX_HARM_SHAPES) {
         set_error("search: harm_shape must be 0..%d", PSX_HARM_SHAPES);
         return PSX_ERR_INVALID;
@@ -948,22 +991,31 @@ static int effective_batch(const psx_search_config* c)
     return p;
 }
 
+static int effective_lanes(const psx_search_config* c)
+{
+    if (c->mode != PSX_MODE_BATCHED) return 1;
+    // one lane by default: measured on B200 at 2^23, a second lane did not
+    // raise throughput (the persistent harmonic grid already fills every SM)
+    return c->lanes ? c->lanes : 1;
+}
+
 size_t psx_search_footprint(const psx_search_config* c)
 {
     if (check_config(c) != PSX_OK) return 0;
     const size_t N = c->fft_size, B = N / 2 + 1, Bp = round_up(B, 64);
     const size_t b = (size_t)effective_batch(c);
+    const size_t L = (size_t)effective_lanes(c);
     const bool cb = c->mode == PSX_MODE_BATCHED && c->use_fft_callback;
     size_t bytes = 0;
     bytes += 2 * sizeof(float) * (N + 3 * Bp);        // per slot: series, prologue spectra
     bytes += 2 * median_scratch_bytes(B);
-    bytes += sizeof(float) * N * (cb ? 1 : b);        // resampled series
-    bytes += sizeof(float) * 2 * Bp * b;              // complex spectra
-    bytes += sizeof(float) * Bp * b;                  // normalised spectra
+    bytes += L * sizeof(float) * N * (cb ? 1 : b);    // resampled series, per lane
+    bytes += L * sizeof(float) * 2 * Bp * b;          // complex spectra, per lane
+    bytes += L * sizeof(float) * Bp * b;              // normalised spectra, per lane
     bytes += 2 * sizeof(int4) * ((size_t)1 << 20);    // two initial record slots
-    // cuFFT work areas: about one transform's worth per batched plan size,
-    // plus the batch-1 plans of the two slots' prologues and the plain path
-    bytes += sizeof(float) * 2 * Bp * (2 * b + 6);
+    // cuFFT work areas: about one transform's worth per batched plan size and
+    // lane, plus the batch-1 plans of the two slots' prologues and the plain path
+    bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
     return bytes;
 }
 
@@ -988,6 +1040,7 @@ static void host_setup(psx_search* s, const psx_search_config* cfg)
     s->Bp = round_up(s->B, 64);
     s->F = cfg->nharmonics;
     s->batch = effective_batch(cfg);
+    s->lanes = effective_lanes(cfg);
     s->harm_shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
     unsigned hc = std::thread::hardware_concurrency();
     s->nthreads = (int)std::max(1u, std::min(8u, hc ? hc : 1u));
@@ -1053,9 +1106,14 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     if ((rc = cuda_status(cudaMalloc((void**)&(ptr), (bytes)), "cudaMalloc")) != \
         PSX_OK)                                                                  \
         return fail(rc == PSX_ERR_CUDA ? PSX_ERR_ALLOC : rc);
-    ALLOC(s->d_tr, sizeof(float) * N * (cb ? 1 : b));
-    ALLOC(s->d_X, sizeof(float) * 2 * Bp * b);
-    ALLOC(s->d_p, sizeof(float) * Bp * b);
+    for (int l = 0; l < s->lanes; ++l) {
+        ALLOC(s->d_trl[l], sizeof(float) * N * (cb ? 1 : b));
+        ALLOC(s->d_Xl[l], sizeof(float) * 2 * Bp * b);
+        ALLOC(s->d_pl[l], sizeof(float) * Bp * b);
+    }
+    s->d_tr = s->d_trl[0];
+    s->d_X = s->d_Xl[0];
+    s->d_p = s->d_pl[0];
     ALLOC(s->d_kbatch, sizeof(double) * b);
     for (Slot& sl : s->slot) {
         ALLOC(sl.d_count, sizeof(unsigned) * 4);
@@ -1098,8 +1156,18 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
         cudaMemcpy(s->d_bw, s->bw.data(), sizeof(float) * s->bw.size(), cudaMemcpyHostToDevice);
     }
     // zero the padded tails once so no uninitialised memory is ever read
-    cudaMemsetAsync(s->d_X, 0, sizeof(float) * 2 * Bp * b, s->st);
-    cudaMemsetAsync(s->d_p, 0, sizeof(float) * Bp * b, s->st);
+    for (int l = 0; l < s->lanes; ++l) {
+        cudaMemsetAsync(s->d_Xl[l], 0, sizeof(float) * 2 * Bp * b, s->st);
+        cudaMemsetAsync(s->d_pl[l], 0, sizeof(float) * Bp * b, s->st);
+    }
+    if (s->lanes > 1) {
+        if ((rc = cuda_status(cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking),
+                              "cudaStreamCreate")) != PSX_OK)
+            return fail(rc);
+        if (cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
+            return fail(PSX_ERR_CUDA);
+    }
     cudaMemsetAsync(s->d_kbatch, 0, sizeof(double) * b, s->st);
     for (Slot& sl : s->slot) {
         cudaMemsetAsync(sl.d_Xp, 0, sizeof(float) * 2 * Bp, s->st);
@@ -1110,7 +1178,8 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     if ((rc = s->r2c1.create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
     if (s->batched()) {
         FftPlan* p = nullptr;
-        if ((rc = s->get_plan(s->batch, &p)) != PSX_OK) return fail(rc);
+        for (int l = 0; l < s->lanes; ++l)
+            if ((rc = s->get_plan(s->batch, &p, l)) != PSX_OK) return fail(rc);
     }
     if ((rc = cuda_status(cudaStreamSynchronize(s->st), "search create")) != PSX_OK)
         return fail(rc);
@@ -1140,9 +1209,10 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     const int shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
     const bool cb = cfg->mode == PSX_MODE_BATCHED && cfg->use_fft_callback;
     if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
-        effective_batch(cfg) != s->batch || shape != s->harm_shape || cb != s->callback()) {
-        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape and callback "
-                  "must match the instance");
+        effective_batch(cfg) != s->batch || shape != s->harm_shape || cb != s->callback() ||
+        effective_lanes(cfg) != s->lanes) {
+        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, callback and "
+                  "lanes must match the instance");
         return PSX_ERR_INVALID;
     }
     PSX_CUDA(cudaSetDevice(s->device));

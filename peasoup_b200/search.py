@@ -57,6 +57,7 @@ class SearchParams:
     fft_callback: bool = False
     graph: bool = True             # batched: CUDA-graph trial schedule
     harm_shape: int = 0            # harmonic-kernel tile shape (0 = default)
+    lanes: int = 0                 # batched: streams the launch groups alternate over (0 = 1)
 
     def to_c(self):
         cfg = SearchConfig()
@@ -76,6 +77,7 @@ class SearchParams:
         cfg.use_fft_callback = int(self.fft_callback)
         cfg.use_graph = int(self.graph)
         cfg.harm_shape = int(self.harm_shape)
+        cfg.lanes = int(self.lanes)
         return cfg, keep
 
 

@@ -208,6 +208,27 @@ def test_dm_forest_output(S, ref_host):
         assert np.array_equal(got_n, want[0]) and np.array_equal(got_s, want[1])
 
 
+@pytest.mark.parametrize("graph", [False, True])
+def test_two_lanes_identical(S, graph):
+    """Launch groups alternating over two streams (own buffers and plans,
+    fork/join, also inside a captured graph) give the one-lane result."""
+    search, synth = S
+    n, ts = 1 << 16, 64e-6
+    x = synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(2.9e-3, -25.0, 0.05, 0.8)]), 31)
+    outs = []
+    for lanes in (1, 2):
+        s = search.AccelSearch(_params(S, n, ts, acc_lo=-150.0, acc_hi=150.0, nharmonics=5,
+                                       min_snr=5.5, batch=4, lanes=lanes, graph=graph))
+        outs.append(s.search(x, 0.0, 0, per_dm=False)[0])
+        outs.append(s.search(x, 0.0, 0, per_dm=False)[0])   # replay
+        assert s.info()["graph"] == int(graph)
+        s.close()
+    assert len(outs[0]) > 5
+    for c in outs[1:]:
+        assert np.array_equal(c, outs[0])
+
+
 def test_autotune_picks_a_timed_pair(S):
     """The autotuner times every (batch, shape) pair it may use and returns
     the fastest; the tuned engine finds what the default engine finds."""
