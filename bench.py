@@ -624,6 +624,7 @@ def run_psx(args, ws, rank, local):
     pr = make_params(plan, "batched", batch, shape)
     pr.graph = not args.no_graph
     pr.lanes = args.lanes
+    pr.fft_form = args.fft_form
     eng = search.AccelSearch(pr)
     eng.set_stream(stream.cuda_stream)
 
@@ -800,6 +801,8 @@ def run_psx(args, ws, rank, local):
                        "dms_per_step": S, "mode": "batched",
                        "batch": batch_used, "harm_shape": shape_used,
                        "graphs": not args.no_graph, "lanes": args.lanes or 1,
+                       "fft_form": "real transform + form" if args.fft_form == 2 else
+                                   "complex transform + fused unpack/interbin/normalise",
                        "tuned": "autotuner (batch x harmonic shape)" if tune else "fixed",
                        "parallelism": f"dm-sharded x{ws}",
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
@@ -824,6 +827,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fft-form", type=int, default=0,
+                    help="1: complex transform + fused unpack/interbin/normalise (default); "
+                         "2: the reference's real transform + interbin/normalise")
     ap.add_argument("--lanes", type=int, default=0,
                     help="streams the launch groups alternate over (0: the engine's default)")
     ap.add_argument("--no-graph", action="store_true",

@@ -372,6 +372,11 @@ typedef struct {
                                   many streams with their own buffers, so one
                                   group's harmonic sums overlap the next one's
                                   transform (1 or 2; 0 = 1) */
+    int fft_form;              /* batched: 0 = default (1); 1 = complex transform
+                                  of the series read as interleaved pairs, then
+                                  one kernel that unpacks the real spectrum,
+                                  interbins and normalises; 2 = the reference's
+                                  real transform, then interbin + normalise */
 } psx_search_config;
 
 /* Number of tile shapes of the fused harmonic-sum kernel (tile bins,

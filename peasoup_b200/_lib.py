@@ -61,7 +61,7 @@ class SearchConfig(C.Structure):
                 ("birdie_freqs", C.POINTER(C.c_float)), ("birdie_widths", C.POINTER(C.c_float)),
                 ("nbirdies", C.c_size_t), ("mode", C.c_int), ("batch", C.c_int),
                 ("use_fft_callback", C.c_int), ("use_graph", C.c_int), ("harm_shape", C.c_int),
-                ("lanes", C.c_int)]
+                ("lanes", C.c_int), ("fft_form", C.c_int)]
 
 
 class SearchInfo(C.Structure):

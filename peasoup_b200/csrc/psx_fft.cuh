@@ -9,6 +9,10 @@ namespace psx {
 
 bool fft_size_supported(size_t n);
 
+// Internal plan kind (beside PSX_FFT_R2C / PSX_FFT_C2R): forward complex
+// transform of length n, distances in complex elements.
+constexpr int kFftC2C = 100;
+
 struct FftPlan {
     cufftHandle h = 0;
     bool have = false;

@@ -70,6 +70,70 @@ __global__ void __launch_bounds__(256) k_form_norm(const float* __restrict__ X, 
     }
 }
 
+// The real spectrum of a length-N series from the complex transform Z of
+// length M = N/2 of z[n] = x[2n] + i x[2n+1] (the series read as interleaved
+// pairs), unpacked, interbinned and normalised in one pass: for j and M - j
+//   X[j]   = ((ar + u) + i (ai - v)) / 2,  X[M-j] = ((ar - u) + i (-ai - v)) / 2
+// with Z[j] = (zr, zi), Z[M-j] = (wr, wi), ar = zr + wr, ai = zi - wi,
+// br = zr - wr, bi = zi + wi, u = c bi - s br, v = s bi + c br and
+// (c, s) = (cos, sin)(pi j / M).  It is the step cuFFT's R2C runs after its
+// complex passes, merged with the interbinning and normalisation of the
+// reference (src/kernels.cu:238-259, :496-507) that come next.  Each thread
+// takes the four bins k0..k0+3 (k0 = 4q) and their mirrors M-k0-3..M-k0;
+// the previous bin each interbin value needs is one more unpacked pair.
+// M is a multiple of 8; thread 0 also forms bin M/2.
+__device__ __forceinline__ void unpack_pair(const float2* __restrict__ z, unsigned M, unsigned j,
+                                            float inv_m, float2& lo, float2& hi)
+{
+    const float2 a = z[j], w = z[j ? M - j : 0];
+    const float ar = a.x + w.x, ai = a.y - w.y, br = a.x - w.x, bi = a.y + w.y;
+    float sn, cs;
+    sincospif((float)j * inv_m, &sn, &cs);
+    const float u = cs * bi - sn * br, v = sn * bi + cs * br;
+    lo = make_float2(0.5f * (ar + u), 0.5f * (ai - v));
+    hi = make_float2(0.5f * (ar - u), 0.5f * (-ai - v));
+}
+
+__global__ void __launch_bounds__(256) k_unpack_form_norm(const float* __restrict__ Zf, size_t zpitch,
+                                                          float* __restrict__ p, size_t ppitch,
+                                                          unsigned M, float inv_m,
+                                                          const float* __restrict__ stat)
+{
+    const float meanN = stat[3], stdN = stat[4];
+    const float2* z = reinterpret_cast<const float2*>(Zf) + (size_t)blockIdx.y * zpitch;
+    float* o = p + (size_t)blockIdx.y * ppitch;
+    const unsigned Q = M / 8;
+    const unsigned stride = gridDim.x * blockDim.x;
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < Q; q += stride) {
+        const unsigned k0 = 4 * q;
+        float2 lo[6], hi[6];  // X[k0-1+t], X[M-(k0-1+t)], t = 0..5
+        if (k0 == 0) {
+            lo[0] = hi[0] = make_float2(0.f, 0.f);  // X[-1] := 0; hi[0] is never used
+        } else {
+            unpack_pair(z, M, k0 - 1, inv_m, lo[0], hi[0]);
+        }
+#pragma unroll
+        for (int t = 1; t < 6; ++t) unpack_pair(z, M, k0 - 1 + t, inv_m, lo[t], hi[t]);
+        float4 r;
+        r.x = normalise(interbin(lo[1].x, lo[1].y, lo[0].x, lo[0].y), meanN, stdN);
+        r.y = normalise(interbin(lo[2].x, lo[2].y, lo[1].x, lo[1].y), meanN, stdN);
+        r.z = normalise(interbin(lo[3].x, lo[3].y, lo[2].x, lo[2].y), meanN, stdN);
+        r.w = normalise(interbin(lo[4].x, lo[4].y, lo[3].x, lo[3].y), meanN, stdN);
+        reinterpret_cast<float4*>(o)[q] = r;
+        // bins M - k0 - t use X[M - k0 - t] (hi[t+1]) and X[M - k0 - t - 1] (hi[t+2])
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            o[M - k0 - t] = normalise(interbin(hi[t + 1].x, hi[t + 1].y, hi[t + 2].x, hi[t + 2].y),
+                                      meanN, stdN);
+        if (q == 0) {  // bin M/2 (its own mirror) with bin M/2 - 1
+            float2 a, b, c, d;
+            unpack_pair(z, M, M / 2, inv_m, a, b);
+            unpack_pair(z, M, M / 2 - 1, inv_m, c, d);
+            o[M / 2] = normalise(interbin(a.x, a.y, c.x, c.y), meanN, stdN);
+        }
+    }
+}
+
 // One pass of the device-side baseline loop (reference src/kernels.cu:
 // 463-479): while state[0] (active) is set, the float mean of the block
 // partials (float sum / float count, as the reference forms it) is
@@ -375,6 +439,8 @@ struct psx_search {
 
     bool batched() const { return cfg.mode == PSX_MODE_BATCHED; }
     bool callback() const { return batched() && cfg.use_fft_callback; }
+    // batched trials through the complex transform + fused unpack kernel
+    bool fused_form() const { return batched() && !callback() && cfg.fft_form != 2; }
 
     int get_plan(int b, FftPlan** out, int lane = 0);
     int grow_records(Slot& s, size_t need);
@@ -401,7 +467,10 @@ int psx_search::get_plan(int b, FftPlan** out, int lane)
     }
     FftPlan* p = new (std::nothrow) FftPlan;
     if (!p) return PSX_ERR_ALLOC;
-    int rc = p->create(N, b, PSX_FFT_R2C, N, Bp, callback());
+    // fused form: a complex transform of length N/2 over the series read as
+    // interleaved pairs (row distances in complex elements)
+    int rc = fused_form() ? p->create(N / 2, b, kFftC2C, N / 2, Bp, false)
+                          : p->create(N, b, PSX_FFT_R2C, N, Bp, callback());
     if (rc == PSX_OK && callback()) rc = p->set_resample(slot[0].d_tim, d_kbatch, st);
     if (rc != PSX_OK) {
         delete p;
@@ -583,8 +652,14 @@ int psx_search::trials_enqueue(Slot& s, int nacc)
             ++s.ffts;
         }
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 1], ls));
-        dim3 gf(grid_for(B / 2 + 1, T, 4), (unsigned)b);
-        k_form_norm<<<gf, T, 0, ls>>>(X, 2 * Bp, pp, Bp, (unsigned)B, s.d_stat);
+        if (fused_form()) {
+            const unsigned M = (unsigned)(N / 2);
+            dim3 gu(grid_for(M / 8, T, 4), (unsigned)b);
+            k_unpack_form_norm<<<gu, T, 0, ls>>>(X, Bp, pp, Bp, M, 1.0f / (float)M, s.d_stat);
+        } else {
+            dim3 gf(grid_for(B / 2 + 1, T, 4), (unsigned)b);
+            k_form_norm<<<gf, T, 0, ls>>>(X, 2 * Bp, pp, Bp, (unsigned)B, s.d_stat);
+        }
         ++s.launches;
         PSX_TRY(launch_status("form kernel"));
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 2], ls));
@@ -935,6 +1010,7 @@ void psx_search_config_defaults(psx_search_config* c, size_t fft_size, float tsa
     c->use_graph = 1;
     c->harm_shape = 0;
     c->lanes = 0;
+    c->fft_form = 0;
 }
 
 static int check_config(const psx_search_config* c)
@@ -961,6 +1037,10 @@ static int check_config(const psx_search_config* c)
     }
     if (c->batch < 0 || c->batch > 1024) {
         set_error("search: batch must be 0..1024");
+        return PSX_ERR_INVALID;
+    }
+    if (c->fft_form < 0 || c->fft_form > 2) {
+        set_error("search: fft_form must be 0..2");
         return PSX_ERR_INVALID;
     }
     if (c->lanes < 0 || c->lanes > 2) {
@@ -1210,7 +1290,8 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     const bool cb = cfg->mode == PSX_MODE_BATCHED && cfg->use_fft_callback;
     if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
         effective_batch(cfg) != s->batch || shape != s->harm_shape || cb != s->callback() ||
-        effective_lanes(cfg) != s->lanes) {
+        effective_lanes(cfg) != s->lanes ||
+        (cfg->fft_form == 2) != (s->cfg.fft_form == 2)) {
         set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, callback and "
                   "lanes must match the instance");
         return PSX_ERR_INVALID;

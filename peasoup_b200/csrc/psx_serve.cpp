@@ -41,18 +41,19 @@ using Clock = std::chrono::steady_clock;
 
 struct EngineKey {
     size_t n;
-    int folds, mode, batch, shape, callback, lanes;
+    int folds, mode, batch, shape, callback, lanes, form;
     bool operator==(const EngineKey& o) const
     {
         return n == o.n && folds == o.folds && mode == o.mode && batch == o.batch &&
-               shape == o.shape && callback == o.callback && lanes == o.lanes;
+               shape == o.shape && callback == o.callback && lanes == o.lanes &&
+               form == o.form;
     }
 };
 
 EngineKey key_of(const psx_search_config& c)
 {
     return {c.fft_size, c.nharmonics, c.mode, c.batch, c.harm_shape,
-            c.mode == PSX_MODE_BATCHED && c.use_fft_callback ? 1 : 0, c.lanes};
+            c.mode == PSX_MODE_BATCHED && c.use_fft_callback ? 1 : 0, c.lanes, c.fft_form};
 }
 
 struct Engine {

@@ -58,6 +58,8 @@ class SearchParams:
     graph: bool = True             # batched: CUDA-graph trial schedule
     harm_shape: int = 0            # harmonic-kernel tile shape (0 = default)
     lanes: int = 0                 # batched: streams the launch groups alternate over (0 = 1)
+    fft_form: int = 0              # batched: 1 complex transform + fused unpack/interbin (default),
+                                   # 2 the reference's real transform + interbin
 
     def to_c(self):
         cfg = SearchConfig()
@@ -78,6 +80,7 @@ class SearchParams:
         cfg.use_graph = int(self.graph)
         cfg.harm_shape = int(self.harm_shape)
         cfg.lanes = int(self.lanes)
+        cfg.fft_form = int(self.fft_form)
         return cfg, keep
 
 
