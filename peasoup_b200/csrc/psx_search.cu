@@ -106,14 +106,41 @@ __global__ void __launch_bounds__(256) k_unpack_form_norm(const float* __restric
     const unsigned stride = gridDim.x * blockDim.x;
     for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < Q; q += stride) {
         const unsigned k0 = 4 * q;
-        float2 lo[6], hi[6];  // X[k0-1+t], X[M-(k0-1+t)], t = 0..5
+        // Z[k0-1+t] and Z[(M-(k0-1+t)) mod M], t = 0..5: the four interior
+        // pairs of each side with two 128-bit loads (k0 and M-k0-4 are even)
+        float2 zl[6], zh[6];
+        const float4* z4 = reinterpret_cast<const float4*>(z);
+        const float4 l0 = z4[k0 / 2], l1 = z4[k0 / 2 + 1];
+        const float4 h0 = z4[(M - k0 - 4) / 2], h1 = z4[(M - k0 - 4) / 2 + 1];
+        zl[1] = make_float2(l0.x, l0.y);
+        zl[2] = make_float2(l0.z, l0.w);
+        zl[3] = make_float2(l1.x, l1.y);
+        zl[4] = make_float2(l1.z, l1.w);
+        zl[5] = z[k0 + 4];
+        zh[5] = make_float2(h0.x, h0.y);  // Z[M-k0-4]
+        zh[4] = make_float2(h0.z, h0.w);  // Z[M-k0-3]
+        zh[3] = make_float2(h1.x, h1.y);  // Z[M-k0-2]
+        zh[2] = make_float2(h1.z, h1.w);  // Z[M-k0-1]
         if (k0 == 0) {
-            lo[0] = hi[0] = make_float2(0.f, 0.f);  // X[-1] := 0; hi[0] is never used
+            zl[0] = zh[0] = make_float2(0.f, 0.f);
+            zh[1] = zl[1];  // j = 0 is its own mirror
         } else {
-            unpack_pair(z, M, k0 - 1, inv_m, lo[0], hi[0]);
+            zl[0] = z[k0 - 1];
+            zh[0] = z[M - k0 + 1];
+            zh[1] = z[M - k0];
         }
+        float2 lo[6], hi[6];  // X[k0-1+t], X[M-(k0-1+t)]
 #pragma unroll
-        for (int t = 1; t < 6; ++t) unpack_pair(z, M, k0 - 1 + t, inv_m, lo[t], hi[t]);
+        for (int t = 0; t < 6; ++t) {
+            const float2 a = zl[t], w = zh[t];
+            const float ar = a.x + w.x, ai = a.y - w.y, br = a.x - w.x, bi = a.y + w.y;
+            float sn, cs;
+            sincospif((float)((int)k0 + t - 1) * inv_m, &sn, &cs);
+            const float u = cs * bi - sn * br, v = sn * bi + cs * br;
+            lo[t] = make_float2(0.5f * (ar + u), 0.5f * (ai - v));
+            hi[t] = make_float2(0.5f * (ar - u), 0.5f * (-ai - v));
+        }
+        if (k0 == 0) lo[0] = make_float2(0.f, 0.f);  // X[-1] := 0; hi[0] is not used
         float4 r;
         r.x = normalise(interbin(lo[1].x, lo[1].y, lo[0].x, lo[0].y), meanN, stdN);
         r.y = normalise(interbin(lo[2].x, lo[2].y, lo[1].x, lo[1].y), meanN, stdN);
@@ -448,6 +475,7 @@ struct psx_search {
     int ensure_events(Slot& s, int groups);
     int prologue(Slot& s);
     int trials_enqueue(Slot& s, int nacc);
+    int trials_range(Slot& s, int t_begin, int t_end, bool reset);
     int run_trials(Slot& s, int nacc);
     int enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
                 int dm_idx);
@@ -608,8 +636,18 @@ int psx_search::prologue(Slot& s)
 // s.d_ktab) plus the reset of the record counter.
 int psx_search::trials_enqueue(Slot& s, int nacc)
 {
-    PSX_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned) * 2, st));
-    if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2], st));
+    s.groups = 0;
+    return trials_range(s, 0, nacc, true);
+}
+
+// Enqueues trials [t_begin, t_end) of the DM in launch groups (numbered on
+// from s.groups), after the reset of the record counter when `reset`.
+int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
+{
+    if (reset) {
+        PSX_CUDA(cudaMemsetAsync(s.d_count, 0, sizeof(unsigned) * 2, st));
+        if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[2], st));
+    }
     const unsigned T = 256;
     const unsigned span = pk.hi > pk.lo ? pk.hi - pk.lo : 0;
     // launch groups alternate over the lanes; lane 1 starts after the
@@ -620,7 +658,7 @@ int psx_search::trials_enqueue(Slot& s, int nacc)
         PSX_CUDA(cudaEventRecord(ev_fork, st));
         PSX_CUDA(cudaStreamWaitEvent(st2, ev_fork, 0));
     }
-    int t0 = 0, g = 0;
+    int t0 = t_begin, g = s.groups;
     while (t0 < nacc) {
         const int lane = g % L;
         cudaStream_t ls = lane ? st2 : st;
@@ -700,8 +738,19 @@ int psx_search::run_trials(Slot& s, int nacc)
     const bool graph = batched() && cfg.use_graph && !s.profiled;
     if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
     if (!graph) return trials_enqueue(s, nacc);
-    const long long key = ((long long)nacc << 2) | ((&s == &slot[1]) ? 2 : 0) | (s.profiled ? 1 : 0);
+    // One lane: the graph holds the counter reset and the full launch groups
+    // and is keyed by their number, which neighbouring DM trials share (the
+    // trial count changes slowly with DM), so few graphs are captured; the
+    // shorter tail groups are launched directly after it.  Two lanes: one
+    // graph per trial count.
+    const int upto = lanes == 1 ? (nacc / batch) * batch : nacc;
+    if (upto == 0) return trials_enqueue(s, nacc);
+    const long long key = ((long long)upto << 2) | ((&s == &slot[1]) ? 2 : 0);
     auto it = graphs.find(key);
+    auto tail = [&]() -> int {
+        if (upto >= nacc) return PSX_OK;
+        return trials_range(s, upto, nacc, false);
+    };
     if (it == graphs.end() && capture_failures[key] >= 2) return trials_enqueue(s, nacc);
     if (it == graphs.end()) {
         // plans must exist before capture (creation allocates)
@@ -712,7 +761,7 @@ int psx_search::run_trials(Slot& s, int nacc)
             }
         const int l0 = s.launches, f0 = s.ffts;
         PSX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        int rc = trials_enqueue(s, nacc);
+        int rc = trials_enqueue(s, upto);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (rc != PSX_OK || e != cudaSuccess) {
@@ -744,6 +793,7 @@ int psx_search::run_trials(Slot& s, int nacc)
     s.launches += it->second.launches;
     s.ffts += it->second.ffts;
     s.groups = it->second.groups;
+    PSX_TRY(tail());
     return PSX_OK;
 }
 
