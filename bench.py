@@ -616,7 +616,7 @@ def run_psx(args, ws, rank, local):
     batch, shape = args.batch, 0
     if not args.batch:
         t0 = time.perf_counter()
-        tune = search.autotune(make_params(plan, "batched"), batches=(2, 4, 8, 16), reps=2)
+        tune = search.autotune(make_params(plan, "batched"), batches=(4, 8, 16, 32), reps=2)
         batch, shape = tune["batch"], tune["harm_shape"]
         log(f"[rank {rank}] autotune: batch {batch}, harmonic shape {shape} "
             f"({time.perf_counter() - t0:.1f}s)")
