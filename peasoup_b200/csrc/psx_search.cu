@@ -94,9 +94,15 @@ __device__ __forceinline__ void unpack_pair(const float2* __restrict__ z, unsign
     hi = make_float2(0.5f * (ar - u), 0.5f * (-ai - v));
 }
 
+// (cos, sin)(pi d / M) for d = -1 .. 4, rounded once from double: the
+// twiddles of a thread's six pairs are W(k0) times these.
+struct TwSteps {
+    float2 w[6];
+};
+
 __global__ void __launch_bounds__(256) k_unpack_form_norm(const float* __restrict__ Zf, size_t zpitch,
                                                           float* __restrict__ p, size_t ppitch,
-                                                          unsigned M, float inv_m,
+                                                          unsigned M, float inv_m, TwSteps steps,
                                                           const float* __restrict__ stat)
 {
     const float meanN = stat[3], stdN = stat[4];
@@ -130,12 +136,14 @@ __global__ void __launch_bounds__(256) k_unpack_form_norm(const float* __restric
             zh[1] = z[M - k0];
         }
         float2 lo[6], hi[6];  // X[k0-1+t], X[M-(k0-1+t)]
+        float s0, c0;
+        sincospif((float)k0 * inv_m, &s0, &c0);  // one call per thread
 #pragma unroll
         for (int t = 0; t < 6; ++t) {
             const float2 a = zl[t], w = zh[t];
             const float ar = a.x + w.x, ai = a.y - w.y, br = a.x - w.x, bi = a.y + w.y;
-            float sn, cs;
-            sincospif((float)((int)k0 + t - 1) * inv_m, &sn, &cs);
+            const float2 d = steps.w[t];  // angle of pair k0-1+t = angle(k0) + angle(t-1)
+            const float cs = c0 * d.x - s0 * d.y, sn = s0 * d.x + c0 * d.y;
             const float u = cs * bi - sn * br, v = sn * bi + cs * br;
             lo[t] = make_float2(0.5f * (ar + u), 0.5f * (ai - v));
             hi[t] = make_float2(0.5f * (ar - u), 0.5f * (-ai - v));
@@ -387,6 +395,7 @@ struct psx_search {
     size_t bird_cap = 0;  // entries d_bf / d_bw hold
     double* d_kbatch = nullptr;
     float* h_mean = nullptr;
+    TwSteps tw_steps{};  // unit rotations of the fused unpack kernel
 
     Slot slot[2];
     FftPlan r2c1;                      // plain-mode trials and the debug tap
@@ -693,7 +702,8 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
         if (fused_form()) {
             const unsigned M = (unsigned)(N / 2);
             dim3 gu(grid_for(M / 8, T, 4), (unsigned)b);
-            k_unpack_form_norm<<<gu, T, 0, ls>>>(X, Bp, pp, Bp, M, 1.0f / (float)M, s.d_stat);
+            k_unpack_form_norm<<<gu, T, 0, ls>>>(X, Bp, pp, Bp, M, 1.0f / (float)M, tw_steps,
+                                                 s.d_stat);
         } else {
             dim3 gf(grid_for(B / 2 + 1, T, 4), (unsigned)b);
             k_form_norm<<<gf, T, 0, ls>>>(X, 2 * Bp, pp, Bp, (unsigned)B, s.d_stat);
@@ -1172,6 +1182,12 @@ static void host_setup(psx_search* s, const psx_search_config* cfg)
     s->batch = effective_batch(cfg);
     s->lanes = effective_lanes(cfg);
     s->harm_shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
+    {
+        const double M = (double)(s->N / 2), pi = 3.14159265358979323846;
+        for (int t = 0; t < 6; ++t)
+            s->tw_steps.w[t] = make_float2((float)std::cos(pi * (t - 1) / M),
+                                           (float)std::sin(pi * (t - 1) / M));
+    }
     unsigned hc = std::thread::hardware_concurrency();
     s->nthreads = (int)std::max(1u, std::min(8u, hc ? hc : 1u));
     // pipeline_multi.cu:126-128: tobs and bin width are floats
