@@ -475,7 +475,7 @@ def run_config3(args):
                                    nharmonics=4, min_snr=7.0, cfreq_hz=synth.CFREQ_HZ,
                                    ch_bw_hz=synth.CH_BW_HZ, mode=mode, batch=batch,
                                    harm_shape=shape)
-    tune = search.autotune(params("batched"), batches=(2, 4, 8, 16), reps=4)
+    tune = search.autotune(params("batched"), batches=(4, 8, 16, 32), reps=4)
     ap = AccelerationPlan(-50.0, 50.0, 1.10, 64e-6, n, ts, synth.CFREQ_HZ, synth.CH_BW_HZ)
     ntr = [len(ap.generate_accel_list(float(d), 0.0)) for d in dms]
     stream = torch.cuda.Stream()
@@ -562,7 +562,7 @@ def run_config5(args):
         a = AccelerationPlan(-half, half, 1.10, 64e-6, n, ts, synth.CFREQ_HZ, synth.CH_BW_HZ)
         return sum(len(a.generate_accel_list(float(plan.dms[d]), 0.0)) for d in dlist)
 
-    tune = search.autotune(params("batched", 500.0), batches=(2, 4, 8, 16), reps=1,
+    tune = search.autotune(params("batched", 500.0), batches=(2, 4, 8), reps=1,
                            max_trials=64)
     stream = torch.cuda.Stream()
     rows = [block[i] for i in range(nuse)]
@@ -627,7 +627,7 @@ def run_psx(args, ws, rank, local):
     batch, shape = args.batch, 0
     if not args.batch:
         t0 = time.perf_counter()
-        tune = search.autotune(make_params(plan, "batched"), batches=(4, 8, 16, 32), reps=2)
+        tune = search.autotune(make_params(plan, "batched"), batches=(8, 16, 32, 64), reps=2)
         batch, shape = tune["batch"], tune["harm_shape"]
         log(f"[rank {rank}] autotune: batch {batch}, harmonic shape {shape} "
             f"({time.perf_counter() - t0:.1f}s)")

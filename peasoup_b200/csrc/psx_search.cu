@@ -303,9 +303,12 @@ namespace {
 
 size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 
+// Untuned trials per launch group: about 2^28 samples (1 GB of resampled
+// series) per group, 1..32; cuFFT's batched transforms get faster with the
+// batch up to that size on B200 (psx_autotune picks per configuration).
 int default_batch(size_t n)
 {
-    size_t b = ((size_t)1 << 25) / n;
+    size_t b = ((size_t)1 << 28) / n;
     if (b < 1) b = 1;
     if (b > 32) b = 32;
     size_t p = 1;
