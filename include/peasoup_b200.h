@@ -190,6 +190,26 @@ int psx_find_peaks_noalloc(const float* d_spec, int n, int start, float thresh,
                            int* d_idx, float* d_val, int cap, int* h_count,
                            psx_stream_t stream);
 
+/* Fused fractional harmonic sums, threshold test and compaction over `rows`
+   normalised spectra of nbins bins (row r at d_spec + r*pitch; pitch a
+   multiple of 4 floats, d_spec 16-byte aligned): for every fold h in
+   0..nharms (0 = the spectrum itself) and bin i in [h_start[h], h_end[h])
+   whose fold value exceeds `thresh`, one record of four ints {row, h, i,
+   the value's float bits} is appended to d_records (order unspecified;
+   the folds are never written).  Sums, scales and order are the
+   reference's (src/kernels.cu:34-100); this replaces the pair
+   HarmonicFolder::fold + PeakFinder's device_find_peaks per fold
+   (harmonicfolder.hpp:26-38, kernels.cu:398-423).  *h_count = records (the
+   need, with PSX_ERR_OVERFLOW).  Every barrier wait of the kernel is
+   bounded by wait_limit polls (0 = the default); one that runs out makes
+   the call fail with PSX_ERR_CUDA and a message, and leaves the context
+   usable.  flags: 0, or 1 to stage nothing, so that the waits run out (a
+   test of that path).  Synchronous. */
+int psx_harmonic_peaks(const float* d_spec, size_t pitch, size_t nbins, int rows,
+                       int nharms, const int* h_start, const int* h_end,
+                       float thresh, int* d_records, size_t cap, size_t* h_count,
+                       unsigned wait_limit, unsigned flags, psx_stream_t stream);
+
 /* ------------------------------------------------------------------ */
 /* Real transforms (cuFFT)                                             */
 /* ------------------------------------------------------------------ */

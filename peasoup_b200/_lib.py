@@ -127,6 +127,8 @@ SIGNATURES = {
     "psx_harmonic_sum": (_i, [_vp, _vp, _sz, _i, _vp]),
     "psx_find_peaks": (_i, [_vp, _i, _i, _f, _vp, _vp, _i, C.POINTER(_i), _vp]),
     "psx_find_peaks_noalloc": (_i, [_vp, _i, _i, _f, _vp, _vp, _i, C.POINTER(_i), _vp]),
+    "psx_harmonic_peaks": (_i, [_vp, _sz, _sz, _i, _i, _vp, _vp, _f, _vp, _sz, C.POINTER(_sz),
+                                C.c_uint, C.c_uint, _vp]),
     "psx_fft_plan_create": (_i, [C.POINTER(_vp), _sz, C.c_longlong, _i]),
     "psx_fft_exec": (_i, [_vp, _vp, _vp, _vp]),
     "psx_fft_plan_destroy": (_i, [_vp]),

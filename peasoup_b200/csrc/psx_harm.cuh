@@ -35,7 +35,16 @@ struct PeakParams {
     unsigned lo, hi;  // union of the ranges; lo is rounded down to 128
     float thresh;
     float vote;       // fast-pass vote level: thresh lowered by 2^-20 relative
+    unsigned wait_limit;  // polls of one bounded barrier wait (kHarmWaitLimit)
+    unsigned flags;       // kHarmNoCopies: stage nothing (every wait runs out)
 };
+
+// Default bound of one barrier wait (polls; each may suspend briefly).
+constexpr unsigned kHarmWaitLimit = 1u << 22;
+// Test hook: the producer arrives on the stage barriers but issues no
+// copies, so the consumers' waits run out and the timeout path runs
+// (no fault: every wait is bounded and nothing is left in flight).
+constexpr unsigned kHarmNoCopies = 1u;
 
 // Packed two-lane float arithmetic (sm_100): one instruction for two
 // independent IEEE round-to-nearest operations.
@@ -359,7 +368,9 @@ __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
 // (row, tile) are taken round-robin over the grid.  full[s] completes when
 // a stage's bytes have landed, empty[s] when every consumer warp is done
 // with it.  No CTA-wide barrier is used in the loop; every wait is bounded
-// and a timeout is reported in counter[1].
+// (pp.wait_limit polls).  A wait that runs out sets a CTA-wide abort flag:
+// both sides stop at their next item, the copies already issued are waited
+// for (bounded) before the CTA exits, and counter[1] reports the timeout.
 template <int F, int T, int NC, int MINB, bool OOL>
 __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __restrict__ p,
                                                            size_t ppitch, unsigned row_len,
@@ -372,9 +383,13 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
     static_assert(T % 128 == 0 && NC % 32 == 0 && T % (2 * NC) == 0, "tile shape");
     constexpr int STAGE = harm_smem_floats(F, T);
     constexpr int NW = nfrac(F) + 1;  // windows (tile + fractions)
-    constexpr unsigned kLimit = 1u << 22;
+    const unsigned kLimit = pp.wait_limit ? pp.wait_limit : kHarmWaitLimit;
     extern __shared__ float4 smem4[];
     __shared__ __align__(8) uint64_t full[2], empty[2];
+    // abort: set by whoever's wait ran out, ends both loops at their next item;
+    // issued/landed per stage let the CTA wait for its copies before exiting
+    __shared__ volatile int abort_flag;
+    __shared__ unsigned issued[2], landed[2];
     float* smem = reinterpret_cast<float*>(smem4);
     const unsigned nitems = ntiles * (unsigned)rows;
     if (blockIdx.x >= nitems) return;
@@ -383,7 +398,10 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
         for (int s = 0; s < 2; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], NC / 32);
+            issued[s] = 0;
+            landed[s] = 0;
         }
+        abort_flag = 0;
         mbar_init_fence();
     }
     __syncthreads();
@@ -405,8 +423,14 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
         window_params<T>(lane, m, h, off);
         for (unsigned j = 0; row < (unsigned)rows; ++j, advance()) {
             const unsigned s = j & 1u;
+            if (__any_sync(0xffffffffu, abort_flag != 0)) break;  // warp-uniform
             if (j >= 2) {  // wait until the consumers released stage s
-                if (!mbar_wait_bounded(&empty[s], ((j >> 1) - 1) & 1u, kLimit)) ok = false;
+                const bool got = mbar_wait_bounded(&empty[s], ((j >> 1) - 1) & 1u, kLimit);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    if (lane == 0) abort_flag = 1;
+                    break;
+                }
             }
             float* sm = smem + s * STAGE;
             const float* src = p + (size_t)row * ppitch;
@@ -426,7 +450,9 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
             __syncwarp();
             if (lane == 0) mbar_arrive_expect_tx(&full[s], total);
             __syncwarp();
+            if (pp.flags & kHarmNoCopies) continue;  // nothing staged, nothing in flight
             if (len) bulk_g2s(sm + off, src + a4, 4u * len, &full[s]);
+            if (lane == 0) issued[s] += 1;
         }
     } else {
         // ---------------- consumers
@@ -442,11 +468,14 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
         for (;;) {
 #pragma unroll
             for (unsigned s = 0; s < 2; ++s) {  // s is a compile-time stage index
-                if (row >= (unsigned)rows) break;
-                if (!mbar_wait_bounded(&full[s], ph, kLimit)) {
+                if (row >= (unsigned)rows || __any_sync(0xffffffffu, abort_flag != 0)) break;
+                const bool got = mbar_wait_bounded(&full[s], ph, kLimit);
+                if (!__all_sync(0xffffffffu, got)) {  // the warp decides together
                     ok = false;
-                    mbar_wait_bounded(&full[s], ph, kLimit);  // let the copies land
+                    if (lane == 0) abort_flag = 1;
+                    break;
                 }
+                if (tid == 0) landed[s] += 1;
                 sum_item<F, T, NC, OOL>(smem + s * STAGE, base, fs, pp.lo + tile * (unsigned)T,
                                         tid, pp, trial0 + (int)row, rec, counter, cap);
                 __syncwarp();
@@ -455,11 +484,21 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
                                  : "memory");
                 advance();
             }
-            if (row >= (unsigned)rows) break;
+            if (row >= (unsigned)rows || __any_sync(0xffffffffu, abort_flag != 0)) break;
             ph ^= 1u;
         }
     }
-    if (!ok && lane == 0) atomicExch(counter + 1, kHarmStagingTimeout);
+    // After an abort, copies the producer issued may still be landing in this
+    // CTA's shared memory: wait for them (bounded) before the CTA exits.
+    __syncthreads();
+    if (abort_flag && threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s)
+            while (landed[s] < issued[s]) {
+                if (!mbar_wait_bounded(&full[s], landed[s] & 1u, kLimit)) break;
+                landed[s] += 1;
+            }
+    }
+    if ((!ok || abort_flag) && lane == 0) atomicExch(counter + 1, kHarmStagingTimeout);
 }
 
 }  // namespace psx

@@ -1221,6 +1221,8 @@ static void host_setup(psx_search* s, const psx_search_config* cfg)
     s->pk.hi = hi > lo ? hi : 0;
     s->pk.thresh = cfg->min_snr;
     s->pk.vote = cfg->min_snr - std::fabs(cfg->min_snr) * 0x1p-20f;
+    s->pk.wait_limit = kHarmWaitLimit;
+    s->pk.flags = 0;
 }
 
 int psx_search_create(const psx_search_config* cfg, psx_search** out)
@@ -1344,6 +1346,68 @@ int psx_search_destroy(psx_search* s)
     clear_error();
     if (!s) return PSX_OK;
     delete s;
+    return PSX_OK;
+}
+
+int psx_harmonic_peaks(const float* d_spec, size_t pitch, size_t nbins, int rows, int nharms,
+                       const int* h_start, const int* h_end, float thresh, int* d_records,
+                       size_t cap, size_t* h_count, unsigned wait_limit, unsigned flags,
+                       psx_stream_t stream)
+{
+    clear_error();
+    if (!d_spec || !h_start || !h_end || !h_count || rows < 1 || nharms < 0 || nharms > 5 ||
+        nbins == 0 || nbins > 0x7fffffffu || pitch < nbins || (cap && !d_records) ||
+        (pitch & 3u) || (reinterpret_cast<uintptr_t>(d_spec) & 15u)) {
+        set_error("harmonic_peaks: bad arguments (nharms 0..5, pitch >= nbins and a multiple of "
+                  "4, spectra 16-byte aligned)");
+        return PSX_ERR_INVALID;
+    }
+    *h_count = 0;
+    PeakParams pk{};
+    unsigned lo = 0xffffffffu, hi = 0;
+    for (int h = 0; h <= 5; ++h) {
+        int st = h <= nharms ? std::max(0, h_start[h]) : 0;
+        int en = h <= nharms ? std::min((int)nbins, h_end[h]) : 0;
+        if (en < st) en = st;
+        pk.start[h] = st;
+        pk.end[h] = en;
+        if (en > st) {
+            lo = std::min(lo, (unsigned)st);
+            hi = std::max(hi, (unsigned)en);
+        }
+    }
+    if (hi <= lo) return PSX_OK;  // empty search ranges
+    pk.lo = lo & ~127u;
+    pk.hi = hi;
+    pk.thresh = thresh;
+    pk.vote = thresh - std::fabs(thresh) * 0x1p-20f;
+    pk.wait_limit = wait_limit ? wait_limit : kHarmWaitLimit;
+    pk.flags = flags;
+    cudaStream_t cs_ = cs(stream);
+    PSX_TRY(configure_harm(nharms));
+    unsigned* d_counter = nullptr;
+    PSX_CUDA(cudaMallocAsync((void**)&d_counter, sizeof(unsigned) * 2, cs_));
+    int rc = cuda_status(cudaMemsetAsync(d_counter, 0, sizeof(unsigned) * 2, cs_), "memset");
+    if (rc == PSX_OK)
+        rc = launch_harm(nharms, kHarmDefaultShape, d_spec, pitch, (unsigned)nbins, pk, 0, rows,
+                         reinterpret_cast<int4*>(d_records), d_counter, (unsigned)cap, cs_);
+    unsigned hcnt[2] = {0, 0};
+    if (rc == PSX_OK)
+        rc = cuda_status(cudaMemcpyAsync(hcnt, d_counter, sizeof hcnt, cudaMemcpyDeviceToHost, cs_),
+                         "harmonic_peaks copy");
+    cudaFreeAsync(d_counter, cs_);
+    if (rc == PSX_OK) rc = cuda_status(cudaStreamSynchronize(cs_), "harmonic_peaks");
+    if (rc != PSX_OK) return rc;
+    if (hcnt[1] != 0) {
+        set_error("harmonic_peaks: a staging wait ran out after %u polls (status 0x%x)",
+                  pk.wait_limit, hcnt[1]);
+        return PSX_ERR_CUDA;
+    }
+    *h_count = hcnt[0];
+    if (hcnt[0] > cap) {
+        set_error("harmonic_peaks: %u hits, buffer holds %zu", hcnt[0], cap);
+        return PSX_ERR_OVERFLOW;
+    }
     return PSX_OK;
 }
 
