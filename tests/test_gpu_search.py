@@ -229,6 +229,29 @@ def test_two_lanes_identical(S, graph):
         assert np.array_equal(c, outs[0])
 
 
+@pytest.mark.parametrize("n", [1 << 25, 3 << 23])
+def test_large_transform_fused_matches_reference_form(S, n):
+    """At large N (and 3*2^k) the batched path (complex transform of length
+    N/2 + fused unpack) finds what the plain path (the reference's real
+    transform + interbin) finds, S/N within 1e-5."""
+    import torch
+    search, synth = S
+    ts = 64e-6
+    g = torch.Generator(device="cuda").manual_seed(41)
+    x = torch.randn(n, device="cuda", generator=g)
+    t = torch.arange(n, device="cuda", dtype=torch.float64)
+    ph = torch.frac(t * ts / 7.3e-3)
+    x += (0.15 * torch.exp(-0.5 * ((ph - 0.5) / 0.02) ** 2)).float()
+    kw = dict(acc_lo=-0.3, acc_hi=0.3, nharmonics=5, min_snr=6.0)
+    outs = []
+    for mode in ("plain", "batched"):
+        s = search.AccelSearch(_params(S, n, ts, mode=mode, batch=4, **kw))
+        outs.append(s.search(x, 0.0, 0, per_dm=False)[0])
+        s.close()
+    nm, ua, ub, worst = match_candidates(outs[1], outs[0], 6.0)
+    assert nm > 3 and not ua and not ub and worst < 1e-5, (ua[:3], ub[:3], worst)
+
+
 def test_autotune_picks_a_timed_pair(S):
     """The autotuner times every (batch, shape) pair it may use and returns
     the fastest; the tuned engine finds what the default engine finds."""
