@@ -579,6 +579,100 @@ int psx_server_wait(psx_server* srv, long long ticket, double timeout_s,
 int psx_server_status(psx_server* srv, size_t* used_bytes, int* active,
                       int* pending, int* pooled);
 
+/* ------------------------------------------------------------------ */
+/* Producer side: SIGPROC filterbank input and dedispersion            */
+/* ------------------------------------------------------------------ */
+
+/* The keywords of a SIGPROC header (SigprocHeader,
+   include/data_types/header.hpp:171-212); unset values are zero. */
+typedef struct {
+    char source_name[80];
+    char rawdatafile[80];
+    double az_start, za_start, src_raj, src_dej, tstart, tsamp, period;
+    double fch1, foff, refdm;
+    int nchans, telescope_id, machine_id, data_type, ibeam, nbeams, nbits;
+    int barycentric, pulsarcentric, nbins, nsamples, nifs, npuls;
+    unsigned char signed_data;
+    size_t header_size; /* bytes before the first sample */
+} psx_sigproc_header;
+
+/* Reads the header of a SIGPROC file.  nsamples == 0 in the file is
+   replaced by (file size - header size) / nchans * 8 / nbits.  Unknown
+   keywords are skipped with a warning on stderr, as the reference does.
+   Replaces read_header (include/data_types/header.hpp:339-403) behind the
+   SigprocFilterbank constructor (include/data_types/filterbank.hpp:261-300).
+   PSX_ERR_IO: unreadable file or no HEADER_START. */
+int psx_sigproc_read_header(const char* path, psx_sigproc_header* h);
+
+/* Reads up to nsamples sample rows starting at start_sample into h_dst
+   (nsamples * nchans * nbits / 8 bytes); *h_nread = rows read (fewer at
+   the end of the file).  Replaces SigprocFilterbank::load_gulp
+   (include/data_types/filterbank.hpp:308-328). */
+int psx_sigproc_read(const char* path, const psx_sigproc_header* h, size_t start_sample,
+                     size_t nsamples, void* h_dst, size_t* h_nread);
+
+/* Writes a SIGPROC header (HEADER_START, the set keywords, HEADER_END)
+   to a new file and returns its size in *h_size.  The writer side of
+   header_write (include/data_types/header.hpp:222-300). */
+int psx_sigproc_write_header(const char* path, const psx_sigproc_header* h,
+                             size_t* h_size);
+
+/* Reads a DM list, one value per line; an empty line repeats the previous
+   value (0 for a leading empty line), as getFileContent does
+   (src/pipeline_multi.cu:313-337).  PSX_ERR_OVERFLOW: *n_out = need. */
+int psx_read_dm_file(const char* path, float* h_out, size_t cap, size_t* n_out);
+
+/* Direct incoherent dedispersion plan (dedisp_plan behind Dedisperser,
+   include/transforms/dedisperser.hpp:13-188).  The plan owns its device
+   scratch (channel-major samples, shift tables), grown on first use. */
+typedef struct psx_dedisp_plan psx_dedisp_plan;
+
+/* dedisp_create_plan_multi(nchans, tsamp, fch1, foff): per-channel delays
+   of 4.15e3/tsamp * (f_c^-2 - fch1^-2) samples per unit DM, f_c = fch1 +
+   c*foff (MHz).  foff must be negative (fch1 the highest frequency). */
+int psx_dedisp_create(size_t nchans, float tsamp, float fch1, float foff,
+                      psx_dedisp_plan** out);
+int psx_dedisp_destroy(psx_dedisp_plan* plan);
+/* Dedisperser::set_dm_list (dedisperser.hpp:43-57). */
+int psx_dedisp_set_dm_list(psx_dedisp_plan* plan, const float* h_dms, size_t n);
+/* Dedisperser::generate_dm_list (dedisperser.hpp:63-71): DMs from dm_start
+   upward, each step the largest whose smearing, combined with the pulse
+   width (microseconds) and sampling time, stays within `tol` times the
+   width at the previous DM; the last DM is the first at or past dm_end. */
+int psx_dedisp_generate_dm_list(psx_dedisp_plan* plan, float dm_start, float dm_end,
+                                float width_us, float tol);
+size_t psx_dedisp_get_dm_count(const psx_dedisp_plan* plan);
+int psx_dedisp_get_dm_list(const psx_dedisp_plan* plan, float* h_out, size_t cap);
+int psx_dedisp_get_delay_table(const psx_dedisp_plan* plan, float* h_out);
+/* Dedisperser::set_killmask (dedisperser.hpp:73-110): h_mask[c] == 0 drops
+   channel c from every sum; NULL restores all channels. */
+int psx_dedisp_set_killmask(psx_dedisp_plan* plan, const int* h_mask);
+/* Samples the largest DM delays the last channel by (rounded half up);
+   each output series is nsamps - max_delay long. */
+size_t psx_dedisp_get_max_delay(const psx_dedisp_plan* plan);
+
+#define PSX_DEDISP_RAW 1 /* output the plain channel sums */
+
+/* Dedisperses nsamps SIGPROC sample rows (device memory, nchans*nbits/8
+   bytes each; nbits 1, 2, 4, 8 or 16) into d_out: row d (DM trial d of the
+   list), out_pitch floats apart, holds nsamps - max_delay samples.  The
+   channel sums are exact integers; unless PSX_DEDISP_RAW they are mapped
+   to (sum - nchans*m/2) / (m*sqrt(nchans)) + 1/2, m = 2^nbits - 1.
+   d_out must be 16-byte aligned and out_pitch a multiple of 4.
+   Asynchronous on `stream`.  Replaces dedisp_execute
+   (dedisperser.hpp:148-156) with the block left in device memory for the
+   search, where the reference copied it to the host. */
+int psx_dedisp_execute(psx_dedisp_plan* plan, size_t nsamps, const uint8_t* d_in,
+                       int nbits, float* d_out, size_t out_pitch, int flags,
+                       psx_stream_t stream);
+
+/* As psx_dedisp_execute with the sample rows in host memory: the rows
+   cross to the device in pieces that overlap the unpacking of the
+   previous piece.  Pinned h_in gives asynchronous copies. */
+int psx_dedisp_execute_host(psx_dedisp_plan* plan, size_t nsamps, const uint8_t* h_in,
+                            int nbits, float* d_out, size_t out_pitch, int flags,
+                            psx_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -699,3 +699,157 @@ def ref_worker_search(series2d, tsamp, dms, fft_size, p: SearchParams, zapfile: 
                                      C.byref(a), out.ctypes.data, na, cap, C.byref(n)),
          "worker_search")
     return out[:n.value].copy(), na[:n.value].copy()
+
+
+# ---------------------------------------------------------------- dedispersion
+def _dedisp_lib():
+    L = lib()
+    if not getattr(L, "_dedisp_ready", False):
+        L.orc_delay_table.argtypes = [C.c_size_t, C.c_float, C.c_float, C.c_float, _fp]
+        L.orc_dm_list.restype = C.c_size_t
+        L.orc_dm_list.argtypes = [C.c_size_t] + [C.c_float] * 7 + [_fp, C.c_size_t]
+        L.orc_max_delay.restype = C.c_size_t
+        L.orc_max_delay.argtypes = [_fp, C.c_size_t, _fp, C.c_size_t]
+        L.orc_dedisperse.restype = C.c_int
+        L.orc_dedisperse.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t, C.c_int, _fp, _fp,
+                                     C.c_size_t, C.c_void_p, C.c_int, _fp, C.c_size_t]
+        L.orc_sigproc_value.restype = C.c_uint
+        L.orc_sigproc_value.argtypes = [C.c_void_p, C.c_size_t, C.c_int]
+        L._dedisp_ready = True
+    return L
+
+
+def delay_table(nchans, tsamp, fch1, foff) -> np.ndarray:
+    out = np.zeros(nchans, np.float32)
+    _dedisp_lib().orc_delay_table(nchans, tsamp, fch1, foff, out)
+    return out
+
+
+def dm_list(nchans, tsamp, fch1, foff, dm_start, dm_end, width_us, tol) -> np.ndarray:
+    L = _dedisp_lib()
+    args = (nchans, tsamp, fch1, foff, dm_start, dm_end, width_us, tol)
+    n = L.orc_dm_list(*args, np.zeros(1, np.float32), 0)
+    out = np.zeros(n, np.float32)
+    L.orc_dm_list(*args, out, n)
+    return out
+
+
+def max_delay(delays, dms) -> int:
+    d = np.ascontiguousarray(delays, np.float32)
+    m = np.ascontiguousarray(dms, np.float32)
+    return int(_dedisp_lib().orc_max_delay(d, d.size, m, m.size))
+
+
+def dedisperse(rows, nbits: int, nchans: int, delays, dms, killmask=None, raw=False):
+    """rows: (nsamps, nchans*nbits/8) packed uint8 SIGPROC rows.  Returns
+    (ndm, nsamps - max_delay) float32."""
+    rows = np.ascontiguousarray(rows, np.uint8)
+    d = np.ascontiguousarray(delays, np.float32)
+    m = np.ascontiguousarray(dms, np.float32)
+    ns = rows.shape[0]
+    md = max_delay(d, m)
+    out = np.zeros((m.size, ns - md), np.float32)
+    km = None if killmask is None else np.ascontiguousarray(killmask, np.int32)
+    rc = _dedisp_lib().orc_dedisperse(rows.ctypes.data, ns, nchans, nbits, d, m, m.size,
+                                      None if km is None else km.ctypes.data, int(raw), out,
+                                      out.shape[1])
+    if rc:
+        raise ValueError("orc_dedisperse: the samples do not exceed the maximum delay")
+    return out
+
+
+def unpack_rows(rows, nchans: int, nbits: int) -> np.ndarray:
+    """Packed SIGPROC rows -> (nsamps, nchans) unsigned samples (numpy
+    restatement of orc_sigproc_value for whole arrays)."""
+    rows = np.ascontiguousarray(rows, np.uint8)
+    if nbits == 8:
+        return rows[:, :nchans].astype(np.uint32)
+    if nbits == 16:
+        return rows.view("<u2")[:, :nchans].astype(np.uint32)
+    per = 8 // nbits
+    mask = (1 << nbits) - 1
+    out = np.zeros((rows.shape[0], nchans), np.uint32)
+    for k in range(per):
+        out[:, k::per] = (rows[:, :nchans // per] >> (k * nbits)) & mask
+    return out
+
+
+def parse_sigproc_header(path: str) -> dict:
+    """Independent SIGPROC header parse (keyword, typed value) in Python,
+    restating read_header (include/data_types/header.hpp:339-403)."""
+    import struct
+    ints = {"nchans", "telescope_id", "machine_id", "data_type", "ibeam", "nbeams", "nbits",
+            "barycentric", "pulsarcentric", "nbins", "nsamples", "nifs", "npuls"}
+    dbls = {"az_start", "za_start", "src_raj", "src_dej", "tstart", "tsamp", "period", "fch1",
+            "foff", "refdm"}
+    data = open(path, "rb").read()
+    pos = 0
+
+    def rs():
+        nonlocal pos
+        n = struct.unpack_from("<i", data, pos)[0]
+        pos += 4
+        s = data[pos:pos + n].decode()
+        pos += n
+        return s
+
+    assert rs() == "HEADER_START"
+    out = {}
+    while True:
+        k = rs()
+        if k == "HEADER_END":
+            break
+        if k in ("source_name", "rawdatafile"):
+            out[k] = rs()
+        elif k in ints:
+            out[k] = struct.unpack_from("<i", data, pos)[0]
+            pos += 4
+        elif k in dbls:
+            out[k] = struct.unpack_from("<d", data, pos)[0]
+            pos += 8
+        elif k == "signed":
+            out["signed_data"] = data[pos]
+            pos += 1
+    out["header_size"] = pos
+    if not out.get("nsamples"):
+        out["nsamples"] = (len(data) - pos) // out["nchans"] * 8 // out["nbits"]
+    return out
+
+
+_REF_HDR_KEYS = ["az_start", "za_start", "src_raj", "src_dej", "tstart", "tsamp", "period",
+                 "fch1", "foff", "refdm", "nchans", "telescope_id", "machine_id", "data_type",
+                 "ibeam", "nbeams", "nbits", "barycentric", "pulsarcentric", "nbins",
+                 "nsamples", "nifs", "npuls", "signed_data", "header_size"]
+
+
+def ref_sigproc_header(path: str) -> dict:
+    """The reference's own read_header on `path` (oracle/_ref)."""
+    L = ref_host()
+    fn = L.ref_sigproc_header
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_char_p, _dp, C.c_char_p, C.c_char_p]
+    v = np.zeros(25, np.float64)
+    sn = C.create_string_buffer(80)
+    rd = C.create_string_buffer(80)
+    if fn(path.encode(), v, sn, rd):
+        raise OSError(path)
+    out = dict(zip(_REF_HDR_KEYS, v.tolist()))
+    out["source_name"] = sn.value.decode()
+    out["rawdatafile"] = rd.value.decode()
+    return out
+
+
+def ref_filterbank_gulp(path: str, seg_start: int, seg_n: int, start: int, n: int,
+                        row_bytes: int):
+    """SigprocFilterbank(path, seg_start, seg_n).load_gulp(start, n): the
+    bytes read and [tsamp, fch1, foff, cfreq, start, end, effective, total,
+    pepoch at size 2^16]."""
+    L = ref_host()
+    fn = L.ref_filterbank_gulp
+    fn.restype = C.c_size_t
+    fn.argtypes = [C.c_char_p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_size_t, C.c_void_p,
+                   C.c_size_t, _dp]
+    out = np.zeros(max(1, n * row_bytes), np.uint8)
+    meta = np.zeros(9, np.float64)
+    got = fn(path.encode(), seg_start, seg_n, start, n, out.ctypes.data, out.size, meta)
+    return out[:got * row_bytes], meta

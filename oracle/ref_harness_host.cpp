@@ -195,3 +195,52 @@ size_t ref_overview_text(const float* dms, size_t ndm, const float* accs, size_t
 }
 
 }  // extern "C"
+
+/* The reference's SIGPROC reader: read_header (include/data_types/header.hpp:
+   339-403) into SigprocHeader, flattened into doubles in a fixed order:
+   az_start za_start src_raj src_dej tstart tsamp period fch1 foff refdm
+   nchans telescope_id machine_id data_type ibeam nbeams nbits barycentric
+   pulsarcentric nbins nsamples nifs npuls signed size (25 values). */
+extern "C" int ref_sigproc_header(const char* path, double* out, char* source_name,
+                                  char* rawdatafile)
+{
+    std::ifstream f(path, std::ifstream::in | std::ifstream::binary);
+    if (!f) return 1;
+    SigprocHeader h;
+    read_header(f, h);
+    double v[25] = {h.az_start, h.za_start, h.src_raj, h.src_dej, h.tstart, h.tsamp, h.period,
+                    h.fch1, h.foff, h.refdm, (double)h.nchans, (double)h.telescope_id,
+                    (double)h.machine_id, (double)h.data_type, (double)h.ibeam,
+                    (double)h.nbeams, (double)h.nbits, (double)h.barycentric,
+                    (double)h.pulsarcentric, (double)h.nbins, (double)h.nsamples,
+                    (double)h.nifs, (double)h.npuls, (double)h.signed_data, (double)h.size};
+    std::memcpy(out, v, sizeof(v));
+    std::snprintf(source_name, 80, "%s", h.source_name.c_str());
+    std::snprintf(rawdatafile, 80, "%s", h.rawdatafile.c_str());
+    return 0;
+}
+
+/* SigprocFilterbank(path, seg_start, seg_n) and one load_gulp(start, n)
+   (include/data_types/filterbank.hpp:261-328): the metadata the program
+   uses (tsamp, fch1, foff, cfreq as float; start, end, effective) and the
+   bytes read. */
+extern "C" size_t ref_filterbank_gulp(const char* path, size_t seg_start, size_t seg_n,
+                                      size_t start, size_t n, unsigned char* out, size_t cap,
+                                      double* meta)
+{
+    SigprocFilterbank fil(path, seg_start, seg_n);
+    size_t got = fil.load_gulp(start, n);
+    size_t bytes = got * (size_t)fil.get_nchans() * (size_t)fil.get_nbits() / 8;
+    std::memcpy(out, fil.get_data(), std::min(bytes, cap));
+    meta[0] = fil.get_tsamp();
+    meta[1] = fil.get_fch1();
+    meta[2] = fil.get_foff();
+    meta[3] = fil.get_cfreq();
+    meta[4] = (double)fil.get_start_sample();
+    meta[5] = (double)fil.get_end_sample();
+    meta[6] = (double)fil.get_effective_nsamps();
+    meta[7] = (double)fil.get_total_nsamps();
+    fil.size = 1u << 16;
+    meta[8] = fil.get_segment_pepoch();
+    return got;
+}

@@ -96,6 +96,22 @@ class RequestStats(C.Structure):
                 ("status", C.c_int), ("engine_reused", C.c_int)]
 
 
+class SigprocHeader(C.Structure):
+    """psx_sigproc_header == the keywords of SigprocHeader (header.hpp:171-212)."""
+    _fields_ = [("source_name", C.c_char * 80), ("rawdatafile", C.c_char * 80),
+                ("az_start", C.c_double), ("za_start", C.c_double), ("src_raj", C.c_double),
+                ("src_dej", C.c_double), ("tstart", C.c_double), ("tsamp", C.c_double),
+                ("period", C.c_double), ("fch1", C.c_double), ("foff", C.c_double),
+                ("refdm", C.c_double), ("nchans", C.c_int), ("telescope_id", C.c_int),
+                ("machine_id", C.c_int), ("data_type", C.c_int), ("ibeam", C.c_int),
+                ("nbeams", C.c_int), ("nbits", C.c_int), ("barycentric", C.c_int),
+                ("pulsarcentric", C.c_int), ("nbins", C.c_int), ("nsamples", C.c_int),
+                ("nifs", C.c_int), ("npuls", C.c_int), ("signed_data", C.c_ubyte),
+                ("header_size", C.c_size_t)]
+
+
+PSX_DEDISP_RAW = 1
+
 _vp = C.c_void_p
 _sz = C.c_size_t
 _f = C.c_float
@@ -173,6 +189,22 @@ SIGNATURES = {
                              C.POINTER(RequestStats)]),
     "psx_server_status": (_i, [_vp, C.POINTER(_sz), C.POINTER(_i), C.POINTER(_i),
                                C.POINTER(_i)]),
+    "psx_sigproc_read_header": (_i, [C.c_char_p, C.POINTER(SigprocHeader)]),
+    "psx_sigproc_read": (_i, [C.c_char_p, C.POINTER(SigprocHeader), _sz, _sz, _vp,
+                              C.POINTER(_sz)]),
+    "psx_sigproc_write_header": (_i, [C.c_char_p, C.POINTER(SigprocHeader), C.POINTER(_sz)]),
+    "psx_read_dm_file": (_i, [C.c_char_p, _vp, _sz, C.POINTER(_sz)]),
+    "psx_dedisp_create": (_i, [_sz, _f, _f, _f, C.POINTER(_vp)]),
+    "psx_dedisp_destroy": (_i, [_vp]),
+    "psx_dedisp_set_dm_list": (_i, [_vp, _vp, _sz]),
+    "psx_dedisp_generate_dm_list": (_i, [_vp, _f, _f, _f, _f]),
+    "psx_dedisp_get_dm_count": (_sz, [_vp]),
+    "psx_dedisp_get_dm_list": (_i, [_vp, _vp, _sz]),
+    "psx_dedisp_get_delay_table": (_i, [_vp, _vp]),
+    "psx_dedisp_set_killmask": (_i, [_vp, _vp]),
+    "psx_dedisp_get_max_delay": (_sz, [_vp]),
+    "psx_dedisp_execute": (_i, [_vp, _sz, _vp, _i, _vp, _sz, _i, _vp]),
+    "psx_dedisp_execute_host": (_i, [_vp, _sz, _vp, _i, _vp, _sz, _i, _vp]),
 }
 
 _lib = None

@@ -196,3 +196,45 @@ def survey_block_torch(plan: SurveyBlock, seed: int = 2, device: str = "cuda",
         out[c0:c0 + len(rows)] = torch.clamp(torch.round(x), 0, 255).to(torch.float32)
         del x
     return out
+
+
+# ------------------------------------------------------------ filterbanks
+K_DM_S = 4.15e3  # s MHz^2 cm^3 / pc, the dispersion constant of the delay table
+
+
+@dataclass
+class FilterbankSpec:
+    """A SIGPROC block: nchans channels from fch1 downwards in steps of
+    |foff|, nbits-bit samples around mid-range, and pulsars dispersed at
+    `dm` (the arrival at channel c is delayed by K/tsamp*(f_c^-2 -
+    fch1^-2)*dm samples)."""
+    nsamps: int
+    tsamp: float = 320e-6
+    nchans: int = NCHANS
+    nbits: int = 8
+    fch1: float = FCH1_MHZ
+    foff: float = FOFF_MHZ
+    dm: float = 0.0
+    sigma: float = 0.0          # per-channel noise in sample units (0: a quarter range)
+    pulsars: List[Pulsar] = field(default_factory=list)
+
+
+def filterbank_values(spec: FilterbankSpec, seed: int = 0) -> np.ndarray:
+    """(nsamps, nchans) unsigned samples, seeded (numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    top = (1 << spec.nbits) - 1
+    sigma = spec.sigma or max(0.5, (top + 1) / 6.0)
+    mean = top / 2.0
+    f = spec.fch1 + spec.foff * np.arange(spec.nchans)
+    delay = K_DM_S * (f ** -2 - spec.fch1 ** -2) * spec.dm  # seconds
+    out = np.empty((spec.nsamps, spec.nchans), np.uint32 if spec.nbits == 16 else np.uint8)
+    i = np.arange(spec.nsamps, dtype=np.float64)
+    for c in range(spec.nchans):
+        x = rng.standard_normal(spec.nsamps)
+        for p in spec.pulsars:
+            phi = (i * spec.tsamp - delay[c]) / p.period + p.phase0
+            d = phi - np.round(phi)
+            s = p.duty / (2.0 * np.sqrt(2.0 * np.log(2.0)))
+            x += p.amp * np.exp(-0.5 * (d / s) ** 2)
+        out[:, c] = np.clip(np.round(mean + sigma * x), 0, top)
+    return out

@@ -1,0 +1,193 @@
+"""Dedispersion on the GPU against the oracle, bit for bit: every input
+width (1, 2, 4, 8, 16 bits), raw and mapped output, sorted, generated and
+unsorted DM lists (the wide-spread window path), killed channels, more
+channels than a packed 16-bit accumulator holds (4096), DM counts that do
+not fill a CTA, a single output sample, host and device input; then the
+Dedisperser class on a file, and the whole program (run) on a synthetic
+tutorial-shaped filterbank: its pulsar is found at its DM, and its
+candidates equal a search of the oracle's dedispersed block."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from peasoup_b200 import _lib, sigproc, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _plan(psx, nchans, tsamp, fch1, foff):
+    h = C.c_void_p()
+    assert psx.psx_dedisp_create(nchans, tsamp, fch1, foff, C.byref(h)) == 0
+    return h
+
+
+def _run(psx, torch, h, rows, nbits, ndm, nout, raw, host=False):
+    pitch = (nout + 3) // 4 * 4 + 4
+    out = torch.full((ndm, pitch), -7.0, dtype=torch.float32, device="cuda")
+    flags = _lib.PSX_DEDISP_RAW if raw else 0
+    if host:
+        rc = psx.psx_dedisp_execute_host(h, rows.shape[0], rows.ctypes.data, nbits,
+                                         C.c_void_p(out.data_ptr()), pitch, flags, None)
+    else:
+        d_rows = torch.from_numpy(rows).cuda()
+        rc = psx.psx_dedisp_execute(h, rows.shape[0], C.c_void_p(d_rows.data_ptr()), nbits,
+                                    C.c_void_p(out.data_ptr()), pitch, flags, None)
+    assert rc == 0, psx.psx_last_error()
+    torch.cuda.synchronize()
+    o = out.cpu().numpy()
+    assert np.all(o[:, nout:] == -7.0)  # nothing past the series is written
+    return o[:, :nout]
+
+
+CASES = [
+    # nchans, nbits, tsamp, fch1, foff, dm list, nsamps past max delay
+    (64, 2, 320e-6, 1510.0, -1.09, "gen:0:120", 3000),
+    (64, 8, 64e-6, 1510.0, -1.09, "gen:0:300", 5000),
+    (96, 4, 64e-6, 1400.0, -1.5, "gen:10:200", 2049),
+    (64, 1, 64e-6, 1510.0, -1.09, "sorted:13", 1111),
+    (32, 16, 128e-6, 1200.0, -2.0, "sorted:9", 1500),
+    (64, 8, 64e-6, 1510.0, -1.09, "unsorted:2000:21", 700),
+    (4096, 8, 64e-6, 1500.0, -0.0732421875, "sorted:8", 777),
+    (300, 8, 64e-6, 1500.0, -0.5, "sorted:3", 1),
+    (64, 8, 64e-6, 1510.0, -1.09, "zero", 513),
+]
+
+
+def _dm_list(psx, h, spec, oracle, case):
+    nchans, nbits, tsamp, fch1, foff = case[:5]
+    rng = np.random.default_rng(len(spec))
+    if spec.startswith("gen:"):
+        _, lo, hi = spec.split(":")
+        assert psx.psx_dedisp_generate_dm_list(h, float(lo), float(hi), 64.0, 1.11) == 0
+        n = psx.psx_dedisp_get_dm_count(h)
+        dms = np.zeros(n, np.float32)
+        psx.psx_dedisp_get_dm_list(h, dms.ctypes.data, n)
+        assert np.array_equal(dms, oracle.dm_list(nchans, tsamp, fch1, foff, float(lo),
+                                                  float(hi), 64.0, 1.11))
+        return dms
+    if spec.startswith("sorted:"):
+        dms = np.sort(rng.uniform(0, 120, int(spec.split(":")[1]))).astype(np.float32)
+    elif spec.startswith("unsorted:"):
+        _, hi, n = spec.split(":")
+        dms = rng.uniform(0, float(hi), int(n)).astype(np.float32)
+    else:
+        dms = np.zeros(1, np.float32)
+    assert psx.psx_dedisp_set_dm_list(h, dms.ctypes.data, dms.size) == 0
+    return dms
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}ch-{c[1]}bit-{c[5]}" for c in CASES])
+def test_dedisperse_equals_oracle(psx, cuda, oracle, case):
+    torch = cuda
+    nchans, nbits, tsamp, fch1, foff, spec, extra = case
+    h = _plan(psx, nchans, tsamp, fch1, foff)
+    try:
+        dms = _dm_list(psx, h, spec, oracle, case)
+        delays = oracle.delay_table(nchans, tsamp, fch1, foff)
+        md = psx.psx_dedisp_get_max_delay(h)
+        assert md == oracle.max_delay(delays, dms)
+        ns = md + extra
+        rng = np.random.default_rng(nchans + nbits)
+        v = rng.integers(0, 1 << nbits, (ns, nchans), dtype=np.uint32)
+        rows = sigproc.pack_samples(v, nbits)
+        want_raw = oracle.dedisperse(rows, nbits, nchans, delays, dms, raw=True)
+        want = oracle.dedisperse(rows, nbits, nchans, delays, dms)
+        got_raw = _run(psx, torch, h, rows, nbits, dms.size, extra, True)
+        assert np.array_equal(got_raw, want_raw)
+        got = _run(psx, torch, h, rows, nbits, dms.size, extra, False, host=True)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        # killed channels
+        km = (rng.random(nchans) > 0.2).astype(np.int32)
+        assert psx.psx_dedisp_set_killmask(h, km.ctypes.data) == 0
+        got = _run(psx, torch, h, rows, nbits, dms.size, extra, True)
+        assert np.array_equal(got, oracle.dedisperse(rows, nbits, nchans, delays, dms,
+                                                     killmask=km, raw=True))
+        zero = np.zeros(nchans, np.int32)
+        assert psx.psx_dedisp_set_killmask(h, zero.ctypes.data) == 0
+        assert np.all(_run(psx, torch, h, rows, nbits, dms.size, extra, True) == 0)
+        assert psx.psx_dedisp_set_killmask(h, None) == 0
+        assert np.array_equal(_run(psx, torch, h, rows, nbits, dms.size, extra, True), want_raw)
+    finally:
+        psx.psx_dedisp_destroy(h)
+
+
+def test_dedisperser_class_on_a_file(psx, cuda, oracle, tmp_path):
+    from peasoup_b200.dedisperse import Dedisperser
+    spec = synth.FilterbankSpec(nsamps=20000, tsamp=64e-6, nbits=4, dm=50.0,
+                                pulsars=[synth.Pulsar(0.0371, 0.0, 0.03, 2.0)])
+    v = synth.filterbank_values(spec, seed=3)
+    path = str(tmp_path / "f.fil")
+    sigproc.write_filterbank(path, sigproc.pack_samples(v, 4), nchans=64, nbits=4,
+                             tsamp=64e-6, fch1=synth.FCH1_MHZ, foff=synth.FOFF_MHZ, tstart=60000.0,
+                             nifs=1, data_type=1)
+    fb = sigproc.SigprocFilterbank(path, 1000, 15000)
+    dd = Dedisperser(fb)
+    dd.generate_dm_list(0.0, 100.0, 64.0, 1.11)
+    dms = dd.get_dm_list()
+    tr = dd.dedisperse(gulp=4096)
+    rows = sigproc.pack_samples(v[1000:16000], 4)
+    want = oracle.dedisperse(rows, 4, 64, dd.get_delay_table(), dms)
+    assert tr.get_nsamps() == 15000 - dd.get_max_delay()
+    assert np.array_equal(tr.to_host().view(np.uint32), want.view(np.uint32))
+    # the trial nearest DM 50 carries the most pulse power
+    power = [np.abs(np.fft.rfft(r - r.mean()))[1:].max() for r in want]
+    assert abs(dms[int(np.argmax(power))] - 50.0) < 12.0
+    dd.close()
+
+
+def _family(f, f0):
+    """f is a harmonic (up to 16) or sub-harmonic of f0, within 1e-3."""
+    r = f / f0 if f >= f0 else f0 / f
+    return round(r) <= 16 and abs(r - round(r)) < 1e-3 * r
+
+
+def test_whole_program_on_synthetic_tutorial(psx, cuda, oracle, tmp_path):
+    """Tutorial shape (2-bit, 64 channels, 320 us) with the tutorial's
+    250 ms pulsar and a 4.7 ms pulsar, both at DM 30.  run()'s outputs equal
+    search_to_outputs on the oracle's dedispersion of the same file; the
+    250 ms pulsar is found; the 4.7 ms pulsar, whose harmonics a few DM steps
+    of smearing wash out, peaks within 7 of DM 30.  (A 250 ms pulse barely
+    changes with DM in a 16-harmonic search, so its own best DM is not a
+    known answer.)"""
+    from peasoup_b200 import output, pipeline
+    from peasoup_b200.search import SearchParams
+    spec = synth.FilterbankSpec(nsamps=140000, tsamp=320e-6, nbits=2, dm=30.0,
+                                pulsars=[synth.Pulsar(0.25, 0.0, 0.01, 0.9),
+                                         synth.Pulsar(0.0047, 0.0, 0.1, 0.35)])
+    v = synth.filterbank_values(spec, seed=11)
+    path = str(tmp_path / "tut.fil")
+    sigproc.write_filterbank(path, sigproc.pack_samples(v, 2), source_name="P: 250 ms, DM: 30",
+                             nchans=64, nbits=2, tsamp=320e-6, fch1=1510.0, foff=-1.09,
+                             tstart=50000.0, nifs=1, data_type=1)
+    opts = pipeline.Options(path, outdir=str(tmp_path / "out"), dm_start=0.0, dm_end=60.0,
+                            min_snr=8.0)
+    nodes, sizes, scores, offsets, timers = pipeline.run(opts)
+    xml = open(os.path.join(opts.outdir, "overview.xml")).read()
+    for sec in ("header_parameters", "search_parameters", "segment_parameters", "dedispersion_trials",
+                "candidates"):
+        assert f"<{sec}" in xml
+    assert os.path.getsize(os.path.join(opts.outdir, "candidates.peasoup")) > 0
+    # the same search on the oracle's dedispersion of the file
+    fb = sigproc.SigprocFilterbank(path)
+    dms = oracle.dm_list(64, np.float32(320e-6), 1510.0, -1.09, 0.0, 60.0, 64.0, 1.11)
+    delays = oracle.delay_table(64, np.float32(320e-6), 1510.0, -1.09)
+    block = oracle.dedisperse(sigproc.pack_samples(v, 2), 2, 64, delays, dms)
+    size = sigproc.prev_power_of_two(fb.get_effective_nsamps())
+    cf = fb.get_cfreq()
+    params = SearchParams(fft_size=size, tsamp=float(np.float32(320e-6)),
+                          cfreq_hz=float(np.float32(float(np.float32(cf)) * 1e6)),
+                          ch_bw_hz=float(np.float32(float(np.float32(-1.09)) * 1e6)),
+                          min_snr=8.0, acc_pulse_width=float(np.float32(64.0 * 1e-6)))
+    n2, s2, _, _, _ = pipeline.search_to_outputs(
+        block, dms, params, str(tmp_path / "out2"), foff_mhz=float(np.float32(-1.09)),
+        nchans=64, cfreq_mhz=cf, dm_chunk=len(dms))
+    assert np.array_equal(nodes, n2) and np.array_equal(sizes, s2)
+    # known answers
+    top = nodes[output.roots(sizes)]
+    assert any(_family(float(c["freq"]), 4.0) for c in top)
+    fast = [c for c in top if _family(float(c["freq"]), 1.0 / 0.0047)]
+    assert fast
+    best = max(fast, key=lambda c: c["snr"])
+    assert abs(best["dm"] - 30.0) <= 7.0, (best["dm"], best["snr"], best["freq"])
