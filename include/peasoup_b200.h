@@ -651,6 +651,11 @@ int psx_dedisp_set_killmask(psx_dedisp_plan* plan, const int* h_mask);
    each output series is nsamps - max_delay long. */
 size_t psx_dedisp_get_max_delay(const psx_dedisp_plan* plan);
 
+/* Upper bound on the plan's channel-major scratch (default 4 GiB): longer
+   inputs are dedispersed in time gulps that overlap by the maximum delay,
+   as Dedisperser::dedisperse gulps (dedisperser.hpp:112-186). */
+int psx_dedisp_set_scratch_limit(psx_dedisp_plan* plan, size_t bytes);
+
 #define PSX_DEDISP_RAW 1 /* output the plain channel sums */
 
 /* Dedisperses nsamps SIGPROC sample rows (device memory, nchans*nbits/8

@@ -203,6 +203,7 @@ SIGNATURES = {
     "psx_dedisp_get_delay_table": (_i, [_vp, _vp]),
     "psx_dedisp_set_killmask": (_i, [_vp, _vp]),
     "psx_dedisp_get_max_delay": (_sz, [_vp]),
+    "psx_dedisp_set_scratch_limit": (_i, [_vp, _sz]),
     "psx_dedisp_execute": (_i, [_vp, _sz, _vp, _i, _vp, _sz, _i, _vp]),
     "psx_dedisp_execute_host": (_i, [_vp, _sz, _vp, _i, _vp, _sz, _i, _vp]),
 }

@@ -39,7 +39,9 @@ namespace {
 
 constexpr int kDdThreads = 256;
 constexpr int kDdWarps = 8;    // DM trials per CTA
-constexpr int kDdTile = 512;   // output samples per CTA
+constexpr int kDdTile8 = 1024; // output samples per CTA, 1..8-bit samples
+constexpr int kDdTile16 = 512; // output samples per CTA, 16-bit samples
+inline int dd_tile(int elem) { return elem == 1 ? kDdTile8 : kDdTile16; }
 constexpr int kUpRows = 64;    // unpack tile: samples
 constexpr int kUpChans = 64;   // unpack tile: channels
 constexpr float kDmConst = 4.15e3f;
@@ -69,7 +71,7 @@ __device__ __forceinline__ unsigned sigproc_value(const uint8_t* row, int c)
 template <int NBITS>
 __global__ void __launch_bounds__(256) k_unpack_chanmajor(
     const uint8_t* __restrict__ rows, size_t row_bytes, size_t nrows, size_t r0, size_t ncols,
-    int nchans, typename Sample<NBITS>::T* __restrict__ cm, size_t pitch)
+    int nchans, typename Sample<NBITS>::T* __restrict__ cm, size_t pitch, int vec)
 {
     using T = typename Sample<NBITS>::T;
     constexpr int kPad = 16 / (int)sizeof(T) / 4;  // row stride 68 B (u8) or 132 B (u16)
@@ -77,12 +79,34 @@ __global__ void __launch_bounds__(256) k_unpack_chanmajor(
     __shared__ __align__(16) T tile[kUpChans * kStride];
     const size_t col0 = (size_t)blockIdx.x * kUpRows;
     const int c0 = blockIdx.y * kUpChans;
-    for (int i = threadIdx.x; i < kUpRows * kUpChans; i += blockDim.x) {
-        int r = i / kUpChans, c = i % kUpChans;
-        size_t rr = col0 + r;
-        unsigned v = 0;
-        if (rr < nrows && c0 + c < nchans) v = sigproc_value<NBITS>(rows + rr * row_bytes, c0 + c);
-        tile[c * kStride + r] = (T)v;
+    if (vec) {
+        // 32-bit loads: a row's 64 channels are 2*NBITS words (rows 4-byte aligned)
+        constexpr int kWords = 2 * NBITS;
+        constexpr int kPerWord = 32 / NBITS;
+        const size_t seg = (size_t)c0 * NBITS / 8;
+        for (int i = threadIdx.x; i < kUpRows * kWords; i += blockDim.x) {
+            int r = i / kWords, q = i % kWords;
+            size_t rr = col0 + r;
+            size_t byte = seg + 4 * (size_t)q;
+            uint32_t w = 0;
+            if (rr < nrows && byte < row_bytes)
+                w = *reinterpret_cast<const uint32_t*>(rows + rr * row_bytes + byte);
+#pragma unroll
+            for (int k = 0; k < kPerWord; ++k) {
+                unsigned v;
+                if constexpr (NBITS == 16) v = (w >> (16 * k)) & 0xffffu;
+                else v = (w >> (k * NBITS)) & ((1u << NBITS) - 1u);
+                tile[(q * kPerWord + k) * kStride + r] = (T)v;
+            }
+        }
+    } else {
+        for (int i = threadIdx.x; i < kUpRows * kUpChans; i += blockDim.x) {
+            int r = i / kUpChans, c = i % kUpChans;
+            size_t rr = col0 + r;
+            unsigned v = 0;
+            if (rr < nrows && c0 + c < nchans) v = sigproc_value<NBITS>(rows + rr * row_bytes, c0 + c);
+            tile[c * kStride + r] = (T)v;
+        }
     }
     __syncthreads();
     constexpr int kVec = 16 / (int)sizeof(T);           // samples per 16-byte store
@@ -118,6 +142,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+__device__ __forceinline__ uint32_t lds32(uint32_t addr)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];\n" : "=r"(v) : "r"(addr));
+    return v;
+}
+template <int OFF>
+__device__ __forceinline__ uint32_t lds32o(uint32_t addr)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1+%2];\n" : "=r"(v) : "r"(addr), "n"(OFF));
+    return v;
+}
+
 __device__ __forceinline__ float map_sum(unsigned s, float mid, float scale, int raw)
 {
     float v = (float)s;
@@ -125,13 +163,14 @@ __device__ __forceinline__ float map_sum(unsigned s, float mid, float scale, int
     return v;
 }
 
-template <typename T>
+template <typename T, bool FLUSH>
 __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int blk = blockIdx.x % a.nblk;
-    const size_t t0 = (size_t)(blockIdx.x / a.nblk) * kDdTile;
+    constexpr int kTile = sizeof(T) == 1 ? kDdTile8 : kDdTile16;
+    const size_t t0 = (size_t)(blockIdx.x / a.nblk) * kTile;
     const int d = blk * kDdWarps + warp;
     const int nwin = kDdWarps / a.group;
     const int gw = warp / a.group;
@@ -162,11 +201,20 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
     float* out = a.out + (size_t)(active ? d : 0) * a.out_pitch;
 
     if constexpr (sizeof(T) == 1) {
-        // lane: outputs t0 + 4*lane + 128*k + {0..3}, k = 0..3, as packed
-        // 16-bit pairs (a pair holds at most 257 * 255 before a flush)
-        uint32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        uint32_t full[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        // lane: outputs t0 + 4*lane + 128*k + {0..3}, k = 0..7, as packed
+        // 16-bit pairs; with more than 257 channels a pair is flushed into
+        // 32-bit sums before it can overflow (257 * 255 = 65535)
+        constexpr int kUnits = kDdTile8 / 128;
+        uint32_t acc[2 * kUnits];
+        uint32_t full[FLUSH ? 4 * kUnits : 1];
+#pragma unroll
+        for (int k = 0; k < 2 * kUnits; ++k) acc[k] = 0;
+#pragma unroll
+        for (int k = 0; k < (FLUSH ? 4 * kUnits : 1); ++k) full[k] = 0;
         int since = 0;
+        const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(smem);
+        const uint32_t s_offs = s_base + 2u * stage_bytes + (uint32_t)warp * a.cc * 4u;
+        const uint32_t wstep = (uint32_t)(nwin * win_bytes);
         load_chunk(0, 0);
         for (int q = 0; q < nq; ++q) {
             if (q + 1 < nq) { load_chunk(q + 1, (q + 1) & 1); cp_async_wait<1>(); }
@@ -175,45 +223,61 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
             const int st = q & 1;
             const int nj = min(a.cc, a.nlive - q * a.cc);
             if (active) {
-                const uint8_t* wbase = smem + st * stage_bytes + gw * win_bytes;
-                const int* offs = s_off + (st * kDdWarps + warp) * a.cc;
-                for (int j = 0; j < nj; ++j) {
-                    const uint32_t* w = reinterpret_cast<const uint32_t*>(wbase + j * nwin * win_bytes);
-                    const int o = offs[j] + 4 * lane;
-                    const int sh = (o & 3) * 8;
-                    const int wi = o >> 2;
+                if constexpr (FLUSH) {
+                    if (since + nj > 257) {
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        uint32_t v = __funnelshift_r(w[wi + 32 * k], w[wi + 32 * k + 1], sh);
-                        acc[2 * k] += __byte_perm(v, 0, 0x4140);
-                        acc[2 * k + 1] += __byte_perm(v, 0, 0x4342);
-                    }
-                    if (++since == 257) {
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
+                        for (int k = 0; k < 2 * kUnits; ++k) {
                             full[2 * k] += acc[k] & 0xffffu;
                             full[2 * k + 1] += acc[k] >> 16;
                             acc[k] = 0;
                         }
                         since = 0;
                     }
+                    since += nj;
+                }
+                uint32_t wa = s_base + (uint32_t)(st * stage_bytes + gw * win_bytes) + 4u * lane;
+                const uint32_t oa = s_offs + (uint32_t)st * kDdWarps * a.cc * 4u;
+#pragma unroll 2
+                for (int j = 0; j < nj; ++j, wa += wstep) {
+                    const int o = (int)lds32(oa + 4u * j);
+                    const uint32_t ad = wa + (uint32_t)(o & ~3);
+                    const uint32_t sh = (uint32_t)(o & 3) << 3;
+#define PSX_DD_STEP(k)                                                            \
+                    {                                                             \
+                        uint32_t v = __funnelshift_r(lds32o<128 * (k)>(ad),       \
+                                                     lds32o<128 * (k) + 4>(ad), sh); \
+                        acc[2 * (k)] += __byte_perm(v, 0, 0x4140);                \
+                        acc[2 * (k) + 1] += __byte_perm(v, 0, 0x4342);            \
+                    }
+                    PSX_DD_STEP(0)
+                    PSX_DD_STEP(1)
+                    PSX_DD_STEP(2)
+                    PSX_DD_STEP(3)
+                    PSX_DD_STEP(4)
+                    PSX_DD_STEP(5)
+                    PSX_DD_STEP(6)
+                    PSX_DD_STEP(7)
+#undef PSX_DD_STEP
                 }
             }
             __syncthreads();
         }
         if (!active) return;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            full[2 * k] += acc[k] & 0xffffu;
-            full[2 * k + 1] += acc[k] >> 16;
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kUnits; ++k) {
+            uint32_t s0 = acc[2 * k] & 0xffffu, s1 = acc[2 * k] >> 16;
+            uint32_t s2 = acc[2 * k + 1] & 0xffffu, s3 = acc[2 * k + 1] >> 16;
+            if constexpr (FLUSH) {
+                s0 += full[4 * k];
+                s1 += full[4 * k + 1];
+                s2 += full[4 * k + 2];
+                s3 += full[4 * k + 3];
+            }
             size_t t = t0 + 4 * lane + 128 * k;
-            float4 v = make_float4(map_sum(full[4 * k], a.mid, a.scale, a.raw),
-                                   map_sum(full[4 * k + 1], a.mid, a.scale, a.raw),
-                                   map_sum(full[4 * k + 2], a.mid, a.scale, a.raw),
-                                   map_sum(full[4 * k + 3], a.mid, a.scale, a.raw));
+            float4 v = make_float4(map_sum(s0, a.mid, a.scale, a.raw),
+                                   map_sum(s1, a.mid, a.scale, a.raw),
+                                   map_sum(s2, a.mid, a.scale, a.raw),
+                                   map_sum(s3, a.mid, a.scale, a.raw));
             if (t + 3 < a.nout) {
                 *reinterpret_cast<float4*>(out + t) = v;
             } else {
@@ -279,6 +343,7 @@ struct psx_dedisp_plan {
     int elem = 0;
     int nlive = 0, ndm_pad = 0, nblk = 0, group = 8, lwin = 0, cc = 0;
     size_t ngroups = 0, max_lo = 0;
+    size_t scratch_limit = 4ull << 30;  // bytes of channel-major samples
     std::vector<int> h_tab;
     int* d_tab = nullptr;
     size_t tab_cap = 0;
@@ -342,7 +407,7 @@ struct psx_dedisp_plan {
                     spread = std::max(spread, mx - l);
                     mlo = std::max(mlo, (size_t)l);
                 }
-            *lwin_out = (int)round_up((size_t)spread + kDdTile + 8, (size_t)align);
+            *lwin_out = (int)round_up((size_t)spread + dd_tile(el) + 8, (size_t)align);
             *max_lo_out = mlo;
             if (lo_out) lo_out->swap(lo);
         };
@@ -453,8 +518,12 @@ int check_input(psx_dedisp_plan* p, size_t nsamps, int nbits, float* d_out, size
     return PSX_OK;
 }
 
-// Tables uploaded, cm sized; returns the pitch of cm in samples.
-int prepare(psx_dedisp_plan* p, size_t nsamps, size_t nout, int el, cudaStream_t st, size_t* pitch)
+// Tables uploaded and cm sized.  The outputs are made in gulps of *gulp
+// samples (a multiple of the CTA tile) so that cm, *pitch samples per
+// channel, stays within the plan's scratch limit; one gulp covers the
+// whole series when it fits.
+int prepare(psx_dedisp_plan* p, size_t nout, int el, cudaStream_t st, size_t* gulp,
+            size_t* pitch)
 {
     bool rebuilt = p->dirty || el != p->elem;
     PSX_TRY(p->build_tables(el));
@@ -465,9 +534,21 @@ int prepare(psx_dedisp_plan* p, size_t nsamps, size_t nout, int el, cudaStream_t
         PSX_CUDA(cudaMemcpyAsync(p->d_tab, p->h_tab.data(), bytes, cudaMemcpyHostToDevice, st));
         p->dirty = false;
     }
-    size_t ntiles = (nout + kDdTile - 1) / kDdTile;
-    size_t need = (ntiles - 1) * kDdTile + p->max_lo + (size_t)p->lwin;
-    *pitch = round_up(std::max(need, round_up(nsamps, kUpRows)), kUpRows);
+    const size_t tile = dd_tile(el);
+    const size_t md = p->max_delay();
+    auto pitch_for = [&](size_t g) {
+        size_t nt = (g + tile - 1) / tile;
+        size_t need = (nt - 1) * tile + p->max_lo + (size_t)p->lwin;
+        return round_up(std::max(need, g + md), kUpRows);
+    };
+    size_t g = round_up(nout, tile);
+    const size_t limit = p->scratch_limit / (p->nchans * (size_t)el);
+    if (pitch_for(g) > limit) {
+        size_t fixed = pitch_for(tile) - tile;
+        g = limit > fixed + tile ? (limit - fixed) / tile * tile : tile;
+    }
+    *gulp = g;
+    *pitch = pitch_for(g);
     return grow(&p->d_cm, &p->cm_cap, *pitch * p->nchans * el, "channel-major samples");
 }
 
@@ -479,8 +560,12 @@ int launch_unpack(const uint8_t* rows, size_t nrows, size_t r0, size_t ncols, ps
     size_t row_bytes = p->nchans * NBITS / 8;
     dim3 grid((unsigned)((ncols + kUpRows - 1) / kUpRows),
               (unsigned)((p->nchans + kUpChans - 1) / kUpChans));
+    // word loads when every row starts 4-byte aligned; channels past the
+    // last whole word of a row then read as zero and are never stored
+    const int vec = (row_bytes % 4 == 0 && (reinterpret_cast<uintptr_t>(rows) & 3) == 0) ? 1 : 0;
     k_unpack_chanmajor<NBITS><<<grid, 256, 0, st>>>(rows, row_bytes, nrows, r0, ncols,
-                                                    (int)p->nchans, static_cast<T*>(p->d_cm), pitch);
+                                                    (int)p->nchans, static_cast<T*>(p->d_cm), pitch,
+                                                    vec);
     return launch_status("k_unpack_chanmajor");
 }
 
@@ -518,21 +603,27 @@ int dedisperse(psx_dedisp_plan* p, int nbits, size_t pitch, size_t nout, float* 
     a.mid = (float)(0.5 * (double)p->nchans * (double)m);
     a.scale = (float)(1.0 / ((double)m * std::sqrt((double)p->nchans)));
     a.raw = (flags & PSX_DEDISP_RAW) ? 1 : 0;
-    size_t ntiles = (nout + kDdTile - 1) / kDdTile;
+    const size_t tile = dd_tile(nbits == 16 ? 2 : 1);
+    size_t ntiles = (nout + tile - 1) / tile;
     size_t nblocks = ntiles * (size_t)p->nblk;
     if (nblocks > 0x7fffffffull) {
         set_error("psx_dedisp: %zu blocks exceed one launch", nblocks);
         return PSX_ERR_UNSUPPORTED;
     }
     size_t smem = p->smem_bytes();
+    const unsigned grid = (unsigned)nblocks;
     if (nbits == 16) {
-        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint16_t>,
+        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint16_t, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_dedisperse<uint16_t><<<(unsigned)nblocks, kDdThreads, smem, st>>>(a);
+        k_dedisperse<uint16_t, false><<<grid, kDdThreads, smem, st>>>(a);
+    } else if (p->nlive > 257) {
+        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint8_t, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_dedisperse<uint8_t, true><<<grid, kDdThreads, smem, st>>>(a);
     } else {
-        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint8_t>,
+        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint8_t, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_dedisperse<uint8_t><<<(unsigned)nblocks, kDdThreads, smem, st>>>(a);
+        k_dedisperse<uint8_t, false><<<grid, kDdThreads, smem, st>>>(a);
     }
     return launch_status("k_dedisperse");
 }
@@ -657,34 +748,48 @@ int psx_dedisp_set_killmask(psx_dedisp_plan* p, const int* h_mask)
 
 size_t psx_dedisp_get_max_delay(const psx_dedisp_plan* p) { return p ? p->max_delay() : 0; }
 
+int psx_dedisp_set_scratch_limit(psx_dedisp_plan* p, size_t bytes)
+{
+    if (!p || bytes == 0) return PSX_ERR_INVALID;
+    p->scratch_limit = bytes;
+    return PSX_OK;
+}
+
 int psx_dedisp_execute(psx_dedisp_plan* p, size_t nsamps, const uint8_t* d_in, int nbits,
                        float* d_out, size_t out_pitch, int flags, psx_stream_t stream)
 {
     clear_error();
-    size_t nout = 0, pitch = 0;
+    size_t nout = 0, pitch = 0, gulp = 0;
     PSX_TRY(check_input(p, nsamps, nbits, d_out, out_pitch, &nout));
     if (!d_in) return PSX_ERR_INVALID;
     cudaStream_t st = cs(stream);
     const int el = nbits == 16 ? 2 : 1;
-    PSX_TRY(prepare(p, nsamps, nout, el, st, &pitch));
-    PSX_TRY(unpack(nbits, d_in, nsamps, 0, pitch, p, pitch, st));
-    return dedisperse(p, nbits, pitch, nout, d_out, out_pitch, flags, st);
+    PSX_TRY(prepare(p, nout, el, st, &gulp, &pitch));
+    const size_t row_bytes = p->nchans * (size_t)nbits / 8;
+    const size_t md = p->max_delay();
+    for (size_t g0 = 0; g0 < nout; g0 += gulp) {
+        const size_t n = std::min(gulp, nout - g0);
+        PSX_TRY(unpack(nbits, d_in + g0 * row_bytes, n + md, 0, pitch, p, pitch, st));
+        PSX_TRY(dedisperse(p, nbits, pitch, n, d_out + g0, out_pitch, flags, st));
+    }
+    return PSX_OK;
 }
 
 int psx_dedisp_execute_host(psx_dedisp_plan* p, size_t nsamps, const uint8_t* h_in, int nbits,
                             float* d_out, size_t out_pitch, int flags, psx_stream_t stream)
 {
     clear_error();
-    size_t nout = 0, pitch = 0;
+    size_t nout = 0, pitch = 0, gulp = 0;
     PSX_TRY(check_input(p, nsamps, nbits, d_out, out_pitch, &nout));
     if (!h_in) return PSX_ERR_INVALID;
     cudaStream_t st = cs(stream);
     const int el = nbits == 16 ? 2 : 1;
-    PSX_TRY(prepare(p, nsamps, nout, el, st, &pitch));
+    PSX_TRY(prepare(p, nout, el, st, &gulp, &pitch));
     const size_t row_bytes = p->nchans * (size_t)nbits / 8;
+    const size_t md = p->max_delay();
     // pieces of about 32 MB, a multiple of the unpack tile
     size_t rows = std::max<size_t>(kUpRows, (32u << 20) / row_bytes / kUpRows * kUpRows);
-    rows = std::min(rows, round_up(nsamps, kUpRows));
+    rows = std::min(rows, round_up(std::min(gulp, nout) + md, kUpRows));
     PSX_TRY(grow(reinterpret_cast<void**>(&p->d_stage), &p->stage_cap, 2 * rows * row_bytes,
                  "input staging"));
     if (!p->copy_stream) {
@@ -699,20 +804,25 @@ int psx_dedisp_execute_host(psx_dedisp_plan* p, size_t nsamps, const uint8_t* h_
     PSX_CUDA(cudaEventRecord(p->ev_used[0], st));
     PSX_CUDA(cudaEventRecord(p->ev_used[1], st));
     size_t k = 0;
-    for (size_t r0 = 0; r0 < nsamps; r0 += rows, ++k) {
-        const int b = (int)(k & 1);
-        const size_t n = std::min(rows, nsamps - r0);
-        uint8_t* buf = p->d_stage + (size_t)b * rows * row_bytes;
-        PSX_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_used[b], 0));
-        PSX_CUDA(cudaMemcpyAsync(buf, h_in + r0 * row_bytes, n * row_bytes,
-                                 cudaMemcpyHostToDevice, p->copy_stream));
-        PSX_CUDA(cudaEventRecord(p->ev_copied[b], p->copy_stream));
-        PSX_CUDA(cudaStreamWaitEvent(st, p->ev_copied[b], 0));
-        const bool last = r0 + n >= nsamps;
-        PSX_TRY(unpack(nbits, buf, n, r0, last ? pitch - r0 : n, p, pitch, st));
-        PSX_CUDA(cudaEventRecord(p->ev_used[b], st));
+    for (size_t g0 = 0; g0 < nout; g0 += gulp) {
+        const size_t n_out = std::min(gulp, nout - g0);
+        const size_t n_in = n_out + md;
+        for (size_t r0 = 0; r0 < n_in; r0 += rows, ++k) {
+            const int b = (int)(k & 1);
+            const size_t n = std::min(rows, n_in - r0);
+            uint8_t* buf = p->d_stage + (size_t)b * rows * row_bytes;
+            PSX_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_used[b], 0));
+            PSX_CUDA(cudaMemcpyAsync(buf, h_in + (g0 + r0) * row_bytes, n * row_bytes,
+                                     cudaMemcpyHostToDevice, p->copy_stream));
+            PSX_CUDA(cudaEventRecord(p->ev_copied[b], p->copy_stream));
+            PSX_CUDA(cudaStreamWaitEvent(st, p->ev_copied[b], 0));
+            const bool last = r0 + n >= n_in;
+            PSX_TRY(unpack(nbits, buf, n, r0, last ? pitch - r0 : n, p, pitch, st));
+            PSX_CUDA(cudaEventRecord(p->ev_used[b], st));
+        }
+        PSX_TRY(dedisperse(p, nbits, pitch, n_out, d_out + g0, out_pitch, flags, st));
     }
-    return dedisperse(p, nbits, pitch, nout, d_out, out_pitch, flags, st);
+    return PSX_OK;
 }
 
 }  // extern "C"

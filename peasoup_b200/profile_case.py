@@ -1,6 +1,7 @@
 """A small, self-contained search case for profiler captures.
 
     python -m peasoup_b200.profile_case [--ndm 2] [--nsamps 8388608] [--graph]
+    python -m peasoup_b200.profile_case --dedisp [--ndm 32] [--nsamps 8388608]
 
 Searches `ndm` DM trials of the survey-shape synthetic block (2^23
 samples, tsamp 76 us, acceleration -100..100 m/s^2, 5 folds, 20 birdies)
@@ -10,6 +11,11 @@ trials hold about 1.5 GB on the device (series, trial buffers, cuFFT work
 area), so a capture of any of its kernels stays small while every buffer
 a kernel streams exceeds the 126 MB L2.  Graph capture is off unless
 `--graph` is given, so each kernel is an ordinary stream launch.
+
+With --dedisp: `ndm` DM trials (DM_i = 0.5 i) of nsamps x 64-channel 8-bit
+rows (tsamp as given, fch1 1510 MHz, foff -1.09 MHz), dedispersed four
+times from device memory; at 2^23 samples and 32 DM trials the case holds
+about 2.2 GB.
 """
 from __future__ import annotations
 
@@ -25,7 +31,10 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--harm-shape", type=int, default=0)
+    ap.add_argument("--dedisp", action="store_true")
     a = ap.parse_args(argv)
+    if a.dedisp:
+        return dedisp_case(a)
 
     import torch
     from . import search, synth
@@ -44,6 +53,38 @@ def main(argv=None) -> int:
     if not a.graph:
         print(s.profile(), flush=True)
     s.close()
+    return 0
+
+
+
+def dedisp_case(a) -> int:
+    import ctypes as C
+
+    import numpy as np
+    import torch
+    from . import _lib, synth
+    L = _lib.load()
+    dms = (0.5 * np.arange(a.ndm)).astype(np.float32)
+    plan = C.c_void_p()
+    _lib.check(L.psx_dedisp_create(64, a.tsamp, synth.FCH1_MHZ, synth.FOFF_MHZ, C.byref(plan)),
+               "dedisp_create")
+    _lib.check(L.psx_dedisp_set_dm_list(plan, dms.ctypes.data, dms.size), "set_dm_list")
+    nout = a.nsamps - int(L.psx_dedisp_get_max_delay(plan))
+    pitch = (nout + 3) // 4 * 4
+    g = torch.Generator(device="cuda").manual_seed(7)
+    rows = torch.randint(0, 256, (a.nsamps, 64), dtype=torch.uint8, device="cuda", generator=g)
+    out = torch.empty((a.ndm, pitch), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+    for i in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        _lib.check(L.psx_dedisp_execute(plan, a.nsamps, C.c_void_p(rows.data_ptr()), 8,
+                                        C.c_void_p(out.data_ptr()), pitch, 0,
+                                        C.c_void_p(st.cuda_stream)), "dedisp_execute")
+        e1.record(st)
+        e1.synchronize()
+        print(f"dedisperse {a.ndm} DM x {nout} samples: {e0.elapsed_time(e1):.3f} ms")
+    L.psx_dedisp_destroy(plan)
     return 0
 
 

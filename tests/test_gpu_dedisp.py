@@ -191,3 +191,30 @@ def test_whole_program_on_synthetic_tutorial(psx, cuda, oracle, tmp_path):
     assert fast
     best = max(fast, key=lambda c: c["snr"])
     assert abs(best["dm"] - 30.0) <= 7.0, (best["dm"], best["snr"], best["freq"])
+
+
+@pytest.mark.parametrize("nchans,nbits", [(64, 8), (4096, 8), (64, 2), (32, 16)])
+def test_time_gulps_equal_one_pass(psx, cuda, oracle, nchans, nbits):
+    """A scratch limit a few tiles long splits the series into time gulps
+    (overlapping by the maximum delay); device and host input both stay bit
+    for bit equal to the oracle."""
+    torch = cuda
+    tsamp, fch1, foff = 64e-6, 1500.0, -300.0 / nchans
+    h = _plan(psx, nchans, tsamp, fch1, foff)
+    try:
+        dms = np.linspace(0.0, 40.0, 11).astype(np.float32)
+        assert psx.psx_dedisp_set_dm_list(h, dms.ctypes.data, dms.size) == 0
+        md = psx.psx_dedisp_get_max_delay(h)
+        extra = 5000 + 333
+        rng = np.random.default_rng(nchans)
+        v = rng.integers(0, 1 << nbits, (md + extra, nchans), dtype=np.uint32)
+        rows = sigproc.pack_samples(v, nbits)
+        delays = oracle.delay_table(nchans, tsamp, fch1, foff)
+        want = oracle.dedisperse(rows, nbits, nchans, delays, dms, raw=True)
+        el = 2 if nbits == 16 else 1
+        assert psx.psx_dedisp_set_scratch_limit(h, nchans * el * (md + 3000)) == 0
+        assert np.array_equal(_run(psx, torch, h, rows, nbits, dms.size, extra, True), want)
+        assert np.array_equal(_run(psx, torch, h, rows, nbits, dms.size, extra, True,
+                                   host=True), want)
+    finally:
+        psx.psx_dedisp_destroy(h)
