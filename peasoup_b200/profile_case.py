@@ -12,10 +12,10 @@ area), so a capture of any of its kernels stays small while every buffer
 a kernel streams exceeds the 126 MB L2.  Graph capture is off unless
 `--graph` is given, so each kernel is an ordinary stream launch.
 
-With --dedisp: `ndm` DM trials (DM_i = 0.5 i) of nsamps x 64-channel 8-bit
-rows (tsamp as given, fch1 1510 MHz, foff -1.09 MHz), dedispersed four
-times from device memory; at 2^23 samples and 32 DM trials the case holds
-about 2.2 GB.
+With --dedisp: `ndm` DM trials (DM_i = 0.5 i) of nsamps x nchans 8-bit
+rows (tsamp as given, a 70 MHz band from 1510 MHz down: foff -1.09 MHz at
+64 channels), dedispersed four times from device memory; at 2^23 samples,
+64 channels and 32 DM trials the case holds about 2.2 GB.
 """
 from __future__ import annotations
 
@@ -32,6 +32,7 @@ def main(argv=None) -> int:
     ap.add_argument("--graph", action="store_true")
     ap.add_argument("--harm-shape", type=int, default=0)
     ap.add_argument("--dedisp", action="store_true")
+    ap.add_argument("--nchans", type=int, default=64)
     a = ap.parse_args(argv)
     if a.dedisp:
         return dedisp_case(a)
@@ -66,13 +67,15 @@ def dedisp_case(a) -> int:
     L = _lib.load()
     dms = (0.5 * np.arange(a.ndm)).astype(np.float32)
     plan = C.c_void_p()
-    _lib.check(L.psx_dedisp_create(64, a.tsamp, synth.FCH1_MHZ, synth.FOFF_MHZ, C.byref(plan)),
+    foff = synth.FOFF_MHZ * 64 / a.nchans
+    _lib.check(L.psx_dedisp_create(a.nchans, a.tsamp, synth.FCH1_MHZ, foff, C.byref(plan)),
                "dedisp_create")
     _lib.check(L.psx_dedisp_set_dm_list(plan, dms.ctypes.data, dms.size), "set_dm_list")
     nout = a.nsamps - int(L.psx_dedisp_get_max_delay(plan))
     pitch = (nout + 3) // 4 * 4
     g = torch.Generator(device="cuda").manual_seed(7)
-    rows = torch.randint(0, 256, (a.nsamps, 64), dtype=torch.uint8, device="cuda", generator=g)
+    rows = torch.randint(0, 256, (a.nsamps, a.nchans), dtype=torch.uint8, device="cuda",
+                         generator=g)
     out = torch.empty((a.ndm, pitch), dtype=torch.float32, device="cuda")
     st = torch.cuda.current_stream()
     for i in range(4):
@@ -83,7 +86,9 @@ def dedisp_case(a) -> int:
                                         C.c_void_p(st.cuda_stream)), "dedisp_execute")
         e1.record(st)
         e1.synchronize()
-        print(f"dedisperse {a.ndm} DM x {nout} samples: {e0.elapsed_time(e1):.3f} ms")
+        ms = e0.elapsed_time(e1)
+        print(f"dedisperse {a.ndm} DM x {nout} samples x {a.nchans} channels: {ms:.3f} ms, "
+              f"{a.ndm * nout * a.nchans / ms / 1e9:.3f} T channel-adds/s")
     L.psx_dedisp_destroy(plan)
     return 0
 
