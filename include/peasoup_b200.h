@@ -604,6 +604,13 @@ typedef struct {
    PSX_ERR_IO: unreadable file or no HEADER_START. */
 int psx_sigproc_read_header(const char* path, psx_sigproc_header* h);
 
+/* Parses a SIGPROC header held in memory (the first n bytes of a file);
+   nsamples is left as the header gives it.  PSX_ERR_OVERFLOW: the bytes
+   end before HEADER_END (read more and call again); PSX_ERR_IO: not a
+   SIGPROC header.  The parsing half of read_header
+   (include/data_types/header.hpp:339-392). */
+int psx_sigproc_parse_header(const void* h_bytes, size_t n, psx_sigproc_header* h);
+
 /* Reads up to nsamples sample rows starting at start_sample into h_dst
    (nsamples * nchans * nbits / 8 bytes); *h_nread = rows read (fewer at
    the end of the file).  Replaces SigprocFilterbank::load_gulp

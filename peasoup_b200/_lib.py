@@ -190,6 +190,7 @@ SIGNATURES = {
     "psx_server_status": (_i, [_vp, C.POINTER(_sz), C.POINTER(_i), C.POINTER(_i),
                                C.POINTER(_i)]),
     "psx_sigproc_read_header": (_i, [C.c_char_p, C.POINTER(SigprocHeader)]),
+    "psx_sigproc_parse_header": (_i, [_vp, _sz, C.POINTER(SigprocHeader)]),
     "psx_sigproc_read": (_i, [C.c_char_p, C.POINTER(SigprocHeader), _sz, _sz, _vp,
                               C.POINTER(_sz)]),
     "psx_sigproc_write_header": (_i, [C.c_char_p, C.POINTER(SigprocHeader), C.POINTER(_sz)]),

@@ -8,6 +8,7 @@
 // followed by its value in the file's binary layout (int, double or one
 // byte), except source_name and rawdatafile whose value is the next
 // string.  The sample rows follow the header, time slowest.
+#include <algorithm>
 #include <cerrno>
 #include <cstdio>
 #include <cstdlib>
@@ -46,17 +47,78 @@ const Key kKeys[] = {
 
 size_t value_size(Kind k) { return k == kInt ? sizeof(int) : k == kDouble ? sizeof(double) : 1; }
 
-// One header string; false at the end of the file or for a length outside
+// Header bytes in memory, read front to back.
+struct Cursor {
+    const char* p;
+    size_t n, pos;
+    bool read(void* dst, size_t k)
+    {
+        if (pos + k > n) return false;
+        std::memcpy(dst, p + pos, k);
+        pos += k;
+        return true;
+    }
+};
+
+// One header string; false at the end of the bytes or for a length outside
 // 1..79 (the reference's limit).
-bool read_string(std::ifstream& f, std::string* s)
+bool read_string(Cursor& c, std::string* s)
 {
     int len = 0;
-    if (!f.read(reinterpret_cast<char*>(&len), sizeof(int))) return false;
+    if (!c.read(&len, sizeof(int))) return false;
     if (len <= 0 || len >= 80) return false;
     char buf[80];
-    if (!f.read(buf, len)) return false;
+    if (!c.read(buf, (size_t)len)) return false;
     s->assign(buf, (size_t)len);
     return true;
+}
+
+// PSX_OK, PSX_ERR_IO (no HEADER_START, bad string) or PSX_ERR_OVERFLOW
+// (the bytes end before HEADER_END).
+int parse(const char* bytes, size_t n, psx_sigproc_header* h)
+{
+    std::memset(h, 0, sizeof(*h));
+    Cursor c{bytes, n, 0};
+    std::string s;
+    if (!read_string(c, &s) || s != "HEADER_START") {
+        set_error("SIGPROC header: no HEADER_START");
+        return PSX_ERR_IO;
+    }
+    bool want_source = false, want_raw = false;
+    for (;;) {
+        size_t at = c.pos;
+        if (!read_string(c, &s)) {
+            if (at + 80 + sizeof(int) > n) {
+                set_error("SIGPROC header: the bytes end before HEADER_END");
+                return PSX_ERR_OVERFLOW;
+            }
+            set_error("SIGPROC header: malformed keyword at byte %zu", at);
+            return PSX_ERR_IO;
+        }
+        if (s == "HEADER_END") break;
+        if (s == "source_name") { want_source = true; continue; }
+        if (s == "rawdatafile") { want_raw = true; continue; }
+        const Key* key = nullptr;
+        for (const Key& k : kKeys)
+            if (s == k.name) key = &k;
+        if (key) {
+            char* dst = reinterpret_cast<char*>(h) + key->offset;
+            if (!c.read(dst, value_size(key->kind))) {
+                set_error("SIGPROC header: the bytes end inside the value of %s", key->name);
+                return PSX_ERR_OVERFLOW;
+            }
+        } else if (want_source) {
+            std::snprintf(h->source_name, sizeof(h->source_name), "%s", s.c_str());
+            want_source = false;
+        } else if (want_raw) {
+            std::snprintf(h->rawdatafile, sizeof(h->rawdatafile), "%s", s.c_str());
+            want_raw = false;
+        } else {
+            std::fprintf(stderr, "Warning: read_header: unknown parameter %s\n", s.c_str());
+        }
+    }
+    h->header_size = c.pos;
+    return PSX_OK;
 }
 
 void write_string(std::ofstream& f, const char* s)
@@ -70,53 +132,41 @@ void write_string(std::ofstream& f, const char* s)
 
 extern "C" {
 
+int psx_sigproc_parse_header(const void* bytes, size_t n, psx_sigproc_header* h)
+{
+    clear_error();
+    if (!bytes || !h) return PSX_ERR_INVALID;
+    return parse(static_cast<const char*>(bytes), n, h);
+}
+
 int psx_sigproc_read_header(const char* path, psx_sigproc_header* h)
 {
     clear_error();
     if (!path || !h) return PSX_ERR_INVALID;
-    std::memset(h, 0, sizeof(*h));
     std::ifstream f(path, std::ios::in | std::ios::binary);
     if (!f) {
         set_error("psx_sigproc_read_header: cannot open %s", path);
         return PSX_ERR_IO;
     }
-    std::string s;
-    if (!read_string(f, &s) || s != "HEADER_START") {
-        set_error("psx_sigproc_read_header: %s has no HEADER_START", path);
-        return PSX_ERR_IO;
-    }
-    bool want_source = false, want_raw = false;
-    for (;;) {
-        if (!read_string(f, &s)) {
-            set_error("psx_sigproc_read_header: %s: malformed header before HEADER_END", path);
+    f.seekg(0, std::ios::end);
+    const size_t total = (size_t)f.tellg();
+    // headers are a few hundred bytes; read more only if one is longer
+    std::string buf;
+    int rc = PSX_ERR_OVERFLOW;
+    for (size_t want = 4096; rc == PSX_ERR_OVERFLOW; want *= 4) {
+        size_t k = std::min(want, total);
+        buf.resize(k ? k : 1);
+        f.clear();
+        f.seekg(0, std::ios::beg);
+        f.read(&buf[0], (std::streamsize)k);
+        rc = parse(buf.data(), (size_t)f.gcount(), h);
+        if (rc == PSX_ERR_OVERFLOW && k == total) {
+            set_error("psx_sigproc_read_header: %s ends before HEADER_END", path);
             return PSX_ERR_IO;
         }
-        if (s == "HEADER_END") break;
-        if (s == "source_name") { want_source = true; continue; }
-        if (s == "rawdatafile") { want_raw = true; continue; }
-        const Key* key = nullptr;
-        for (const Key& k : kKeys)
-            if (s == k.name) key = &k;
-        if (key) {
-            char* dst = reinterpret_cast<char*>(h) + key->offset;
-            if (!f.read(dst, (std::streamsize)value_size(key->kind))) {
-                set_error("psx_sigproc_read_header: %s: truncated value of %s", path, key->name);
-                return PSX_ERR_IO;
-            }
-        } else if (want_source) {
-            std::snprintf(h->source_name, sizeof(h->source_name), "%s", s.c_str());
-            want_source = false;
-        } else if (want_raw) {
-            std::snprintf(h->rawdatafile, sizeof(h->rawdatafile), "%s", s.c_str());
-            want_raw = false;
-        } else {
-            std::fprintf(stderr, "Warning: read_header: unknown parameter %s\n", s.c_str());
-        }
     }
-    h->header_size = (size_t)f.tellg();
+    if (rc != PSX_OK) return rc;
     if (h->nsamples == 0 && h->nchans > 0 && h->nbits > 0) {
-        f.seekg(0, std::ios::end);
-        size_t total = (size_t)f.tellg();
         size_t data = total >= h->header_size ? total - h->header_size : 0;
         // the reference's order of operations: bytes / nchans * 8 / nbits
         h->nsamples = (int)(data / (size_t)h->nchans * 8 / (size_t)h->nbits);

@@ -218,3 +218,49 @@ def test_time_gulps_equal_one_pass(psx, cuda, oracle, nchans, nbits):
                                    host=True), want)
     finally:
         psx.psx_dedisp_destroy(h)
+
+
+def test_cpp_dropin_headers(psx, cuda, oracle, tmp_path):
+    """The drop-in C++ classes (SigprocFilterbank, read_header, Dedisperser,
+    DispersionTrials), compiled with g++ as the reference's main program
+    uses them: segment, generated DM list and killfile give the oracle's
+    block bit for bit."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "dropin_dedisp")
+    cmd = ["g++", "-O2", "-std=c++17", f"-I{root}/include", "-I/usr/local/cuda/include",
+           f"{root}/tests/cpp/dropin_dedisp.cpp", f"-L{root}/peasoup_b200", "-lpeasoup_b200",
+           "-L/usr/local/cuda/lib64", "-lcudart", f"-Wl,-rpath,{root}/peasoup_b200", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    spec = synth.FilterbankSpec(nsamps=30000, tsamp=128e-6, nbits=2, dm=20.0,
+                                pulsars=[synth.Pulsar(0.0123, 0.0, 0.05, 1.0)])
+    v = synth.filterbank_values(spec, seed=4)
+    path = str(tmp_path / "d.fil")
+    sigproc.write_filterbank(path, sigproc.pack_samples(v, 2), source_name="J1234+5678",
+                             nchans=64, nbits=2, tsamp=128e-6, fch1=synth.FCH1_MHZ,
+                             foff=synth.FOFF_MHZ, tstart=59000.5, nifs=1, data_type=1)
+    kill = tmp_path / "kill.txt"
+    km = np.ones(64, np.int32)
+    km[[3, 40, 41]] = 0
+    kill.write_text("\n".join(str(int(k)) for k in km) + "\n")
+    out = str(tmp_path / "block.bin")
+    r = subprocess.run([exe, path, "2000", "25000", "0", "50", out, "-", str(kill)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    raw = open(out, "rb").read()
+    ndm = int(np.frombuffer(raw, np.int32, 1, 0)[0])
+    ns = int(np.frombuffer(raw, np.int64, 1, 4)[0])
+    meta = np.frombuffer(raw, np.float32, 4, 28)
+    dms = np.frombuffer(raw, np.float32, ndm, 44)
+    block = np.frombuffer(raw, np.float32, ndm * ns, 44 + 4 * ndm).reshape(ndm, ns)
+    fb = sigproc.SigprocFilterbank(path, 2000, 25000)
+    assert list(meta) == [np.float32(fb.get_tsamp()), np.float32(fb.get_fch1()),
+                          np.float32(fb.get_foff()), np.float32(fb.get_cfreq())]
+    want_dms = oracle.dm_list(64, np.float32(128e-6), synth.FCH1_MHZ, synth.FOFF_MHZ, 0.0, 50.0,
+                              64.0, 1.11)
+    assert np.array_equal(dms, want_dms)
+    delays = oracle.delay_table(64, np.float32(128e-6), synth.FCH1_MHZ, synth.FOFF_MHZ)
+    want = oracle.dedisperse(sigproc.pack_samples(v[2000:27000], 2), 2, 64, delays, want_dms,
+                             killmask=km)
+    assert np.array_equal(block.view(np.uint32), want.view(np.uint32))

@@ -263,3 +263,20 @@ def test_oracle_on_tutorial_filterbank(oracle):
     for k in (1, 2, 3):
         i = np.argmin(abs(f - 4.0 * k))
         assert X[i - 2:i + 3].max() > 100
+
+
+def test_parse_header_from_memory(fil_file, psx):
+    """psx_sigproc_parse_header on the file's leading bytes gives the
+    header read_header gives (bar nsamples, which needs the file size);
+    too few bytes ask for more; foreign bytes are rejected."""
+    path, _ = fil_file
+    data = open(path, "rb").read()
+    whole = sigproc.read_header(path)
+    h = _lib.SigprocHeader()
+    assert psx.psx_sigproc_parse_header(data, len(data), C.byref(h)) == 0
+    a, b = _hdr_dict(h), _hdr_dict(whole)
+    a.pop("nsamples"), b.pop("nsamples")
+    assert a == b
+    assert psx.psx_sigproc_parse_header(data, 40, C.byref(h)) == _lib.PSX_ERR_OVERFLOW
+    assert psx.psx_sigproc_parse_header(b"\x03\x00\x00\x00abc" + bytes(200), 207,
+                                        C.byref(h)) == _lib.PSX_ERR_IO
