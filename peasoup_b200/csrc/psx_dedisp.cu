@@ -206,11 +206,16 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
         // 32-bit sums before it can overflow (257 * 255 = 65535)
         constexpr int kUnits = kDdTile8 / 128;
         uint32_t acc[2 * kUnits];
-        uint32_t full[FLUSH ? 4 * kUnits : 1];
+        // 32-bit sums behind the packed pairs, in shared memory (touched once
+        // per 257 channels): s_full[k * 256 + thread], after the offsets
+        uint32_t* s_full = reinterpret_cast<uint32_t*>(
+            smem + 2 * stage_bytes + 2 * kDdWarps * a.cc * (int)sizeof(int));
 #pragma unroll
         for (int k = 0; k < 2 * kUnits; ++k) acc[k] = 0;
+        if constexpr (FLUSH) {
 #pragma unroll
-        for (int k = 0; k < (FLUSH ? 4 * kUnits : 1); ++k) full[k] = 0;
+            for (int k = 0; k < 4 * kUnits; ++k) s_full[k * kDdThreads + threadIdx.x] = 0;
+        }
         int since = 0;
         const uint32_t s_base = (uint32_t)__cvta_generic_to_shared(smem);
         const uint32_t s_offs = s_base + 2u * stage_bytes + (uint32_t)warp * a.cc * 4u;
@@ -227,8 +232,8 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
                     if (since + nj > 257) {
 #pragma unroll
                         for (int k = 0; k < 2 * kUnits; ++k) {
-                            full[2 * k] += acc[k] & 0xffffu;
-                            full[2 * k + 1] += acc[k] >> 16;
+                            s_full[(2 * k) * kDdThreads + threadIdx.x] += acc[k] & 0xffffu;
+                            s_full[(2 * k + 1) * kDdThreads + threadIdx.x] += acc[k] >> 16;
                             acc[k] = 0;
                         }
                         since = 0;
@@ -268,10 +273,10 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
             uint32_t s0 = acc[2 * k] & 0xffffu, s1 = acc[2 * k] >> 16;
             uint32_t s2 = acc[2 * k + 1] & 0xffffu, s3 = acc[2 * k + 1] >> 16;
             if constexpr (FLUSH) {
-                s0 += full[4 * k];
-                s1 += full[4 * k + 1];
-                s2 += full[4 * k + 2];
-                s3 += full[4 * k + 3];
+                s0 += s_full[(4 * k) * kDdThreads + threadIdx.x];
+                s1 += s_full[(4 * k + 1) * kDdThreads + threadIdx.x];
+                s2 += s_full[(4 * k + 2) * kDdThreads + threadIdx.x];
+                s3 += s_full[(4 * k + 3) * kDdThreads + threadIdx.x];
             }
             size_t t = t0 + 4 * lane + 128 * k;
             float4 v = make_float4(map_sum(s0, a.mid, a.scale, a.raw),
@@ -344,6 +349,7 @@ struct psx_dedisp_plan {
     int nlive = 0, ndm_pad = 0, nblk = 0, group = 8, lwin = 0, cc = 0;
     size_t ngroups = 0, max_lo = 0;
     size_t scratch_limit = 4ull << 30;  // bytes of channel-major samples
+    size_t flush_bytes = 0;             // shared 32-bit sums above 257 channels
     std::vector<int> h_tab;
     int* d_tab = nullptr;
     size_t tab_cap = 0;
@@ -423,9 +429,13 @@ struct psx_dedisp_plan {
         ngroups = (size_t)ndm_pad / group;
         const int nwin = kDdWarps / group;
         cc = 0;
+        flush_bytes = (el == 1 && nlive > 257) ? 4ull * (kDdTile8 / 32) * kDdThreads : 0;
+        // with the flush sums, fewer channels per chunk keep 4 CTAs on an SM
+        const size_t cap = flush_bytes ? 56 * 1024 : 96 * 1024;
         for (int c : {16, 8, 4, 2, 1}) {
-            size_t bytes = 2ull * c * nwin * lwin * el + 2ull * kDdWarps * c * sizeof(int);
-            if (bytes <= 96 * 1024 || (c == 1 && bytes <= 200 * 1024)) {
+            size_t bytes = 2ull * c * nwin * lwin * el + 2ull * kDdWarps * c * sizeof(int) +
+                           flush_bytes;
+            if (bytes <= cap || (c == 1 && bytes <= 200 * 1024)) {
                 cc = c;
                 break;
             }
@@ -450,7 +460,8 @@ struct psx_dedisp_plan {
 
     size_t smem_bytes() const
     {
-        return 2ull * cc * (kDdWarps / group) * lwin * elem + 2ull * kDdWarps * cc * sizeof(int);
+        return 2ull * cc * (kDdWarps / group) * lwin * elem + 2ull * kDdWarps * cc * sizeof(int) +
+               flush_bytes;
     }
 
     ~psx_dedisp_plan()

@@ -264,3 +264,48 @@ def test_cpp_dropin_headers(psx, cuda, oracle, tmp_path):
     want = oracle.dedisperse(sigproc.pack_samples(v[2000:27000], 2), 2, 64, delays, want_dms,
                              killmask=km)
     assert np.array_equal(block.view(np.uint32), want.view(np.uint32))
+
+
+def test_whole_program_chunks_dm_file_killfile_zaplist(psx, cuda, tmp_path):
+    """run() with a DM file (an empty line repeats the previous DM), a
+    killfile and a zap list, once in one DM chunk and once in chunks of 4
+    DM trials (the host-RAM rule): the candidates are the same apart from
+    their DM indices, which restart in every chunk as the reference's do."""
+    from peasoup_b200 import output, pipeline
+    spec = synth.FilterbankSpec(nsamps=70000, tsamp=320e-6, nbits=2, dm=30.0,
+                                pulsars=[synth.Pulsar(0.0047, 0.0, 0.1, 0.4)])
+    v = synth.filterbank_values(spec, seed=12)
+    path = str(tmp_path / "c.fil")
+    sigproc.write_filterbank(path, sigproc.pack_samples(v, 2), nchans=64, nbits=2,
+                             tsamp=320e-6, fch1=1510.0, foff=-1.09, tstart=50000.0, nifs=1,
+                             data_type=1)
+    dmf = tmp_path / "dms.txt"
+    dmf.write_text("0\n10\n20\n\n28\n30\n32\n40\n50\n60\n")
+    killf = tmp_path / "kill.txt"
+    km = np.ones(64, np.int32)
+    km[[5, 6, 60]] = 0
+    killf.write_text("\n".join(str(int(k)) for k in km) + "\n")
+    zapf = tmp_path / "zap.txt"
+    zapf.write_text("50.0 0.5\n123.4 0.2\n")
+    dms = sigproc.read_dm_file(str(dmf))
+    assert dms.tolist() == [0, 10, 20, 20, 28, 30, 32, 40, 50, 60]
+    res = {}
+    for name, ram in (("one", 20.0), ("chunks", 4.5 * 70000 * 4 / 1e9)):
+        opts = pipeline.Options(path, outdir=str(tmp_path / name), dm_file=str(dmf),
+                                killfilename=str(killf), zapfilename=str(zapf), min_snr=7.0,
+                                host_ram_limit_gb=ram)
+        res[name] = pipeline.run(opts)
+        assert "<dedispersion_trials" in open(tmp_path / name / "overview.xml").read()
+    (n1, s1), (n2, s2) = res["one"][:2], res["chunks"][:2]
+    assert np.array_equal(s1, s2) and len(n1) > 0
+    for f in ("dm", "acc", "nh", "snr", "freq"):
+        assert np.array_equal(n1[f], n2[f]), f
+    # DM indices: positions in the whole list, then positions within chunks of 4
+    pos = {float(d): i for i, d in reversed(list(enumerate(dms)))}
+    assert all(int(c["dm_idx"]) < 4 for c in n2)
+    assert all(int(c["dm_idx"]) == pos[float(c["dm"])] % 4 or float(c["dm"]) == 20.0
+               for c in n2)
+    top = n1[output.roots(s1)]
+    best = max((c for c in top if _family(float(c["freq"]), 1.0 / 0.0047)),
+               key=lambda c: c["snr"])
+    assert abs(best["dm"] - 30.0) <= 2.0
