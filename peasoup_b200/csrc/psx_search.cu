@@ -23,8 +23,12 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <new>
 #include <thread>
 #include <vector>
@@ -36,6 +40,67 @@
 #include "psx_stages.cuh"
 
 namespace psx {
+
+// Host threads that cluster and distil one DM's records trial by trial.
+// run(fn) calls fn on every worker and on the calling thread and returns
+// when all have returned; fn pulls its own work items.  Each worker takes
+// part in every run: the next run starts only after all of the previous
+// one's calls have returned.
+class WorkPool {
+public:
+    explicit WorkPool(int workers)
+    {
+        for (int i = 0; i < workers; ++i) th_.emplace_back([this] { loop(); });
+    }
+    ~WorkPool()
+    {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    void run(const std::function<void()>& fn)
+    {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            fn_ = &fn;
+            pending_ = (int)th_.size();
+            ++gen_;
+        }
+        cv_.notify_all();
+        fn();
+        std::unique_lock<std::mutex> g(m_);
+        done_.wait(g, [this] { return pending_ == 0; });
+        fn_ = nullptr;
+    }
+
+private:
+    void loop()
+    {
+        int seen = 0;
+        for (;;) {
+            const std::function<void()>* f;
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                f = fn_;
+            }
+            (*f)();
+            std::lock_guard<std::mutex> g(m_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    const std::function<void()>* fn_ = nullptr;
+    int pending_ = 0, gen_ = 0;
+    bool stop_ = false;
+};
 
 // ------------------------------------------------------------ kernels
 // Interbinned amplitude normalised with the DM's statistics
@@ -412,6 +477,7 @@ struct psx_search {
     psx_search_profile prof{};
     psx_search_info info{};
     int nthreads = 1;
+    std::unique_ptr<WorkPool> pool;  // nthreads - 1 workers, made on first use
 
     ~psx_search() { release(); }
 
@@ -931,22 +997,22 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
             per[t].assign(tc.begin(), tc.begin() + keep);
         }
     };
-    const int nth = (nrec > 20000 && nthreads > 1) ? std::min(nthreads, nacc) : 1;
-    if (nth <= 1) {
-        work(0, nacc);
-    } else {
-        std::vector<std::thread> th;
+    // trials in parallel once a DM has enough records to pay for waking the
+    // pool (about 1 us per thread against ~0.1 us of host work per record)
+    if (nrec > 1024 && nacc > 1 && nthreads > 1) {
+        if (!pool) pool.reset(new WorkPool(nthreads - 1));
         std::atomic<int> next{0};
-        const int chunk = std::max(1, nacc / (nth * 4));
-        for (int i = 0; i < nth; ++i)
-            th.emplace_back([&] {
-                for (;;) {
-                    const int b = next.fetch_add(chunk);
-                    if (b >= nacc) break;
-                    work(b, std::min(nacc, b + chunk));
-                }
-            });
-        for (auto& x : th) x.join();
+        const int chunk = std::max(1, nacc / (nthreads * 4));
+        const std::function<void()> fn = [&] {
+            for (;;) {
+                const int b = next.fetch_add(chunk);
+                if (b >= nacc) break;
+                work(b, std::min(nacc, b + chunk));
+            }
+        };
+        pool->run(fn);
+    } else {
+        work(0, nacc);
     }
     out.clear();
     nassoc.clear();
