@@ -5,6 +5,7 @@
 // interleaved float pairs (cufftComplex); all grids are grid-stride loops
 // sized to a multiple of the SM count (psx::grid_for).
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -244,6 +245,111 @@ static float stretch_step(size_t in_count, size_t out_count)
     return (float)(in_count - 1) / (float)(out_count - 1);
 }
 
+// Amplitudes of the complex spectrum X and their three median-of-5
+// levels in one pass: a CTA takes groups of 125 bins (5 * 25) at a time, so
+// every value of the 5-, 25- and 125-bin levels it writes is formed from
+// its own bins; the levels stop where the reference's floor(count / 5)
+// stops them.  The amplitudes themselves are never written.
+constexpr int kScrGroups = 16;  // 125-bin groups per CTA step
+
+__global__ void __launch_bounds__(256) k_amp_scrunch3(const float* __restrict__ X, size_t nbins,
+                                                      float* __restrict__ m5, size_t n5,
+                                                      float* __restrict__ m25, size_t n25,
+                                                      float* __restrict__ m125, size_t n125)
+{
+    __shared__ float s5[kScrGroups * 25];
+    __shared__ float s25[kScrGroups * 5];
+    const size_t ngroups = (n5 + 24) / 25;  // groups holding any 5-level value
+    for (size_t g0 = (size_t)blockIdx.x * kScrGroups; g0 < ngroups;
+         g0 += (size_t)gridDim.x * kScrGroups) {
+        for (int i = threadIdx.x; i < kScrGroups * 25; i += blockDim.x) {
+            const size_t j = g0 * 25 + i;  // 5-level index
+            float v = 0.f;
+            if (j < n5) {
+                const float2* p = reinterpret_cast<const float2*>(X) + 5 * j;
+                float a[5];
+#pragma unroll
+                for (int t = 0; t < 5; ++t) {
+                    const float2 z = p[t];
+                    a[t] = amplitude(z.x, z.y);
+                }
+                v = med5(a[0], a[1], a[2], a[3], a[4]);
+                m5[j] = v;
+            }
+            s5[i] = v;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kScrGroups * 5; i += blockDim.x) {
+            const size_t j = g0 * 5 + i;
+            float v = 0.f;
+            if (j < n25) {
+                const float* q = s5 + 5 * i;
+                v = med5(q[0], q[1], q[2], q[3], q[4]);
+                m25[j] = v;
+            }
+            s25[i] = v;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kScrGroups; i += blockDim.x) {
+            const size_t j = g0 + i;
+            if (j < n125) {
+                const float* q = s25 + 5 * i;
+                m125[j] = med5(q[0], q[1], q[2], q[3], q[4]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+namespace {
+
+// The stretch, splice and division of launch_running_median once the three
+// levels are in the scratch.
+int median_apply(size_t nbins, double bin_width, float b5, float b25, float* d_median, float* d_X,
+                 float* m5, float* m25, float* m125, cudaStream_t s)
+{
+    const size_t n5 = nbins / 5, n25 = nbins / 5 / 5, n125 = nbins / 5 / 5 / 5;
+    int pos5 = (int)((double)b5 / bin_width);
+    int pos25 = (int)((double)b25 / bin_width);
+    MedianLevels L;
+    L.m5 = m5;
+    L.m25 = m25;
+    L.m125 = m125;
+    L.n5 = (unsigned)n5;
+    L.n25 = (unsigned)n25;
+    L.n125 = (unsigned)n125;
+    L.step5 = stretch_step(n5, nbins);
+    L.step25 = stretch_step(n25, nbins);
+    L.step125 = stretch_step(n125, nbins);
+    L.pos5 = (unsigned)(pos5 < 0 ? 0 : (size_t)pos5 > nbins ? nbins : pos5);
+    L.pos25 = (unsigned)(pos25 < 0 ? 0 : (size_t)pos25 > nbins ? nbins : pos25);
+    if (L.pos25 < L.pos5) L.pos25 = L.pos5;
+    k_median_apply<<<grid_for(nbins, 256), 256, 0, s>>>(L, nbins, d_median, d_X);
+    return launch_status("median apply kernel");
+}
+
+}  // namespace
+
+int launch_running_median_spectrum(float* d_X, size_t nbins, double bin_width, float b5,
+                                   float b25, void* d_scratch, cudaStream_t s)
+{
+    if (!d_X || !d_scratch || nbins < 125 || nbins > 0xffffffffu) {
+        set_error("running median: bad arguments (nbins=%zu)", nbins);
+        return PSX_ERR_INVALID;
+    }
+    auto up = [](size_t v) { return (v + 63) / 64 * 64; };
+    float* m5 = static_cast<float*>(d_scratch);
+    float* m25 = m5 + up(nbins / 5 + 1);
+    float* m125 = m25 + up(nbins / 25 + 1);
+    const size_t n5 = nbins / 5, n25 = n5 / 5, n125 = n25 / 5;
+    const size_t ngroups = (n5 + 24) / 25;
+    const unsigned grid = (unsigned)std::min<size_t>((ngroups + kScrGroups - 1) / kScrGroups,
+                                                     (size_t)sm_count() * 8);
+    k_amp_scrunch3<<<grid, 256, 0, s>>>(d_X, nbins, m5, n5, m25, n25, m125, n125);
+    PSX_TRY(launch_status("amplitude + scrunch kernel"));
+    return median_apply(nbins, bin_width, b5, b25, nullptr, d_X, m5, m25, m125, s);
+}
+
 int launch_running_median(const float* d_powers, size_t nbins, double bin_width, float b5,
                           float b25, float* d_median, float* d_X, void* d_scratch,
                           cudaStream_t s)
@@ -459,18 +565,55 @@ __global__ void __launch_bounds__(kVecThreads) k_partials_v4(const float* __rest
     block_partials<kVecThreads>(s, s2, partials);
 }
 
-// One pass of the baseline loop after the mean is known: x -= *mean and,
-// while state[0] says the loop goes on, the partial sums of the new x.  A
-// zero mean (an inactive pass, k_baseline_step writes 0) leaves x as it is
-// and the kernel returns at once.
-__global__ void __launch_bounds__(kVecThreads) k_sub_partials_v4(float* __restrict__ x, size_t n,
-                                                                 const float* __restrict__ mean,
-                                                                 double2* __restrict__ partials,
-                                                                 const unsigned* __restrict__ state)
+// One pass of the device-side baseline loop (reference src/kernels.cu:
+// 463-479) in one kernel.  While *flag_in says the loop goes on, every CTA
+// forms the float mean of the previous pass's partials (float sum / float
+// count; the same fixed-order sum in every CTA), subtracts it, and, while
+// |mean| > 5e-7 n, writes its partials of the new x to part_out; CTA 0
+// records the decision in *flag_out and counts the pass.  Flags and
+// partials alternate between passes, so no CTA reads what this pass writes.
+// With fin_flag set (the last pass) the final decision and the pass count
+// are copied there and to fin_passes.
+__global__ void __launch_bounds__(kVecThreads) k_baseline_pass_v4(
+    float* __restrict__ x, size_t n, double count, const double2* __restrict__ part_in,
+    int nparts, double2* __restrict__ part_out, const unsigned* __restrict__ flag_in,
+    unsigned* __restrict__ flag_out, unsigned* __restrict__ passes,
+    unsigned* __restrict__ fin_flag, unsigned* __restrict__ fin_passes)
 {
-    const float m = *mean;
+    __shared__ float s_mean;
+    __shared__ int s_go;
+    if (*flag_in == 0u) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            *flag_out = 0u;
+            if (fin_flag) {
+                *fin_flag = 0u;
+                *fin_passes = *passes;
+            }
+        }
+        return;
+    }
+    if (threadIdx.x < 32) {
+        double a, b;
+        warp_sum_partials(part_in, nparts, a, b);
+        if (threadIdx.x == 0) {
+            const float mean = __fdiv_rn((float)a, (float)count);
+            s_mean = mean;
+            s_go = (fabsf(mean) > 5e-7 * count) ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    const float m = s_mean;
+    const bool sum = s_go != 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const unsigned np = *passes + 1u;
+        *passes = np;
+        *flag_out = sum ? 1u : 0u;
+        if (fin_flag) {
+            *fin_flag = sum ? 1u : 0u;
+            *fin_passes = np;
+        }
+    }
     if (m == 0.0f) return;
-    const bool sum = state[0] != 0u;
     double s = 0.0, s2 = 0.0;
     const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
     float4* x4 = reinterpret_cast<float4*>(x);
@@ -489,7 +632,7 @@ __global__ void __launch_bounds__(kVecThreads) k_sub_partials_v4(float* __restri
         s += (double)v;
         s2 += (double)v * v;
     }
-    if (sum) block_partials<kVecThreads>(s, s2, partials);
+    if (sum) block_partials<kVecThreads>(s, s2, part_out);
 }
 
 // Partial sums of the interbinned amplitude of the complex spectrum X over
@@ -530,12 +673,15 @@ int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, float* d
     return launch_status("partial sums kernel");
 }
 
-int launch_sub_partials_v4(float* d_x, size_t n, const float* d_mean, double2* d_partials,
-                           const unsigned* d_state, cudaStream_t s)
+int launch_baseline_pass_v4(float* d_x, size_t n, const double2* d_part_in, double2* d_part_out,
+                            const unsigned* d_flag_in, unsigned* d_flag_out, unsigned* d_passes,
+                            unsigned* d_fin_flag, unsigned* d_fin_passes, cudaStream_t s)
 {
-    k_sub_partials_v4<<<reduction_blocks(), kVecThreads, 0, s>>>(d_x, n, d_mean, d_partials,
-                                                                 d_state);
-    return launch_status("baseline subtract kernel");
+    const int nb = reduction_blocks();
+    k_baseline_pass_v4<<<nb, kVecThreads, 0, s>>>(d_x, n, (double)n, d_part_in, nb, d_part_out,
+                                                  d_flag_in, d_flag_out, d_passes, d_fin_flag,
+                                                  d_fin_passes);
+    return launch_status("baseline pass kernel");
 }
 
 int launch_interbin_stats_v4(const float* d_X, size_t nbins, double2* d_partials, double* d_sums,

@@ -234,28 +234,6 @@ __global__ void __launch_bounds__(256) k_unpack_form_norm(const float* __restric
     }
 }
 
-// One pass of the device-side baseline loop (reference src/kernels.cu:
-// 463-479): while state[0] (active) is set, the float mean of the block
-// partials (float sum / float count, as the reference forms it) is
-// written for subtraction and state[0] becomes |mean| > 5e-7 n; once
-// inactive the pass subtracts zero.  state[1] counts the passes.
-__global__ void k_baseline_step(const double2* __restrict__ partials, int nparts, double count,
-                                float* __restrict__ mean_out, unsigned* __restrict__ state)
-{
-    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
-    double a, b;
-    warp_sum_partials(partials, nparts, a, b);
-    if (threadIdx.x != 0) return;
-    const float mean = __fdiv_rn((float)a, (float)count);
-    if (state[0]) {
-        *mean_out = mean;
-        state[1] += 1;
-        state[0] = (fabsf(mean) > 5e-7 * count) ? 1u : 0u;
-    } else {
-        *mean_out = 0.0f;
-    }
-}
-
 // Fused harmonic sums + threshold + compaction: tile shapes and launcher.
 // Persistent grid of MINB CTAs per SM, each one producer warp plus NC
 // consumer threads and kHarmStages shared stages of a T-bin tile and its
@@ -384,7 +362,10 @@ int default_batch(size_t n)
 // Per-DM state that must not be shared by two DMs in flight.
 struct Slot {
     int4* d_rec = nullptr;
-    unsigned* d_count = nullptr;  // [0] hits, [1] kernel error, [2] baseline active, [3] passes
+    // [0] hits, [1] kernel error, [2] baseline still active after the device
+    // passes, [3] passes; [4] the loop's start flag, [5] pass counter, [6..]
+    // the flag each device pass leaves for the next
+    unsigned* d_count = nullptr;
     size_t rec_cap = 0;
     int4* h_rec = nullptr;
     unsigned* h_count = nullptr;
@@ -399,7 +380,6 @@ struct Slot {
     // stream while the previous DM's trials run on the compute stream.
     float* d_tim = nullptr;
     float* d_Xp = nullptr;    // prologue spectrum (Bp complex)
-    float* d_pp = nullptr;    // prologue amplitudes (Bp floats)
     void* d_med = nullptr;
     double2* d_part = nullptr;
     double* d_sums = nullptr;
@@ -523,7 +503,7 @@ struct psx_search {
             if (s.copied) cudaEventDestroy(s.copied);
             for (cudaEvent_t e : s.ev) cudaEventDestroy(e);
             if (s.pst) cudaStreamSynchronize(s.pst);
-            void* sdev[] = {s.d_tim, s.d_Xp, s.d_pp, s.d_med, s.d_part, s.d_sums, s.d_stat,
+            void* sdev[] = {s.d_tim, s.d_Xp, s.d_med, s.d_part, s.d_sums, s.d_stat,
                             s.d_mean};
             for (void* q : sdev)
                 if (q) cudaFree(q);
@@ -656,19 +636,23 @@ int psx_search::prologue(Slot& s)
     // src/kernels.cu:463-479)
     const int nb = reduction_blocks();
     if (!s.host_baseline) {
-        // sums of the series, then per pass: the mean (k_baseline_step)
-        // and one fused subtract + re-sum; passes after convergence return
-        // at once
+        // sums of the series, then per pass one kernel: the mean of the
+        // previous sums, the subtraction and the new sums (which alternate
+        // between the two halves of d_part); passes after convergence
+        // return at once
+        unsigned* st = s.d_count + 4;  // [0] start flag, [1] passes
         if (fused_copy)
-            PSX_TRY(launch_partials_v4(s.series, ncopy, s.d_part, s.d_tim, s.d_count + 2, ps));
+            PSX_TRY(launch_partials_v4(s.series, ncopy, s.d_part, s.d_tim, st, ps));
         else
-            PSX_TRY(launch_partials_v4(s.d_tim, ncopy, s.d_part, nullptr, s.d_count + 2, ps));
+            PSX_TRY(launch_partials_v4(s.d_tim, ncopy, s.d_part, nullptr, st, ps));
         ++s.launches;
         for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
-            k_baseline_step<<<1, 32, 0, ps>>>(s.d_part, nb, (double)ncopy, s.d_mean,
-                                               s.d_count + 2);
-            PSX_TRY(launch_sub_partials_v4(s.d_tim, ncopy, s.d_mean, s.d_part, s.d_count + 2, ps));
-            s.launches += 2;
+            const bool last = pass == kDeviceBaselinePasses - 1;
+            PSX_TRY(launch_baseline_pass_v4(
+                s.d_tim, ncopy, s.d_part + (pass & 1) * nb, s.d_part + ((pass + 1) & 1) * nb,
+                pass == 0 ? st : s.d_count + 6 + pass - 1, s.d_count + 6 + pass, st + 1,
+                last ? s.d_count + 2 : nullptr, last ? s.d_count + 3 : nullptr, ps));
+            ++s.launches;
         }
     } else {
         int count = 0;
@@ -690,12 +674,11 @@ int psx_search::prologue(Slot& s)
     PSX_TRY(s.r2c->exec(s.d_tim, s.d_Xp, ps));
     ++s.ffts;
     // amplitude spectrum (spectrumformer.hpp:16-22)
-    PSX_TRY(psx_form_power_series(s.d_Xp, s.d_pp, B, 0, reinterpret_cast<psx_stream_t>(ps)));
-    ++s.launches;
-    // running median and division (dereddener.hpp:41-66)
-    PSX_TRY(launch_running_median(s.d_pp, B, bin_width, cfg.boundary_5_freq,
-                                  cfg.boundary_25_freq, nullptr, s.d_Xp, s.d_med, ps));
-    s.launches += 4;
+    // amplitudes, their 5/25/125-bin medians, and the division by the
+    // spliced median (spectrumformer.hpp:16-22, dereddener.hpp:41-66)
+    PSX_TRY(launch_running_median_spectrum(s.d_Xp, B, bin_width, cfg.boundary_5_freq,
+                                           cfg.boundary_25_freq, s.d_med, ps));
+    s.launches += 2;
     if (!bf.empty()) {
         PSX_TRY(launch_zap(s.d_Xp, d_bf, d_bw, bin_width_f, bf.size(), B, ps));
         ++s.launches;
@@ -1216,7 +1199,7 @@ size_t psx_search_footprint(const psx_search_config* c)
     const size_t L = (size_t)effective_lanes(c);
     const bool cb = c->mode == PSX_MODE_BATCHED && c->use_fft_callback;
     size_t bytes = 0;
-    bytes += 2 * sizeof(float) * (N + 3 * Bp);        // per slot: series, prologue spectra
+    bytes += 2 * sizeof(float) * (N + 2 * Bp);        // per slot: series, prologue spectrum
     bytes += 2 * median_scratch_bytes(B);
     bytes += L * sizeof(float) * N * (cb ? 1 : b);    // resampled series, per lane
     bytes += L * sizeof(float) * 2 * Bp * b;          // complex spectra, per lane
@@ -1333,12 +1316,11 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->d_p = s->d_pl[0];
     ALLOC(s->d_kbatch, sizeof(double) * b);
     for (Slot& sl : s->slot) {
-        ALLOC(sl.d_count, sizeof(unsigned) * 4);
+        ALLOC(sl.d_count, sizeof(unsigned) * 16);
         ALLOC(sl.d_tim, sizeof(float) * N);
         ALLOC(sl.d_Xp, sizeof(float) * 2 * Bp);
-        ALLOC(sl.d_pp, sizeof(float) * Bp);
         ALLOC(sl.d_med, median_scratch_bytes(s->B));
-        ALLOC(sl.d_part, sizeof(double2) * nb);
+        ALLOC(sl.d_part, sizeof(double2) * 2 * nb);  // two halves: baseline passes alternate
         ALLOC(sl.d_sums, sizeof(double) * 2);
         ALLOC(sl.d_stat, sizeof(float) * 8);
         ALLOC(sl.d_mean, sizeof(float) * 2);
@@ -1388,7 +1370,6 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     cudaMemsetAsync(s->d_kbatch, 0, sizeof(double) * b, s->st);
     for (Slot& sl : s->slot) {
         cudaMemsetAsync(sl.d_Xp, 0, sizeof(float) * 2 * Bp, s->st);
-        cudaMemsetAsync(sl.d_pp, 0, sizeof(float) * Bp, s->st);
     }
     if (cudaEventCreateWithFlags(&s->call_start, cudaEventDisableTiming) != cudaSuccess)
         return fail(PSX_ERR_CUDA);

@@ -45,10 +45,18 @@ int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_
 int launch_partials_v4(const float* d_x, size_t n, double2* d_partials, float* d_copy,
                        unsigned* d_state, cudaStream_t s);
 
-// One baseline pass: x -= *d_mean (nothing when it is 0) and, while
-// d_state[0] is set, the partial sums of the new x.
-int launch_sub_partials_v4(float* d_x, size_t n, const float* d_mean, double2* d_partials,
-                           const unsigned* d_state, cudaStream_t s);
+// One baseline pass in one kernel (the mean of d_part_in formed by every
+// CTA): flags and partials alternate between passes; the last pass also
+// writes the final flag and the pass count to d_fin_flag / d_fin_passes.
+int launch_baseline_pass_v4(float* d_x, size_t n, const double2* d_part_in, double2* d_part_out,
+                            const unsigned* d_flag_in, unsigned* d_flag_out, unsigned* d_passes,
+                            unsigned* d_fin_flag, unsigned* d_fin_passes, cudaStream_t s);
+
+// launch_running_median without the amplitude array: amplitudes of the
+// complex spectrum d_X and their 5/25/125-bin medians in one kernel, then
+// the division of d_X by the spliced median in place.
+int launch_running_median_spectrum(float* d_X, size_t nbins, double bin_width, float b5,
+                                   float b25, void* d_scratch, cudaStream_t s);
 
 // launch_stats(interbinned, first = 0) with 128-bit loads (d_X 16-byte aligned).
 int launch_interbin_stats_v4(const float* d_X, size_t nbins, double2* d_partials, double* d_sums,
