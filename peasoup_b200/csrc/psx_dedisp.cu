@@ -131,6 +131,7 @@ struct DedispArgs {
     size_t out_pitch, nout;
     float mid, scale;
     int raw;
+    int p8, p16;            // channels a byte / a 16-bit sum holds at the input's largest value
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
@@ -163,7 +164,7 @@ __device__ __forceinline__ float map_sum(unsigned s, float mid, float scale, int
     return v;
 }
 
-template <typename T, bool FLUSH>
+template <typename T, bool FLUSH, bool SMALL>
 __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
 {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -202,10 +203,17 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
 
     if constexpr (sizeof(T) == 1) {
         // lane: outputs t0 + 4*lane + 128*k + {0..3}, k = 0..7, as packed
-        // 16-bit pairs; with more than 257 channels a pair is flushed into
-        // 32-bit sums before it can overflow (257 * 255 = 65535)
+        // 16-bit pairs; with more channels than a pair holds (p16: 257 at
+        // 8 bits) a pair is flushed into 32-bit sums before it can overflow.
+        // SMALL (samples of at most 4 bits): the four bytes of a word are
+        // summed as they stand, p8 channels at a time (17 at 4 bits, 85 at
+        // 2, 255 at 1), before they are spread into the 16-bit pairs.
         constexpr int kUnits = kDdTile8 / 128;
         uint32_t acc[2 * kUnits];
+        uint32_t a8[SMALL ? kUnits : 1];
+#pragma unroll
+        for (int k = 0; k < (SMALL ? kUnits : 1); ++k) a8[k] = 0;
+        int since8 = 0;
         // 32-bit sums behind the packed pairs, in shared memory (touched once
         // per 257 channels): s_full[k * 256 + thread], after the offsets
         uint32_t* s_full = reinterpret_cast<uint32_t*>(
@@ -228,8 +236,29 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
             const int st = q & 1;
             const int nj = min(a.cc, a.nlive - q * a.cc);
             if (active) {
+                if constexpr (SMALL) {
+                    if (since8 + nj > a.p8) {
+#pragma unroll
+                        for (int k = 0; k < kUnits; ++k) {
+                            acc[2 * k] += __byte_perm(a8[k], 0, 0x4140);
+                            acc[2 * k + 1] += __byte_perm(a8[k], 0, 0x4342);
+                            a8[k] = 0;
+                        }
+                        since8 = 0;
+                    }
+                    since8 += nj;
+                }
                 if constexpr (FLUSH) {
-                    if (since + nj > 257) {
+                    if (since + nj > a.p16) {
+                        if constexpr (SMALL) {
+#pragma unroll
+                            for (int k = 0; k < kUnits; ++k) {
+                                acc[2 * k] += __byte_perm(a8[k], 0, 0x4140);
+                                acc[2 * k + 1] += __byte_perm(a8[k], 0, 0x4342);
+                                a8[k] = 0;
+                            }
+                            since8 = nj;
+                        }
 #pragma unroll
                         for (int k = 0; k < 2 * kUnits; ++k) {
                             s_full[(2 * k) * kDdThreads + threadIdx.x] += acc[k] & 0xffffu;
@@ -251,8 +280,12 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
                     {                                                             \
                         uint32_t v = __funnelshift_r(lds32o<128 * (k)>(ad),       \
                                                      lds32o<128 * (k) + 4>(ad), sh); \
-                        acc[2 * (k)] += __byte_perm(v, 0, 0x4140);                \
-                        acc[2 * (k) + 1] += __byte_perm(v, 0, 0x4342);            \
+                        if constexpr (SMALL) {                                    \
+                            a8[(k)] += v;                                         \
+                        } else {                                                  \
+                            acc[2 * (k)] += __byte_perm(v, 0, 0x4140);            \
+                            acc[2 * (k) + 1] += __byte_perm(v, 0, 0x4342);        \
+                        }                                                         \
                     }
                     PSX_DD_STEP(0)
                     PSX_DD_STEP(1)
@@ -268,6 +301,13 @@ __global__ void __launch_bounds__(kDdThreads) k_dedisperse(DedispArgs a)
             __syncthreads();
         }
         if (!active) return;
+        if constexpr (SMALL) {
+#pragma unroll
+            for (int k = 0; k < kUnits; ++k) {
+                acc[2 * k] += __byte_perm(a8[k], 0, 0x4140);
+                acc[2 * k + 1] += __byte_perm(a8[k], 0, 0x4342);
+            }
+        }
 #pragma unroll
         for (int k = 0; k < kUnits; ++k) {
             uint32_t s0 = acc[2 * k] & 0xffffu, s1 = acc[2 * k] >> 16;
@@ -614,6 +654,8 @@ int dedisperse(psx_dedisp_plan* p, int nbits, size_t pitch, size_t nout, float* 
     a.mid = (float)(0.5 * (double)p->nchans * (double)m);
     a.scale = (float)(1.0 / ((double)m * std::sqrt((double)p->nchans)));
     a.raw = (flags & PSX_DEDISP_RAW) ? 1 : 0;
+    a.p8 = (int)(255u / m);
+    a.p16 = (int)(65535u / m);
     const size_t tile = dd_tile(nbits == 16 ? 2 : 1);
     size_t ntiles = (nout + tile - 1) / tile;
     size_t nblocks = ntiles * (size_t)p->nblk;
@@ -624,17 +666,19 @@ int dedisperse(psx_dedisp_plan* p, int nbits, size_t pitch, size_t nout, float* 
     size_t smem = p->smem_bytes();
     const unsigned grid = (unsigned)nblocks;
     if (nbits == 16) {
-        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint16_t, false>,
+        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint16_t, false, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_dedisperse<uint16_t, false><<<grid, kDdThreads, smem, st>>>(a);
-    } else if (p->nlive > 257) {
-        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint8_t, true>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_dedisperse<uint8_t, true><<<grid, kDdThreads, smem, st>>>(a);
+        k_dedisperse<uint16_t, false, false><<<grid, kDdThreads, smem, st>>>(a);
     } else {
-        PSX_CUDA(cudaFuncSetAttribute(k_dedisperse<uint8_t, false>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_dedisperse<uint8_t, false><<<grid, kDdThreads, smem, st>>>(a);
+        // 8 bits and below: the flush and small-sample variants
+        const bool flush = p->nlive > a.p16, small = nbits <= 4;
+        auto kern = small ? (flush ? k_dedisperse<uint8_t, true, true>
+                                   : k_dedisperse<uint8_t, false, true>)
+                          : (flush ? k_dedisperse<uint8_t, true, false>
+                                   : k_dedisperse<uint8_t, false, false>);
+        PSX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        kern<<<grid, kDdThreads, smem, st>>>(a);
     }
     return launch_status("k_dedisperse");
 }

@@ -12,7 +12,7 @@ area), so a capture of any of its kernels stays small while every buffer
 a kernel streams exceeds the 126 MB L2.  Graph capture is off unless
 `--graph` is given, so each kernel is an ordinary stream launch.
 
-With --dedisp: `ndm` DM trials (DM_i = 0.5 i) of nsamps x nchans 8-bit
+With --dedisp: `ndm` DM trials (DM_i = 0.5 i) of nsamps x nchans nbits-bit
 rows (tsamp as given, a 70 MHz band from 1510 MHz down: foff -1.09 MHz at
 64 channels), dedispersed four times from device memory; at 2^23 samples,
 64 channels and 32 DM trials the case holds about 2.2 GB.
@@ -33,6 +33,7 @@ def main(argv=None) -> int:
     ap.add_argument("--harm-shape", type=int, default=0)
     ap.add_argument("--dedisp", action="store_true")
     ap.add_argument("--nchans", type=int, default=64)
+    ap.add_argument("--nbits", type=int, default=8)
     a = ap.parse_args(argv)
     if a.dedisp:
         return dedisp_case(a)
@@ -74,20 +75,21 @@ def dedisp_case(a) -> int:
     nout = a.nsamps - int(L.psx_dedisp_get_max_delay(plan))
     pitch = (nout + 3) // 4 * 4
     g = torch.Generator(device="cuda").manual_seed(7)
-    rows = torch.randint(0, 256, (a.nsamps, a.nchans), dtype=torch.uint8, device="cuda",
-                         generator=g)
+    rows = torch.randint(0, 256, (a.nsamps, a.nchans * a.nbits // 8), dtype=torch.uint8,
+                         device="cuda", generator=g)
     out = torch.empty((a.ndm, pitch), dtype=torch.float32, device="cuda")
     st = torch.cuda.current_stream()
     for i in range(4):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        _lib.check(L.psx_dedisp_execute(plan, a.nsamps, C.c_void_p(rows.data_ptr()), 8,
+        _lib.check(L.psx_dedisp_execute(plan, a.nsamps, C.c_void_p(rows.data_ptr()), a.nbits,
                                         C.c_void_p(out.data_ptr()), pitch, 0,
                                         C.c_void_p(st.cuda_stream)), "dedisp_execute")
         e1.record(st)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
-        print(f"dedisperse {a.ndm} DM x {nout} samples x {a.nchans} channels: {ms:.3f} ms, "
+        print(f"dedisperse {a.ndm} DM x {nout} samples x {a.nchans} {a.nbits}-bit channels: "
+              f"{ms:.3f} ms, "
               f"{a.ndm * nout * a.nchans / ms / 1e9:.3f} T channel-adds/s")
     L.psx_dedisp_destroy(plan)
     return 0

@@ -1,7 +1,8 @@
 """Dedispersion on the GPU against the oracle, bit for bit: every input
 width (1, 2, 4, 8, 16 bits), raw and mapped output, sorted, generated and
 unsorted DM lists (the wide-spread window path), killed channels, more
-channels than a packed 16-bit accumulator holds (4096), DM counts that do
+channels than a packed 16-bit accumulator holds (4096 at 8 bits, 4400 at
+4 bits, where bytes are first summed as they stand), DM counts that do
 not fill a CTA, a single output sample, host and device input; then the
 Dedisperser class on a file, and the whole program (run) on a synthetic
 tutorial-shaped filterbank: its pulsar is found at its DM, and its
@@ -51,6 +52,7 @@ CASES = [
     (64, 8, 64e-6, 1510.0, -1.09, "unsorted:2000:21", 700),
     (4096, 8, 64e-6, 1500.0, -0.0732421875, "sorted:8", 777),
     (300, 8, 64e-6, 1500.0, -0.5, "sorted:3", 1),
+    (4400, 4, 64e-6, 1500.0, -300.0 / 4400, "sorted:3", 300),
     (64, 8, 64e-6, 1510.0, -1.09, "zero", 513),
 ]
 
