@@ -319,16 +319,31 @@ __device__ __forceinline__ void exact_body(const float* __restrict__ sm,
     FracStep<0, F, T, NC, true>::run(sm, base, acc, mx, fs, i0, tid, pp, trial, rec, counter, cap);
 }
 
+// Shared-memory offset of fraction q's source for consumer `tid`.
+template <int F, int T>
+__device__ __forceinline__ void make_bases(unsigned tid,
+                                           unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1])
+{
+#pragma unroll
+    for (int q = 0; q < nfrac(F); ++q) {
+        const unsigned hh = (unsigned)frac_h(q), mm = (unsigned)frac_m(q);
+        base[q] = (unsigned)slot_offset(q, T) + ((tid * mm + (1u << (hh - 1))) >> hh);
+    }
+}
+
 // The same, kept out of line so that the fast pass does not share its
-// registers (a call frame in local memory is the price).
+// registers.  It rebuilds the offsets and scales itself: handing the fast
+// pass's arrays to a call would give them an address and move them from
+// registers to local memory for the fast pass too.
 template <int F, int T, int NC>
-__device__ __noinline__ void exact_pass_ool(const float* __restrict__ sm,
-                                            const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
-                                            const FoldScales& fs, unsigned i0, unsigned tid,
-                                            const PeakParams& pp, int trial,
+__device__ __noinline__ void exact_pass_ool(const float* __restrict__ sm, unsigned i0,
+                                            unsigned tid, const PeakParams& pp, int trial,
                                             int4* __restrict__ rec, unsigned* __restrict__ counter,
                                             unsigned cap)
 {
+    unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
+    make_bases<F, T>(tid, base);
+    const FoldScales fs;
     exact_body<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
 }
 
@@ -356,7 +371,7 @@ __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
     for (int k = 0; k < K; ++k) over |= mx[k] > pp.vote;
     if (__any_sync(0xffffffffu, over)) {
         if (OOL)
-            exact_pass_ool<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
+            exact_pass_ool<F, T, NC>(sm, i0, tid, pp, trial, rec, counter, cap);
         else
             exact_body<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
     }
@@ -459,11 +474,7 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
         const unsigned tid = threadIdx.x - 32;
         const FoldScales fs;
         unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
-#pragma unroll
-        for (int q = 0; q < nfrac(F); ++q) {
-            const unsigned hh = (unsigned)frac_h(q), mm = (unsigned)frac_m(q);
-            base[q] = (unsigned)slot_offset(q, T) + ((tid * mm + (1u << (hh - 1))) >> hh);
-        }
+        make_bases<F, T>(tid, base);
         unsigned ph = 0;
         for (;;) {
 #pragma unroll
