@@ -853,3 +853,22 @@ def ref_filterbank_gulp(path: str, seg_start: int, seg_n: int, start: int, n: in
     meta = np.zeros(9, np.float64)
     got = fn(path.encode(), seg_start, seg_n, start, n, out.ctypes.data, out.size, meta)
     return out[:got * row_bytes], meta
+
+
+def ref_write_timeseries(outdir: str, stem: str, block, dms, idx: int, hd, hi,
+                         source_name: str) -> int:
+    """The reference's DispersionTrials::write_timeseries_to_file (host code
+    of oracle/_ref/libpeasoup_ref_gpu.so; no device call)."""
+    if not os.path.exists(REF_GPU_PATH):
+        raise FileNotFoundError(REF_GPU_PATH)
+    L = C.CDLL(REF_GPU_PATH)
+    f = L.ref_write_timeseries
+    f.restype = C.c_int
+    f.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                  C.c_size_t, C.c_void_p, C.c_void_p, C.c_char_p]
+    b = np.ascontiguousarray(block, np.float32)
+    d = np.ascontiguousarray(dms, np.float32)
+    hd = np.ascontiguousarray(hd, np.float64)
+    hi = np.ascontiguousarray(hi, np.int32)
+    return f(outdir.encode(), stem.encode(), b.ctypes.data, b.shape[1], d.ctypes.data, d.size,
+             idx, hd.ctypes.data, hi.ctypes.data, source_name.encode())

@@ -359,3 +359,37 @@ int ref_worker_search_forest(const float* series, size_t ndm, size_t nsamps, flo
 }
 
 }  // extern "C"
+
+/* DispersionTrials::write_timeseries_to_file (include/data_types/
+   timeseries.hpp:520-594) as the reference's main calls it for a dump
+   (src/pipeline_multi.cu:505-512): series `idx` of a block of ndm series of
+   nsamps samples, under `outdir` with the file stem `stem`.  hd holds
+   src_raj, src_dej, tstart, tsamp, fch1, foff; hi holds telescope_id,
+   machine_id, nchans.  Host code only (no device call). */
+extern "C" int ref_write_timeseries(const char* outdir, const char* stem, const float* data,
+                                    size_t nsamps, const float* dms, size_t ndm, size_t idx,
+                                    const double* hd, const int* hi, const char* source_name)
+{
+    try {
+        DispersionTrials<float> trials((float)hd[3]);
+        std::vector<float> dl(dms, dms + ndm);
+        trials.resize(nsamps, dl);
+        std::memcpy(trials.get_data_ptr(), data, sizeof(float) * nsamps * ndm);
+        SigprocHeader h;
+        h.src_raj = hd[0];
+        h.src_dej = hd[1];
+        h.tstart = hd[2];
+        h.tsamp = hd[3];
+        h.fch1 = hd[4];
+        h.foff = hd[5];
+        h.telescope_id = hi[0];
+        h.machine_id = hi[1];
+        h.nchans = hi[2];
+        h.source_name = source_name;
+        trials.write_timeseries_to_file(outdir, stem, idx, h);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -91,6 +91,8 @@ class Options:
     progress_bar: bool = False
     start_sample: int = 0
     nsamples: int = 0
+    timeseries_dump_dir: str = ""
+    no_search: bool = False
 
     def f32(self, name: str) -> np.float32:
         return np.float32(getattr(self, name))
@@ -129,7 +131,13 @@ def run(opts: Options, *, devices=(0,), params_overrides: Optional[Dict[str, obj
     GPU: read the filterbank segment, make or read the DM list, dedisperse
     each DM chunk into device memory, search it, then distil, score and
     write candidates.peasoup and overview.xml into opts.outdir.  Returns
-    what output.finish returns plus a dict of stage wall times."""
+    what output.finish returns plus a dict of stage wall times.
+
+    With opts.timeseries_dump_dir every dedispersed series is also written
+    there as <stem>_DM<dm>.dat / .inf (sigproc.write_timeseries), and with
+    opts.no_search as well nothing is searched and None is returned.  (The
+    reference stops after dumping its first DM chunk,
+    src/pipeline_multi.cu:505-515; here every chunk is dumped.)"""
     import torch
 
     from .dedisperse import Dedisperser
@@ -198,6 +206,17 @@ def run(opts: Options, *, devices=(0,), params_overrides: Optional[Dict[str, obj
         trials = dd.dedisperse(None, fil.get_start_sample(), fil.get_end_sample(), gulp)
         torch.cuda.synchronize()
         timers["dedispersion"] += time.perf_counter() - t0
+        if opts.timeseries_dump_dir:
+            import os
+            from .sigproc import write_timeseries
+            os.makedirs(opts.timeseries_dump_dir, exist_ok=True)
+            stem = os.path.splitext(os.path.basename(opts.infilename))[0]
+            host = trials.to_host()
+            for ii, dm in enumerate(chunk):
+                write_timeseries(opts.timeseries_dump_dir, stem, host[ii], dm, header)
+            if opts.no_search:
+                dd.close()
+                continue
         t0 = time.perf_counter()
         # DM indices restart in every chunk, as the reference's DMDispenser's do
         nodes, sizes, _, _ = eng.search_block(trials.rows(), chunk,
@@ -208,6 +227,8 @@ def run(opts: Options, *, devices=(0,), params_overrides: Optional[Dict[str, obj
         dd.close()
         del trials
     eng.close()
+    if opts.timeseries_dump_dir and opts.no_search:
+        return None
 
     acc_plan = AccelerationPlan(params.acc_lo, params.acc_hi, params.acc_tol, params.acc_pulse_width,
                                 size, params.tsamp, params.cfreq_hz, params.ch_bw_hz)

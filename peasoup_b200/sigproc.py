@@ -19,7 +19,7 @@ from . import _lib
 from ._lib import SigprocHeader, check, load
 
 __all__ = ["SigprocHeader", "read_header", "write_header", "write_filterbank",
-           "SigprocFilterbank", "read_dm_file", "prev_power_of_two"]
+           "SigprocFilterbank", "read_dm_file", "prev_power_of_two", "write_timeseries"]
 
 
 def read_header(path: str) -> SigprocHeader:
@@ -167,3 +167,65 @@ class SigprocFilterbank:
                                       C.byref(n)), "sigproc_read")
         self.data = buf[:n.value * rb]
         return n.value
+
+
+def _sexagesimal(value: float, signed: bool) -> str:
+    """A SIGPROC angle (hhmmss.s / ddmmss.s packed in a double) as
+    hh:mm:ss.ss, as the reference prints it (src/utils.cpp:14-74): the
+    seconds get two decimals and no zero padding."""
+    sign = -1 if value < 0 else 1
+    a = abs(value)
+    first = int(a / 1e4)
+    second = int((a - first * 1e4) / 1e2)
+    third = a - first * 1e4 - second * 1e2
+    s = "%02d:%02d:%.2f" % (first, second, third)
+    return ("-" + s) if (signed and sign < 0) else s
+
+
+def write_timeseries(outdir: str, stem: str, series: np.ndarray, dm: float,
+                     header: SigprocHeader) -> str:
+    """One dedispersed series as `<outdir>/<stem>_DM<dm>.dat` (float32, an
+    even number of samples) and its PRESTO-style `.inf`, as the reference's
+    time-series dump writes them (DispersionTrials::write_timeseries_to_file,
+    include/data_types/timeseries.hpp:520-594).  Returns the file prefix."""
+    import os
+    import pwd
+    prefix = "%s/%s_DM%09.3f" % (outdir, stem, float(np.float32(dm)))
+    x = np.ascontiguousarray(series, np.float32)
+    n = x.size - (x.size % 2)
+    x[:n].tofile(prefix + ".dat")
+    h = header
+    nchans = int(h.nchans)
+    bw = float(h.foff) * nchans
+    lowest = float(h.fch1) + float(h.foff) * (nchans - 1) if h.foff < 0 else float(h.fch1)
+    try:
+        login = pwd.getpwuid(os.getuid()).pw_name
+    except KeyError:
+        login = str(os.getuid())
+    lines = [
+        " Data file name without suffix          =  %s" % prefix,
+        " Telescope used                         =  %d" % h.telescope_id,
+        " Instrument used                        =  %d" % h.machine_id,
+        " Object being observed                  =  %s" % h.source_name.decode(errors="replace"),
+        " J2000 Right Ascension (hh:mm:ss.ssss)  =  %s" % _sexagesimal(h.src_raj, False),
+        " J2000 Declination     (dd:mm:ss.ssss)  =  %s" % _sexagesimal(h.src_dej, True),
+        " Data observed by                       =  pulsar_astronomer",
+        " Epoch of observation (MJD)             =  %.15f" % h.tstart,
+        " Barycentered?           (1=yes, 0=no)  =  0",
+        " Number of bins in the time series      =  %d" % n,
+        " Width of each time series bin (sec)    =  %.15f" % h.tsamp,
+        " Any breaks in the data? (1 yes, 0 no)  =  0",
+        " Type of observation (EM band)          =  Radio",
+        " Beam diameter (arcsec)                 =  3600",
+        " Dispersion measure (cm-3 pc)           =  %.15f" % float(np.float32(dm)),
+        " Central freq of low channel (Mhz)      =  %.15f" % lowest,
+        " Total bandwidth (Mhz)                  =  %.6f" % abs(bw),
+        " Number of channels                     =  %d" % nchans,
+        " Channel bandwidth (Mhz)                =  %.6f" % abs(bw),
+        " Data analyzed by                       =  %s" % login,
+        " Any additional notes:",
+        "    File written by Peasoup pulsar search package",
+    ]
+    with open(prefix + ".inf", "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return prefix

@@ -311,3 +311,45 @@ def test_whole_program_chunks_dm_file_killfile_zaplist(psx, cuda, tmp_path):
     best = max((c for c in top if _family(float(c["freq"]), 1.0 / 0.0047)),
                key=lambda c: c["snr"])
     assert abs(best["dm"] - 30.0) <= 2.0
+
+
+def test_whole_program_timeseries_dump(psx, cuda, oracle, tmp_path):
+    """run() with a dump directory writes every DM trial's series of every
+    DM chunk (the oracle's dedispersion of that chunk, an even number of
+    samples) and its .inf; with no_search nothing is searched and no output
+    files appear."""
+    from peasoup_b200 import pipeline
+    v = synth.filterbank_values(synth.FilterbankSpec(nsamps=20001, tsamp=320e-6, nbits=2),
+                                seed=13)
+    path = str(tmp_path / "obs.fil")
+    sigproc.write_filterbank(path, sigproc.pack_samples(v, 2), nchans=64, nbits=2, tsamp=320e-6,
+                             fch1=1510.0, foff=-1.09, tstart=50000.0, nifs=1, data_type=1,
+                             source_name="OBS")
+    dmf = tmp_path / "dms.txt"
+    dmf.write_text("0\n5.25\n30\n")
+    dump = tmp_path / "dump"
+    out = pipeline.run(pipeline.Options(path, outdir=str(tmp_path / "out"), dm_file=str(dmf),
+                                        timeseries_dump_dir=str(dump), no_search=True,
+                                        host_ram_limit_gb=2 * 20001 * 4 / 1e9 * 1.1))
+    assert out is None and not (tmp_path / "out").exists()
+    names = sorted(os.listdir(dump))
+    assert names == ["obs_DM00000.000.dat", "obs_DM00000.000.inf", "obs_DM00005.250.dat",
+                     "obs_DM00005.250.inf", "obs_DM00030.000.dat", "obs_DM00030.000.inf"]
+    # chunks of two DM trials, each with its own maximum delay and length
+    delays = oracle.delay_table(64, np.float32(320e-6), 1510.0, -1.09)
+    # the header has no nsamples: the count comes from the file size as the
+    # reference forms it (bytes / nchans * 8 / nbits), 20000 of the 20001
+    total = sigproc.SigprocFilterbank(path).get_total_nsamps()
+    assert total == 20000
+    rows = sigproc.pack_samples(v[:total], 2)
+    want = [oracle.dedisperse(rows, 2, 64, delays, np.array(c, np.float32))
+            for c in ([0.0, 5.25], [30.0])]
+    series = [want[0][0], want[0][1], want[1][0]]
+    assert len(series[0]) != len(series[2])
+    for i, dm in enumerate(("00000.000", "00005.250", "00030.000")):
+        got = np.fromfile(dump / f"obs_DM{dm}.dat", np.float32)
+        n = series[i].size - series[i].size % 2
+        assert got.size == n and np.array_equal(got.view(np.uint32), series[i][:n].view(np.uint32))
+        inf = open(dump / f"obs_DM{dm}.inf").read()
+        assert f"Number of bins in the time series      =  {n}\n" in inf
+        assert "Object being observed                  =  OBS\n" in inf

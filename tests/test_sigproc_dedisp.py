@@ -280,3 +280,40 @@ def test_parse_header_from_memory(fil_file, psx):
     assert psx.psx_sigproc_parse_header(data, 40, C.byref(h)) == _lib.PSX_ERR_OVERFLOW
     assert psx.psx_sigproc_parse_header(b"\x03\x00\x00\x00abc" + bytes(200), 207,
                                         C.byref(h)) == _lib.PSX_ERR_IO
+
+
+def test_timeseries_dump_equals_reference_writer(tmp_path, psx):
+    """sigproc.write_timeseries writes the .dat and .inf files the
+    reference's DispersionTrials::write_timeseries_to_file writes (an odd
+    sample count drops its last sample; coordinates with unpadded seconds;
+    fixed-point fields as the reference's stream leaves them)."""
+    from oracle import oracle as O
+    if not os.path.exists(O.REF_GPU_PATH):
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(9)
+    block = rng.standard_normal((3, 1001)).astype(np.float32)
+    dms = np.array([0.0, 12.5, 123.456], np.float32)
+    cases = [(123405.5, -453012.25, 6, 10, 64, -1.09), (2830.0, 51200.75, 0, 0, 4096, -0.0732),
+             (-10203.25, -5.5, 1, 2, 96, 1.5)]
+    for n, (raj, dej, tel, mach, nch, foff) in enumerate(cases):
+        hd = np.array([raj, dej, 60000.123456789, 6.4e-05, 1510.0, foff])
+        hi = np.array([tel, mach, nch], np.int32)
+        for idx in range(3):
+            ref_dir, our_dir = tmp_path / f"ref{n}{idx}", tmp_path / f"our{n}{idx}"
+            ref_dir.mkdir()
+            our_dir.mkdir()
+            assert O.ref_write_timeseries(str(ref_dir), "stem", block, dms, idx, hd, hi,
+                                          "J0000+0000") == 0
+            h = sigproc.make_header(src_raj=raj, src_dej=dej, tstart=60000.123456789,
+                                    tsamp=6.4e-05, fch1=1510.0, foff=foff, telescope_id=tel,
+                                    machine_id=mach, nchans=nch, source_name="J0000+0000")
+            sigproc.write_timeseries(str(our_dir), "stem", block[idx], dms[idx], h)
+            names = sorted(os.listdir(ref_dir))
+            assert names == sorted(os.listdir(our_dir)) and len(names) == 2
+            for fn in names:
+                a = open(ref_dir / fn, "rb").read()
+                b = open(our_dir / fn, "rb").read()
+                if fn.endswith(".inf"):
+                    a = a.replace(str(ref_dir).encode(), b"DIR")
+                    b = b.replace(str(our_dir).encode(), b"DIR")
+                assert a == b, fn
