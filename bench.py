@@ -624,7 +624,7 @@ def run_psx(args, ws, rank, local):
 
     # ---- autotuner (untimed): trials per launch group x harmonic-kernel shape
     tune = None
-    batch, shape = args.batch, 0
+    batch, shape = args.batch, args.harm_shape
     if not args.batch:
         t0 = time.perf_counter()
         tune = search.autotune(make_params(plan, "batched"), batches=(8, 16, 32, 64), reps=2)
@@ -974,7 +974,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="psx", choices=["psx", "reference"])
     ap.add_argument("--dms-per-step", type=int, default=8)
-    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="trials per launch group (0: autotuned together with the shape)")
+    ap.add_argument("--harm-shape", type=int, default=0,
+                    help="with --batch: harmonic-kernel shape (0: the default shape)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
