@@ -53,6 +53,10 @@ ACC = 100.0
 NFOLDS = 5
 NDM = 256
 SERVED_REQUESTS = 32
+FFT_FORMS = {1: "cuFFT complex transform + fused unpack/interbin/normalise",
+             2: "cuFFT real transform + interbin/normalise (the reference's)",
+             3: "two-pass transform with the resample gather in pass 1 + "
+                "unpack/interbin/normalise"}
 SERVED_TRIAL_BUDGET = 2000
 SERVED_SLOTS = 2
 SERVED_BUDGET = 150_000_000_000
@@ -668,6 +672,7 @@ def run_psx(args, ws, rank, local):
     dt = e0.elapsed_time(e1) / 1e3
     batch_used = eng.info()["batch"]
     shape_used = eng.info()["harm_shape"]
+    form_used = eng.info()["fft_form"]
     dt_max = max_over_ranks(ws, dt)
     tot_trials = sum_over_ranks(ws, ntr)
     value = tot_trials / dt_max
@@ -814,8 +819,7 @@ def run_psx(args, ws, rank, local):
                        "dms_per_step": S, "mode": "batched",
                        "batch": batch_used, "harm_shape": shape_used,
                        "graphs": not args.no_graph, "lanes": args.lanes or 1,
-                       "fft_form": "real transform + form" if args.fft_form == 2 else
-                                   "complex transform + fused unpack/interbin/normalise",
+                       "fft_form": FFT_FORMS.get(form_used, str(form_used)),
                        "tuned": "autotuner (batch x harmonic shape)" if tune else "fixed",
                        "parallelism": f"dm-sharded x{ws}",
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
@@ -982,8 +986,10 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--fft-form", type=int, default=0,
-                    help="1: complex transform + fused unpack/interbin/normalise (default); "
-                         "2: the reference's real transform + interbin/normalise")
+                    help="0: default (3 where the length allows it); 1: cuFFT complex "
+                         "transform + fused unpack/interbin/normalise; 2: the reference's "
+                         "real transform + interbin/normalise; 3: the library's two-pass "
+                         "transform with the resample gather in its first pass")
     ap.add_argument("--lanes", type=int, default=0,
                     help="streams the launch groups alternate over (0: the engine's default)")
     ap.add_argument("--no-graph", action="store_true",

@@ -392,11 +392,16 @@ typedef struct {
                                   many streams with their own buffers, so one
                                   group's harmonic sums overlap the next one's
                                   transform (1 or 2; 0 = 1) */
-    int fft_form;              /* batched: 0 = default (1); 1 = complex transform
-                                  of the series read as interleaved pairs, then
+    int fft_form;              /* batched: 0 = default (3 where fft_size allows
+                                  it, else 1); 1 = cuFFT complex transform of
+                                  the series read as interleaved pairs, then
                                   one kernel that unpacks the real spectrum,
                                   interbins and normalises; 2 = the reference's
-                                  real transform, then interbin + normalise */
+                                  real transform, then interbin + normalise;
+                                  3 = the library's own two-pass transform of
+                                  the interleaved pairs with the resample
+                                  gather in its first pass, then the unpack
+                                  kernel (fft_size 2^19 .. 2^25) */
 } psx_search_config;
 
 /* Number of tile shapes of the fused harmonic-sum kernel (tile bins,
@@ -481,6 +486,10 @@ typedef struct {
     int harm_shape;       /* harmonic-kernel tile shape in use */
     int capture_fallbacks; /* schedules launched directly because their
                               graph capture was invalidated */
+    int fft_form;         /* transform path of the trials: 1 cuFFT complex
+                             transform + fused unpack, 2 real transform (the
+                             reference's), 3 the library's own two-pass
+                             transform with the resample in its first pass */
 } psx_search_info;
 
 int psx_search_last_info(const psx_search* s, psx_search_info* info);
@@ -506,7 +515,8 @@ int psx_search_get_profile(psx_search* s, psx_search_profile* out, int reset);
 /* Debug tap: the dereddened series of the last call (N floats, scaled by
    N as the reference leaves it) and, for trial `trial` of the last call,
    its resampled series (N floats) and normalised interbinned spectrum
-   (N/2+1 floats), recomputed on the device.  Any pointer may be NULL. */
+   (N/2+1 floats), recomputed on the device through the instance's own
+   transform path (psx_search_info::fft_form).  Any pointer may be NULL. */
 int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
                          float* h_tim_r, float* h_pspec, float* h_norm2);
 

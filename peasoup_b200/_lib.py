@@ -69,7 +69,7 @@ class SearchInfo(C.Structure):
                 ("fft_launches", C.c_int), ("above_threshold", C.c_longlong),
                 ("fft_callback", C.c_int), ("graph", C.c_int), ("batch", C.c_int),
                 ("baseline_passes", C.c_int), ("harm_shape", C.c_int),
-                ("capture_fallbacks", C.c_int)]
+                ("capture_fallbacks", C.c_int), ("fft_form", C.c_int)]
 
 
 class SearchProfile(C.Structure):

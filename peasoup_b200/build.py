@@ -32,7 +32,8 @@ HOST_FLAGS = "-fPIC,-O2,-ffp-contract=off,-fno-fast-math"
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", HOST_FLAGS,
               f"-I{INCLUDE}", f"-I{CSRC}", f"-I{BUILD}"]
 
-CU_SOURCES = ["psx_kernels.cu", "psx_fft.cu", "psx_search.cu", "psx_tune.cu", "psx_dedisp.cu"]
+CU_SOURCES = ["psx_kernels.cu", "psx_fft.cu", "psx_fft4.cu", "psx_search.cu", "psx_tune.cu",
+              "psx_dedisp.cu"]
 CPP_SOURCES = ["psx_host.cpp", "psx_serve.cpp", "psx_output.cpp", "psx_sigproc.cpp"]
 
 

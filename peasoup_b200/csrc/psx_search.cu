@@ -35,6 +35,7 @@
 #include "psx_common.cuh"
 #include "psx_device.cuh"
 #include "psx_fft.cuh"
+#include "psx_fft4.cuh"
 #include "psx_harm.cuh"
 #include "psx_host.h"
 #include "psx_stages.cuh"
@@ -447,6 +448,8 @@ struct psx_search {
 
     Slot slot[2];
     FftPlan r2c1;                      // plain-mode trials and the debug tap
+    Fft4Plan f4;                       // the hand-written transform (fft_form 3)
+    bool use_f4 = false;
     cudaEvent_t call_start = nullptr;  // compute-stream position at a call's start
     std::map<int, FftPlan*> r2cb[2];  // batched plans per lane, by batch
     std::map<long long, GraphEntry> graphs;
@@ -524,8 +527,11 @@ struct psx_search {
 
     bool batched() const { return cfg.mode == PSX_MODE_BATCHED; }
     bool callback() const { return batched() && cfg.use_fft_callback; }
-    // batched trials through the complex transform + fused unpack kernel
-    bool fused_form() const { return batched() && !callback() && cfg.fft_form != 2; }
+    // batched trials through the hand-written two-pass transform (resample
+    // gather in its first pass) + the unpack kernel of its transposed output
+    bool fft4() const { return use_f4; }
+    // batched trials through cuFFT's complex transform + fused unpack kernel
+    bool fused_form() const { return batched() && !callback() && cfg.fft_form != 2 && !use_f4; }
 
     int get_plan(int b, FftPlan** out, int lane = 0);
     int grow_records(Slot& s, size_t need);
@@ -727,7 +733,16 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
         float* X = d_Xl[lane];
         float* pp = d_pl[lane];
         int b = 1;
-        if (batched()) {
+        if (fft4()) {
+            // resample gather + transform in two passes, the resample timed
+            // with the transform
+            b = batch;
+            while (b > nacc - t0) b >>= 1;
+            if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], ls));
+            PSX_TRY(f4.exec(s.d_tim, s.d_ktab + t0, b, reinterpret_cast<float2*>(tr), N / 2,
+                            reinterpret_cast<float2*>(X), Bp, ls));
+            s.launches += 2;
+        } else if (batched()) {
             b = batch;
             while (b > nacc - t0) b >>= 1;
             FftPlan* plan = nullptr;
@@ -751,7 +766,9 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
             ++s.ffts;
         }
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 1], ls));
-        if (fused_form()) {
+        if (fft4()) {
+            PSX_TRY(f4.form(reinterpret_cast<const float2*>(X), Bp, b, pp, Bp, s.d_stat, ls));
+        } else if (fused_form()) {
             const unsigned M = (unsigned)(N / 2);
             dim3 gu(grid_for(M / 8, T, 4), (unsigned)b);
             k_unpack_form_norm<<<gu, T, 0, ls>>>(X, Bp, pp, Bp, M, 1.0f / (float)M, tw_steps,
@@ -1151,8 +1168,14 @@ static int check_config(const psx_search_config* c)
         set_error("search: batch must be 0..1024");
         return PSX_ERR_INVALID;
     }
-    if (c->fft_form < 0 || c->fft_form > 2) {
-        set_error("search: fft_form must be 0..2");
+    if (c->fft_form < 0 || c->fft_form > 3) {
+        set_error("search: fft_form must be 0..3");
+        return PSX_ERR_INVALID;
+    }
+    if (c->fft_form == 3 && (c->mode != PSX_MODE_BATCHED || c->use_fft_callback ||
+                             !Fft4Plan::supported(c->fft_size))) {
+        set_error("search: fft_form 3 needs the batched mode without the cuFFT callback and "
+                  "fft_size a power of two from 2^19 to 2^25");
         return PSX_ERR_INVALID;
     }
     if (c->lanes < 0 || c->lanes > 2) {
@@ -1183,6 +1206,16 @@ static int effective_batch(const psx_search_config* c)
     return p;
 }
 
+// Transform path of the trials: 3 = the hand-written two-pass transform,
+// 1 = cuFFT's complex transform + the fused unpack kernel, 2 = the
+// reference's real transform (also plain mode and the cuFFT callback).
+static int effective_form(const psx_search_config* c)
+{
+    if (c->mode != PSX_MODE_BATCHED || c->use_fft_callback || c->fft_form == 2) return 2;
+    if (c->fft_form == 3 || (c->fft_form == 0 && Fft4Plan::supported(c->fft_size))) return 3;
+    return 1;
+}
+
 static int effective_lanes(const psx_search_config* c)
 {
     if (c->mode != PSX_MODE_BATCHED) return 1;
@@ -1208,6 +1241,7 @@ size_t psx_search_footprint(const psx_search_config* c)
     // cuFFT work areas: about one transform's worth per batched plan size and
     // lane, plus the batch-1 plans of the two slots' prologues and the plain path
     bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
+    if (effective_form(c) == 3) bytes += sizeof(float2) * (1024 + 66 * (N / 2048));  // twiddles
     return bytes;
 }
 
@@ -1234,6 +1268,7 @@ static void host_setup(psx_search* s, const psx_search_config* cfg)
     s->batch = effective_batch(cfg);
     s->lanes = effective_lanes(cfg);
     s->harm_shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
+    s->use_f4 = effective_form(cfg) == 3;
     {
         const double M = (double)(s->N / 2), pi = 3.14159265358979323846;
         for (int t = 0; t < 6; ++t)
@@ -1374,7 +1409,9 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     if (cudaEventCreateWithFlags(&s->call_start, cudaEventDisableTiming) != cudaSuccess)
         return fail(PSX_ERR_CUDA);
     if ((rc = s->r2c1.create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
-    if (s->batched()) {
+    if (s->fft4()) {
+        if ((rc = s->f4.create(N)) != PSX_OK) return fail(rc);
+    } else if (s->batched()) {
         FftPlan* p = nullptr;
         for (int l = 0; l < s->lanes; ++l)
             if ((rc = s->get_plan(s->batch, &p, l)) != PSX_OK) return fail(rc);
@@ -1384,6 +1421,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->info.batch = s->batch;
     s->info.harm_shape = s->harm_shape;
     s->info.fft_callback = cb ? 1 : 0;
+    s->info.fft_form = effective_form(cfg);
     *out = s;
     return PSX_OK;
 }
@@ -1471,9 +1509,9 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
         effective_batch(cfg) != s->batch || shape != s->harm_shape || cb != s->callback() ||
         effective_lanes(cfg) != s->lanes ||
-        (cfg->fft_form == 2) != (s->cfg.fft_form == 2)) {
-        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, callback and "
-                  "lanes must match the instance");
+        effective_form(cfg) != effective_form(&s->cfg)) {
+        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, callback, "
+                  "lanes and transform path must match the instance");
         return PSX_ERR_INVALID;
     }
     PSX_CUDA(cudaSetDevice(s->device));
@@ -1551,6 +1589,7 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
     s->info.batch = bp;
     s->info.fft_callback = cbk;
     s->info.harm_shape = s->harm_shape;
+    s->info.fft_form = effective_form(&s->cfg);
     s->info.graph = s->batched() && s->cfg.use_graph && !s->profile ? 1 : 0;
     std::vector<psx_candidate> all, out;
     std::vector<int> all_na, all_tr, all_dm, na, tr;
@@ -1630,7 +1669,27 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
         if (h_tim_r)
             PSX_CUDA(cudaMemcpyAsync(h_tim_r, s->d_tr, sizeof(float) * s->N,
                                      cudaMemcpyDeviceToHost, s->st));
-        if (h_pspec) {
+        if (h_pspec && s->fft4()) {
+            // the trials' own path: gather + two-pass transform + unpack
+            PSX_TRY(s->f4.exec(sl.d_tim, sl.d_ktab + trial, 1, reinterpret_cast<float2*>(s->d_tr),
+                               s->N / 2, reinterpret_cast<float2*>(s->d_X), s->Bp, s->st));
+            PSX_TRY(s->f4.form(reinterpret_cast<const float2*>(s->d_X), s->Bp, 1, s->d_p, s->Bp,
+                               sl.d_stat, s->st));
+            PSX_CUDA(cudaMemcpyAsync(h_pspec, s->d_p, sizeof(float) * s->B,
+                                     cudaMemcpyDeviceToHost, s->st));
+        } else if (h_pspec && s->fused_form()) {
+            // the trials' own path: complex transform + fused unpack
+            FftPlan* plan = nullptr;
+            PSX_TRY(s->get_plan(1, &plan, 0));
+            PSX_TRY(plan->exec(s->d_tr, s->d_X, s->st));
+            const unsigned M = (unsigned)(s->N / 2);
+            dim3 gu(grid_for(M / 8, 256, 4), 1);
+            k_unpack_form_norm<<<gu, 256, 0, s->st>>>(s->d_X, s->Bp, s->d_p, s->Bp, M,
+                                                      1.0f / (float)M, s->tw_steps, sl.d_stat);
+            PSX_TRY(launch_status("debug tap"));
+            PSX_CUDA(cudaMemcpyAsync(h_pspec, s->d_p, sizeof(float) * s->B,
+                                     cudaMemcpyDeviceToHost, s->st));
+        } else if (h_pspec) {
             PSX_TRY(s->r2c1.exec(s->d_tr, s->d_X, s->st));
             dim3 gf(grid_for(s->B / 2 + 1, 256, 4), 1);
             k_form_norm<<<gf, 256, 0, s->st>>>(s->d_X, 2 * s->Bp, s->d_p, s->Bp, (unsigned)s->B,

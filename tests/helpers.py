@@ -25,6 +25,18 @@ def err_vs_rms(a, b):
     return float(np.max(np.abs(a - b)) / scale) if a.size else 0.0
 
 
+def err_vs_mag_or_rms(a, b):
+    """max |a-b| / (|b| + RMS of b): relative where the values are large
+    (spectral peaks, whose own FP32 rounding sets the error there),
+    relative to the RMS elsewhere."""
+    a = _wide(a)
+    b = _wide(b)
+    if not a.size:
+        return 0.0
+    scale = np.sqrt(np.mean(np.abs(b) ** 2))
+    return float(np.max(np.abs(a - b) / (np.abs(b) + scale)))
+
+
 def cand_key(c):
     return (int(c["dm_idx"]), float(c["acc"]), int(c["nh"]), float(c["freq"]))
 

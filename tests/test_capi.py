@@ -52,6 +52,16 @@ def test_invalid_arguments_fail_loudly(psx):
     cfg.nharmonics = 6
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
     assert b"nharmonics" in psx.psx_last_error()
+    # the library's own transform: batched, no cuFFT callback, 2^19 .. 2^25 points
+    for n, mode, cb in ((1 << 16, _lib.PSX_MODE_BATCHED, 0), (3 << 18, _lib.PSX_MODE_BATCHED, 0),
+                        (1 << 26, _lib.PSX_MODE_BATCHED, 0), (1 << 20, _lib.PSX_MODE_PLAIN, 0),
+                        (1 << 20, _lib.PSX_MODE_BATCHED, 1)):
+        psx.psx_search_config_defaults(C.byref(cfg), n, 64e-6)
+        cfg.mode, cfg.use_fft_callback, cfg.fft_form = mode, cb, 3
+        assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
+        assert b"fft_form 3" in psx.psx_last_error()
+    cfg.fft_form = 4
+    assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
 
 
 def test_no_cpu_fallback_without_device(psx):

@@ -1,0 +1,96 @@
+"""The batched path's own transform (fft_form 3: the resample gather in the
+first of two passes of a four-step complex transform of the series read as
+interleaved pairs, then the unpack + interbin + normalise kernel):
+
+  * the normalised interbinned spectrum of tapped trials against FP64
+    (numpy's real transform of the same resampled series) within 1e-5
+    relative, |a - b| <= 1e-5 (|b| + RMS), at every row length the two
+    passes support;
+  * candidate lists identical to cuFFT's complex transform (fft_form 1) and
+    to the reference's real transform (plain mode), S/N within 1e-5.
+"""
+import numpy as np
+import pytest
+
+from helpers import err_vs_mag_or_rms, match_candidates
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def S(cuda, psx):
+    from peasoup_b200 import search, synth
+    return search, synth
+
+
+def _params(S, n, tsamp, **kw):
+    search, synth = S
+    p = dict(fft_size=n, tsamp=tsamp, cfreq_hz=synth.CFREQ_HZ, ch_bw_hz=synth.CH_BW_HZ)
+    p.update(kw)
+    return search.SearchParams(**p)
+
+
+def _fp64_spectrum(tim, idx, norm2):
+    """Interbinned, normalised spectrum of tim[idx] in FP64 (the reference's
+    forming and normalising steps, src/kernels.cu:238-259 and :496-507)."""
+    x = tim[idx.astype(np.int64)].astype(np.float64)
+    X = np.fft.rfft(x)
+    prev = np.concatenate([[0j], X[:-1]])
+    amp = np.sqrt(np.maximum(np.abs(X) ** 2, 0.5 * np.abs(X - prev) ** 2))
+    return (amp - float(norm2[0])) / float(norm2[1])
+
+
+@pytest.mark.parametrize("logn", [19, 20, 21, 22, 23, 24, 25])
+def test_spectrum_vs_fp64(S, oracle, logn):
+    search, synth = S
+    n, ts = 1 << logn, 64e-6
+    x = synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(4.1e-3, 35.0, 0.04, 0.5)]), logn)
+    s = search.AccelSearch(_params(S, n, ts, batch=4, acc_lo=-40.0, acc_hi=40.0,
+                                   nharmonics=2, min_snr=9.0))
+    s.search(x, 0.0, 0, per_dm=False)
+    assert s.info()["fft_form"] == 3
+    from peasoup_b200.transforms import AccelerationPlan
+    accs = AccelerationPlan(-40.0, 40.0, 1.10, 64e-6, n, ts, synth.CFREQ_HZ,
+                            synth.CH_BW_HZ).generate_accel_list(0.0, 0.0)
+    for t in sorted({0, len(accs) // 2, len(accs) - 1}):
+        tim, tr, ps, norm2 = s.debug_tap(t)
+        idx = oracle.resampleII_index(n, float(accs[t]), ts)
+        want = _fp64_spectrum(tim, idx, norm2)
+        err = err_vs_mag_or_rms(ps, want)
+        assert err < 1e-5, (logn, t, err)
+    s.close()
+
+
+@pytest.mark.parametrize("n", [1 << 20, 1 << 22])
+def test_candidates_match_cufft_paths(S, n):
+    search, synth = S
+    ts = 64e-6
+    x = synth.make_series_np(synth.SeriesSpec(
+        nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(3.3e-3, -25.0, 0.05, 0.4),
+                                     synth.Pulsar(0.21, 4.0, 0.03, 0.6)]), 7)
+    kw = dict(acc_lo=-60.0, acc_hi=60.0, nharmonics=4, min_snr=6.5)
+    outs = {}
+    for name, mode, form in (("own", "batched", 3), ("cufft", "batched", 1),
+                             ("plain", "plain", 0)):
+        s = search.AccelSearch(_params(S, n, ts, mode=mode, fft_form=form, batch=8, **kw))
+        outs[name] = s.search(x, 2.0, 5, per_dm=False)[0]
+        if mode == "batched":
+            assert s.info()["fft_form"] == form
+        s.close()
+    assert len(outs["own"]) > 3
+    for other in ("cufft", "plain"):
+        nm, ua, ub, worst = match_candidates(outs["own"], outs[other], 6.5, margin=1e-4)
+        assert not ua and not ub and worst < 1e-5, (other, ua[:3], ub[:3], worst)
+
+
+def test_default_form_by_size(S):
+    search, synth = S
+    ts = 64e-6
+    for n, want in ((1 << 16, 1), (3 << 18, 1), (1 << 19, 3)):
+        s = search.AccelSearch(_params(S, n, ts, batch=2, acc_lo=-1.0, acc_hi=1.0,
+                                       nharmonics=1, min_snr=9.0))
+        s.search(synth.make_series_np(synth.SeriesSpec(nsamps=n, tsamp=ts), 2), 0.0, 0,
+                 per_dm=False)
+        assert s.info()["fft_form"] == want, n
+        s.close()
