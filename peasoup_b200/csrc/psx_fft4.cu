@@ -9,19 +9,20 @@
 // ffter.hpp:23-53) and the spectrum forming and normalising kernels
 // (src/kernels.cu:238-259, :496-507) with three launches:
 //   pass 1 (k_fft4_cols): CTA = 8 columns c of the 1024 x C matrix
-//     z[r * C + c]; each thread gathers 32 rows of its column straight from
-//     the dereddened series through the resample index (FP64, the same
-//     device function the resample kernel uses), a radix-32 Stockham stage
-//     in registers, one exchange through shared memory, the second radix-32
-//     stage, the four-step twiddle W_M^(c k1), then y[k1 * C + c];
+//     z[r * C + c], 512 threads; each thread gathers 16 rows of its column
+//     straight from the dereddened series through the resample index (FP64,
+//     the same device function the resample kernel uses), then Stockham
+//     stages of radix 16, 16 and 4 in registers with two exchanges through
+//     shared memory, the four-step twiddle W_M^(c k1), then y[k1 * C + c];
 //   pass 2 (k_fft4_rows): CTA = one row k1 (or 256/(C/16) rows) of y,
 //     radix-16 Stockham stages (one radix 2/4/8 stage where C is not a
 //     power of 16) through padded shared memory, written in natural order
 //     as zt[k1 * C + k2] = Z[k1 + 1024 k2];
-//   unpack (k_unpack_form_norm_t): lanes take consecutive k1 (30 output
-//     lanes and two helpers per warp), so the neighbour bin k-1 each
-//     interbinned value needs is the previous lane's, and the mirror bin
-//     M-k the next lane's.
+//   unpack (k_unpack_form_norm_t): a CTA stages a 32-row x 32-column tile of
+//     zt and the tile of its mirror bins through shared memory with
+//     coalesced loads; then lanes take consecutive k1 (30 output lanes and
+//     two helpers per warp), so the neighbour bin k-1 each interbinned value
+//     needs is the previous lane's, and the mirror bin M-k the next lane's.
 // All twiddles come from tables rounded once from double precision.
 #include <cuda_runtime.h>
 #include <cmath>
@@ -123,52 +124,75 @@ __device__ __forceinline__ void dft(float2 (&v)[L])
 }
 
 // ------------------------------------------------------------- pass 1
-// Shared layout [e][col], e the row index 0..1023; with 8 columns a row is
-// 64 bytes, and flipping bit 0 of e by bit 5 puts the four rows a warp
-// touches at once two in each half of the banks.
-template <int W>
-__device__ __forceinline__ unsigned swz_a(unsigned e)
-{
-    return W == 16 ? e : (e ^ ((e >> 5) & 1u));
-}
+// Shared layout [e][col], e the row index 0..1023; a row of 8 columns is 64
+// bytes.  Flipping bit 0 of e by bit 4 spreads the four rows a warp touches
+// at once (four consecutive t) two to each half of the banks in every
+// exchange below.
+__device__ __forceinline__ unsigned swz_a(unsigned e) { return e ^ ((e >> 4) & 1u); }
 
-template <int W>
-__global__ void __launch_bounds__(W * 32, 2)
+__global__ void __launch_bounds__(kColsW * 64, 2)
     k_fft4_cols(const float* __restrict__ x, unsigned long long n, const double* __restrict__ ktab,
-                const float2* __restrict__ tab, unsigned offA, unsigned offQ, unsigned offP,
-                unsigned C, float2* __restrict__ y, size_t ypitch)
+                const float2* __restrict__ tab, unsigned offA2, unsigned offA3, unsigned offQ,
+                unsigned offP, unsigned C, float2* __restrict__ y, size_t ypitch)
 {
+    constexpr int W = kColsW;
     extern __shared__ float2 sm_a[];
-    const unsigned col = threadIdx.x % W, j = threadIdx.x / W;  // j in [0, 32)
+    const unsigned col = threadIdx.x % W, t = threadIdx.x / W;  // t in [0, 64)
     const unsigned c = blockIdx.x * W + col;
     const double k = ktab[blockIdx.y], size = (double)n;
-    float2 v[32];
-    // rows e = j + 32 q of column c: z[e C + c] = (x'[2m], x'[2m+1])
+    float2 v[16];
+    // stage 1 (radix 16, span 1): rows e = t + 64 q of column c, where
+    // z[e C + c] = (x'[2m], x'[2m+1]); out[16 t + q]
 #pragma unroll
-    for (int q = 0; q < 32; ++q) {
-        const unsigned long long i0 = 2ull * ((unsigned long long)(j + 32 * q) * C + c);
+    for (int q = 0; q < 16; ++q) {
+        const unsigned long long i0 = 2ull * ((unsigned long long)(t + 64 * q) * C + c);
         v[q].x = gather_at(x, resampleII_index(i0, k, size), n);
         v[q].y = gather_at(x, resampleII_index(i0 + 1, k, size), n);
     }
-    // Stockham radix 32, span 1: out[32 j + q]
-    dft<32>(v);
+    dft<16>(v);
 #pragma unroll
-    for (int q = 0; q < 32; ++q) sm_a[swz_a<W>(32 * j + q) * W + col] = v[q];
+    for (int q = 0; q < 16; ++q) sm_a[swz_a(16 * t + q) * W + col] = v[q];
     __syncthreads();
-    // span 32: in[j + 32 q] * W_1024^(j q), out[j + 32 q] = row k1 of the column DFT
+    // stage 2 (radix 16, span 16): in[t + 64 q] * W_256^((t mod 16) q),
+    // out[(t / 16) 256 + t mod 16 + 16 q]
 #pragma unroll
-    for (int q = 0; q < 32; ++q) v[q] = sm_a[swz_a<W>(j + 32 * q) * W + col];
+    for (int q = 0; q < 16; ++q) v[q] = sm_a[swz_a(t + 64 * q) * W + col];
+    __syncthreads();
 #pragma unroll
-    for (int q = 1; q < 32; ++q) v[q] = cmul(v[q], __ldg(tab + offA + q * 32 + j));
-    dft<32>(v);
-    // four-step twiddle W_M^(c k1), k1 = j + 32 q: W_M^(c j) * W_M^(32 c q)
-    const float2 wq = __ldg(tab + offQ + (size_t)j * C + c);
+    for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], __ldg(tab + offA2 + q * 16 + (t & 15)));
+    dft<16>(v);
+    const unsigned base2 = (t >> 4) * 256 + (t & 15);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) sm_a[swz_a(base2 + 16 * q) * W + col] = v[q];
+    __syncthreads();
+    // stage 3 (radix 4, span 256): butterflies j = t + 64 u, in[j + 256 q]
+    // * W_1024^(j q), out[j + 256 q] = row k1 = t + 64 (u + 4 q)
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[4 * u + q] = sm_a[swz_a(t + 64 * u + 256 * q) * W + col];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        float2 b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            b[q] = q ? cmul(v[4 * u + q], __ldg(tab + offA3 + q * 256 + t + 64 * u)) : v[4 * u];
+        dft<4>(b);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[4 * u + q] = b[q];
+    }
+    // four-step twiddle W_M^(c k1), k1 = t + 64 w (w = u + 4 q):
+    // W_M^(c t) * W_M^(64 c w)
+    const float2 wt = __ldg(tab + offQ + (size_t)t * C + c);
     float2* yo = y + (size_t)blockIdx.y * ypitch;
 #pragma unroll
-    for (int q = 0; q < 32; ++q) {
-        const float2 w = q ? cmul(wq, __ldg(tab + offP + (size_t)q * C + c)) : wq;
-        yo[(size_t)(j + 32 * q) * C + c] = cmul(v[q], w);
-    }
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const unsigned w = u + 4 * q;
+            const float2 tw = w ? cmul(wt, __ldg(tab + offP + (size_t)w * C + c)) : wt;
+            yo[(size_t)(t + 64 * w) * C + c] = cmul(v[4 * u + q], tw);
+        }
 }
 
 // ------------------------------------------------------------- pass 2
@@ -214,7 +238,7 @@ __device__ __forceinline__ void row_stage(float2* s, unsigned t, const float2* _
 }
 
 template <int LOGC>
-__global__ void __launch_bounds__(RowShape<LOGC>::THREADS)
+__global__ void __launch_bounds__(RowShape<LOGC>::THREADS, 1024 / RowShape<LOGC>::THREADS)
     k_fft4_rows(const float2* __restrict__ y, size_t ypitch, float2* __restrict__ zt,
                 size_t zpitch, const float2* __restrict__ tw)
 {
@@ -248,10 +272,6 @@ __global__ void __launch_bounds__(RowShape<LOGC>::THREADS)
 }
 
 // ------------------------------------------------------------- unpack
-struct UnpackSteps {
-    float2 w[4];
-};
-
 __device__ __forceinline__ float2 zt_at(const float2* __restrict__ z, unsigned C, unsigned idx)
 {
     return z[(size_t)(idx & (kFft4Rows - 1)) * C + (idx >> 10)];
@@ -269,77 +289,76 @@ __device__ __forceinline__ void unpack_one(float2 a, float2 w, float cs, float s
     hi = make_float2(0.5f * (ar - u), 0.5f * (-ai - v));
 }
 
-// Grid (ceil(1024/30) * C/64, trials), 256 threads.  Warp (wk, g): lanes
-// take rows k1 = 30 wk - 1 + lane ("virtual" rows -1 and >= 1024 continue
-// into the neighbouring columns), columns k2 = 4g .. 4g+3 < C/2, i.e. the
-// bins j = k1 + 1024 k2 < M/2 and their mirrors M - j.  Lanes 1..30 write
-// bin j (interbinned with lane-1's X[j-1]) and bin M-j (with lane+1's
-// X[M-j-1]); bin M/2 comes from thread 0 of block 0.
+// Grid (ceil(1024/30) * C/64, trials), 256 threads.  CTA (wk, g): rows
+// k1 = 30 wk - 1 + r, r < 32 ("virtual" rows -1 and >= 1024 continue into
+// the neighbouring columns), columns k2 = 32 g .. 32 g + 31 < C/2: the bins
+// j = k1 + 1024 k2 < M/2 and their mirrors M - j.  Both 32 x 32 tiles are
+// loaded coalesced (a warp reads 32 consecutive columns of a row) into
+// padded shared memory; warp w then takes columns 32 g + 4 w .. + 3 with
+// lane = r, and lanes 1..30 write bin j (interbinned with lane-1's X[j-1])
+// and bin M-j (with lane+1's X[M-j-1]); bin M/2 comes from thread 0 of
+// block 0.  The split-step rotation (cos, sin)(pi j / M) is the product of
+// tabulated (cos, sin)(pi k1 / M) (k1 = -1 .. 1055, rv[k1 + 1]) and
+// (cos, sin)(pi k2 / C) (rk[k2]).
 __global__ void __launch_bounds__(256)
     k_unpack_form_norm_t(const float2* __restrict__ zt, size_t zpitch, unsigned C,
-                         float* __restrict__ p, size_t ppitch, float inv_m, UnpackSteps st,
+                         float* __restrict__ p, size_t ppitch, float inv_m,
+                         const float2* __restrict__ rv, const float2* __restrict__ rk,
                          const float* __restrict__ stat)
 {
     constexpr unsigned R = kFft4Rows;
+    __shared__ float2 lo_t[32][33], mi_t[32][33];
     const unsigned M = R * C;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned gblocks = C / 64;
     const unsigned wk = blockIdx.x / gblocks;
-    const unsigned g = (blockIdx.x % gblocks) * 8 + warp;
-    const int k1v = (int)(30 * wk + lane) - 1;
-    const unsigned k20 = 4 * g;
+    const unsigned k2a = (blockIdx.x % gblocks) * 32;
+    const int v0 = (int)(30 * wk) - 1;
     const float2* z = zt + (size_t)blockIdx.y * zpitch;
     float* o = p + (size_t)blockIdx.y * ppitch;
-    float2 a[4], w[4];
-    if (k1v >= 1 && k1v < (int)R) {
-        const float4* r4 = reinterpret_cast<const float4*>(z + (size_t)k1v * C + k20);
-        const float4 a01 = r4[0], a23 = r4[1];
-        // Z[M - j] = zt[(R - k1)][C - 1 - k2]: the group C-4-k20 .. C-1-k20, reversed
-        const float4* m4 =
-            reinterpret_cast<const float4*>(z + (size_t)(R - k1v) * C + (C - 4 - k20));
-        const float4 m01 = m4[0], m23 = m4[1];
-        a[0] = make_float2(a01.x, a01.y);
-        a[1] = make_float2(a01.z, a01.w);
-        a[2] = make_float2(a23.x, a23.y);
-        a[3] = make_float2(a23.z, a23.w);
-        w[3] = make_float2(m01.x, m01.y);
-        w[2] = make_float2(m01.z, m01.w);
-        w[1] = make_float2(m23.x, m23.y);
-        w[0] = make_float2(m23.z, m23.w);
-    } else {
+    if (v0 >= 1 && v0 + 31 < (int)R) {  // every row a real row: direct addresses
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const long long j = (long long)k1v + (long long)R * (k20 + t);
-            if (j < 0) {
-                a[t] = w[t] = make_float2(0.f, 0.f);  // X[-1] := 0
-            } else {
-                const unsigned jj = (unsigned)j;
-                a[t] = zt_at(z, C, jj);
-                w[t] = zt_at(z, C, jj ? M - jj : 0u);
-            }
+        for (int e = 0; e < 4; ++e) {
+            const unsigned r = warp + 8 * e;  // tile row; lane = tile column
+            const unsigned v = (unsigned)v0 + r;
+            lo_t[r][lane] = z[(size_t)v * C + k2a + lane];
+            mi_t[r][lane] = z[(size_t)(R - v) * C + (C - 1 - k2a - lane)];
         }
-    }
-    float s0, c0;
-    sincospif((float)((long long)k1v + (long long)R * k20) * inv_m, &s0, &c0);
-    float2 lo[4], hi[4];
+    } else
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const float2 d = st.w[t];  // angle of column k20 + t = angle(k20) + pi t / C
-        const float cs = t ? c0 * d.x - s0 * d.y : c0, sn = t ? s0 * d.x + c0 * d.y : s0;
-        unpack_one(a[t], w[t], cs, sn, lo[t], hi[t]);
+    for (int e = 0; e < 4; ++e) {
+        const unsigned r = warp + 8 * e;  // tile row; lane = tile column
+        const long long j = (long long)(v0 + (int)r) + (long long)R * (k2a + lane);
+        float2 a = make_float2(0.f, 0.f), w = a;  // X[-1] := 0
+        if (j >= 0) {
+            const unsigned jj = (unsigned)j;
+            a = zt_at(z, C, jj);
+            w = zt_at(z, C, jj ? M - jj : 0u);
+        }
+        lo_t[r][lane] = a;
+        mi_t[r][lane] = w;
     }
+    __syncthreads();
+    const int k1v = v0 + (int)lane;
+    const float2 tv = __ldg(rv + (k1v + 1));
     const float meanN = stat[3], stdN = stat[4];
     const bool out = lane >= 1 && lane <= 30 && k1v < (int)R;
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        const float plx = __shfl_up_sync(0xffffffffu, lo[t].x, 1);
-        const float ply = __shfl_up_sync(0xffffffffu, lo[t].y, 1);
-        const float nhx = __shfl_down_sync(0xffffffffu, hi[t].x, 1);
-        const float nhy = __shfl_down_sync(0xffffffffu, hi[t].y, 1);
+        const unsigned cc = 4 * warp + t, k2 = k2a + cc;
+        const float2 tk = __ldg(rk + k2);
+        const float cs = tv.x * tk.x - tv.y * tk.y, sn = tv.y * tk.x + tv.x * tk.y;
+        float2 lo, hi;
+        unpack_one(lo_t[lane][cc], mi_t[lane][cc], cs, sn, lo, hi);
+        if (k1v < 0 && k2 == 0) lo = hi = make_float2(0.f, 0.f);
+        const float plx = __shfl_up_sync(0xffffffffu, lo.x, 1);
+        const float ply = __shfl_up_sync(0xffffffffu, lo.y, 1);
+        const float nhx = __shfl_down_sync(0xffffffffu, hi.x, 1);
+        const float nhy = __shfl_down_sync(0xffffffffu, hi.y, 1);
         if (out) {
-            const unsigned j = (unsigned)k1v + R * (k20 + t);
-            o[j] = normalise(interbin(lo[t].x, lo[t].y, plx, ply), meanN, stdN);
-            o[M - j] = normalise(interbin(hi[t].x, hi[t].y, nhx, nhy), meanN, stdN);
+            const unsigned j = (unsigned)k1v + R * k2;
+            o[j] = normalise(interbin(lo.x, lo.y, plx, ply), meanN, stdN);
+            o[M - j] = normalise(interbin(hi.x, hi.y, nhx, nhy), meanN, stdN);
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // bin M/2 with bin M/2 - 1
@@ -422,16 +441,28 @@ int Fft4Plan::create(size_t n_)
         return make_float2((float)std::cos(a), (float)-std::sin(a));
     };
     std::vector<float2> h;
-    h.reserve(1024 + 66 * (size_t)Cn);
-    offA = 0;  // [q * 32 + j] = W_1024^(j q)
-    for (unsigned q = 0; q < 32; ++q)
-        for (unsigned j = 0; j < 32; ++j) h.push_back(W((unsigned long long)j * q, 1024));
-    offQ = (unsigned)h.size();  // [j * C + c] = W_M^(c j)
-    for (unsigned j = 0; j < 32; ++j)
-        for (unsigned c = 0; c < Cn; ++c) h.push_back(W((unsigned long long)c * j, M));
-    offP = (unsigned)h.size();  // [q * C + c] = W_M^(32 c q)
-    for (unsigned q = 0; q < 32; ++q)
-        for (unsigned c = 0; c < Cn; ++c) h.push_back(W(32ull * c * q, M));
+    h.reserve(2400 + 82 * (size_t)Cn);
+    offA2 = 0;  // [q * 16 + m] = W_256^(m q)
+    for (unsigned q = 0; q < 16; ++q)
+        for (unsigned m = 0; m < 16; ++m) h.push_back(W((unsigned long long)m * q, 256));
+    offA3 = (unsigned)h.size();  // [q * 256 + j] = W_1024^(j q)
+    for (unsigned q = 0; q < 4; ++q)
+        for (unsigned j = 0; j < 256; ++j) h.push_back(W((unsigned long long)j * q, 1024));
+    offQ = (unsigned)h.size();  // [t * C + c] = W_M^(c t)
+    for (unsigned t = 0; t < 64; ++t)
+        for (unsigned c = 0; c < Cn; ++c) h.push_back(W((unsigned long long)c * t, M));
+    offP = (unsigned)h.size();  // [w * C + c] = W_M^(64 c w)
+    for (unsigned w = 0; w < 16; ++w)
+        for (unsigned c = 0; c < Cn; ++c) h.push_back(W(64ull * c * w, M));
+    // unpack rotations (cos, sin)(pi k1 / M), k1 = -1 .. 1055, and (pi k2 / C)
+    const double pi = two_pi / 2;
+    offRv = (unsigned)h.size();
+    for (int k1 = -1; k1 <= 1055; ++k1)
+        h.push_back(make_float2((float)std::cos(pi * k1 / (double)M),
+                                (float)std::sin(pi * k1 / (double)M)));
+    offRk = (unsigned)h.size();
+    for (unsigned k2 = 0; k2 < Cn / 2; ++k2)
+        h.push_back(make_float2((float)std::cos(pi * k2 / Cn), (float)std::sin(pi * k2 / Cn)));
     offB = (unsigned)h.size();  // row-pass stages: [q * NS + m] = W_(R NS)^(q m)
     int lc = 0;
     while ((1u << lc) < Cn) ++lc;
@@ -444,16 +475,17 @@ int Fft4Plan::create(size_t n_)
     PSX_CUDA(cudaMalloc(&d_tab, sizeof(float2) * h.size()));
     tab_len = h.size();
     PSX_CUDA(cudaMemcpy(d_tab, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
-    const double pi = two_pi / 2;
-    for (int t = 0; t < 4; ++t)
-        steps[t] = make_float2((float)std::cos(pi * t / Cn), (float)std::sin(pi * t / Cn));
     n = n_;
     C = Cn;
     logc = lc;
-    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<kColsW>,
+    // (the default shared/L1 split: measured on B200, forcing the largest
+    // shared carve-out slowed the gather of pass 1 and the twiddle reads of
+    // pass 2, both served from L1)
+    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(kFft4Rows * kColsW * sizeof(float2))),
                         "fft4 column pass attribute"));
+
     switch (logc) {
     case 8: return configure_rows<8>();
     case 9: return configure_rows<9>();
@@ -477,8 +509,8 @@ int Fft4Plan::exec(const float* series, const double* ktab, int ntrials, float2*
         return PSX_ERR_INVALID;
     }
     dim3 ga(C / kColsW, (unsigned)ntrials);
-    k_fft4_cols<kColsW><<<ga, kColsW * 32, kFft4Rows * kColsW * sizeof(float2), s>>>(
-        series, (unsigned long long)n, ktab, d_tab, offA, offQ, offP, C, y, ypitch);
+    k_fft4_cols<<<ga, kColsW * 64, kFft4Rows * kColsW * sizeof(float2), s>>>(
+        series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
     PSX_TRY(launch_status("fft4 column pass"));
     const float2* tw = d_tab + offB;
     switch (logc) {
@@ -503,12 +535,11 @@ int Fft4Plan::form(const float2* zt, size_t zpitch, int ntrials, float* p, size_
         set_error("fft4 form: bad arguments");
         return PSX_ERR_INVALID;
     }
-    UnpackSteps st;
-    for (int t = 0; t < 4; ++t) st.w[t] = steps[t];
     const unsigned nck = (kFft4Rows + 29) / 30;
     dim3 grid(nck * (C / 64), (unsigned)ntrials);
     const float inv_m = 1.0f / (float)(n / 2);
-    k_unpack_form_norm_t<<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, inv_m, st, stat);
+    k_unpack_form_norm_t<<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, inv_m, d_tab + offRv,
+                                              d_tab + offRk, stat);
     return launch_status("fft4 unpack kernel");
 }
 

@@ -19,8 +19,7 @@ struct Fft4Plan {
     int logc = 0;
     float2* d_tab = nullptr;  // twiddle tables (offsets below, in float2)
     size_t tab_len = 0;
-    unsigned offA = 0, offQ = 0, offP = 0, offB = 0;
-    float2 steps[4] = {};     // (cos, sin)(pi t / C), t = 0..3, for the unpack
+    unsigned offA2 = 0, offA3 = 0, offQ = 0, offP = 0, offB = 0, offRv = 0, offRk = 0;
 
     // N = 2^19 .. 2^25 (C = 2^8 .. 2^14).
     static bool supported(size_t n);

@@ -1241,7 +1241,7 @@ size_t psx_search_footprint(const psx_search_config* c)
     // cuFFT work areas: about one transform's worth per batched plan size and
     // lane, plus the batch-1 plans of the two slots' prologues and the plain path
     bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
-    if (effective_form(c) == 3) bytes += sizeof(float2) * (1024 + 66 * (N / 2048));  // twiddles
+    if (effective_form(c) == 3) bytes += sizeof(float2) * (2400 + 82 * (N / 2048));  // twiddles
     return bytes;
 }
 
