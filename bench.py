@@ -754,6 +754,16 @@ def run_psx(args, ws, rank, local):
         "form": 8.0 * B + 4.0 * B,        # read the spectrum, write the amplitudes
         "harm": 4.0 * B,                  # read the normalised spectrum once
     }
+    stage_kernels = {"resample": "k_resample", "fft": "cuFFT", "form": "k_unpack_form_norm",
+                     "harm": "k_harm_tiles"}
+    if form_used == 3:
+        # the two-pass transform: pass 1 (timed as "resample") gathers the
+        # series (4N bytes) and writes the column transforms (M complex =
+        # 4N bytes); pass 2 reads them and writes the spectrum (4N + 4N)
+        per_trial_bytes["resample"] = 8.0 * N_FFT
+        per_trial_bytes["fft"] = 8.0 * N_FFT
+        stage_kernels.update(resample="k_fft4_cols (gather + column transforms)",
+                             fft="k_fft4_rows (row transforms)", form="k_unpack_form_norm_t")
     stage_ms = {"resample": prof["resample_ms"], "fft": prof["fft_ms"],
                 "form": prof["form_ms"], "harm": prof["harm_ms"]}
     trials_prof = max(1, prof["trials"])
@@ -761,14 +771,16 @@ def run_psx(args, ws, rank, local):
     traffic = None
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dom)
+        tj = json.load(open(tp))
+        traffic = (tj.get("two_pass", {}) if form_used == 3 else tj).get(dom)
     stages = {}
     for k, ms in stage_ms.items():
         sec = ms / 1e3 / trials_prof
-        stages[k] = {"us_per_trial": sec * 1e6,
+        stages[k] = {"us_per_trial": sec * 1e6, "kernel": stage_kernels[k],
                      "gbs": per_trial_bytes[k] / sec / 1e9 if sec > 0 else None}
     achieved = stages[dom]["gbs"]
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+    roofline = {"bound": "hbm", "kernel": stage_kernels[dom], "stage": dom,
+                "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak if achieved else None,
                 "traffic": traffic, "peak_kind": peak_kind,
                 "bytes_per_trial": per_trial_bytes[dom], "stages": stages,

@@ -498,8 +498,9 @@ int psx_search_last_info(const psx_search* s, psx_search_info* info);
    stream around every launch group (when enabled). */
 typedef struct {
     double prologue_ms;   /* per-DM prologue */
-    double resample_ms;   /* resample gathers */
-    double fft_ms;        /* trial R2C transforms */
+    double resample_ms;   /* resample gathers (fft_form 3: the first pass of
+                             the two-pass transform, which does the gather) */
+    double fft_ms;        /* trial transforms (fft_form 3: the second pass) */
     double form_ms;       /* interbin + normalise */
     double harm_ms;       /* harmonic sums + threshold + compaction */
     long long groups;     /* launch groups timed */

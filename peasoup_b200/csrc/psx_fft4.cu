@@ -503,15 +503,31 @@ int Fft4Plan::create(size_t n_)
 int Fft4Plan::exec(const float* series, const double* ktab, int ntrials, float2* y,
                    size_t ypitch, float2* zt, size_t zpitch, cudaStream_t s) const
 {
-    if (!d_tab || !series || !ktab || !y || !zt || ntrials <= 0 || ntrials > 65535 ||
-        ypitch < n / 2 || zpitch < n / 2) {
+    PSX_TRY(exec_cols(series, ktab, ntrials, y, ypitch, s));
+    return exec_rows(y, ypitch, ntrials, zt, zpitch, s);
+}
+
+int Fft4Plan::exec_cols(const float* series, const double* ktab, int ntrials, float2* y,
+                        size_t ypitch, cudaStream_t s) const
+{
+    if (!d_tab || !series || !ktab || !y || ntrials <= 0 || ntrials > 65535 || ypitch < n / 2) {
         set_error("fft4: bad arguments");
         return PSX_ERR_INVALID;
     }
     dim3 ga(C / kColsW, (unsigned)ntrials);
     k_fft4_cols<<<ga, kColsW * 64, kFft4Rows * kColsW * sizeof(float2), s>>>(
         series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
-    PSX_TRY(launch_status("fft4 column pass"));
+    return launch_status("fft4 column pass");
+}
+
+int Fft4Plan::exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt, size_t zpitch,
+                        cudaStream_t s) const
+{
+    if (!d_tab || !y || !zt || ntrials <= 0 || ntrials > 65535 || ypitch < n / 2 ||
+        zpitch < n / 2) {
+        set_error("fft4: bad arguments");
+        return PSX_ERR_INVALID;
+    }
     const float2* tw = d_tab + offB;
     switch (logc) {
     case 8: return launch_rows<8>(y, ypitch, zt, zpitch, tw, ntrials, s);

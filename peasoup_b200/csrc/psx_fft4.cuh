@@ -34,6 +34,12 @@ struct Fft4Plan {
     // y (ypitch complex elements per trial, >= M) holds the intermediate.
     int exec(const float* series, const double* ktab, int ntrials, float2* y, size_t ypitch,
              float2* zt, size_t zpitch, cudaStream_t s) const;
+    // The two passes of exec on their own (pass 1: gather + column
+    // transforms into y; pass 2: row transforms of y into zt).
+    int exec_cols(const float* series, const double* ktab, int ntrials, float2* y,
+                  size_t ypitch, cudaStream_t s) const;
+    int exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt, size_t zpitch,
+                  cudaStream_t s) const;
 
     // Real spectrum bins 0..M of each trial from zt, interbinned and
     // normalised with stat[3] (mean*N) and stat[4] (std*N), written at

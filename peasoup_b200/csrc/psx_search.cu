@@ -734,13 +734,15 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
         float* pp = d_pl[lane];
         int b = 1;
         if (fft4()) {
-            // resample gather + transform in two passes, the resample timed
-            // with the transform
+            // resample gather + transform in two passes; the profile times
+            // the first pass (which does the gather) as the resample stage
             b = batch;
             while (b > nacc - t0) b >>= 1;
+            PSX_TRY(f4.exec_cols(s.d_tim, s.d_ktab + t0, b, reinterpret_cast<float2*>(tr), N / 2,
+                                 ls));
             if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], ls));
-            PSX_TRY(f4.exec(s.d_tim, s.d_ktab + t0, b, reinterpret_cast<float2*>(tr), N / 2,
-                            reinterpret_cast<float2*>(X), Bp, ls));
+            PSX_TRY(f4.exec_rows(reinterpret_cast<const float2*>(tr), N / 2, b,
+                                 reinterpret_cast<float2*>(X), Bp, ls));
             s.launches += 2;
         } else if (batched()) {
             b = batch;
