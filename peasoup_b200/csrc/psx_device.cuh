@@ -31,6 +31,18 @@ __device__ __forceinline__ float gather_at(const float* __restrict__ in,
     return idx < n ? in[idx] : 0.0f;
 }
 
+// resampleII read with the output index i given as an exact double and
+// n < 2^32: the expression of resampleII_index, rounded by the same mode to
+// a 32-bit index (both conversions clamp, so indices outside [0, n) read
+// zero in both forms).  The resample kernel and the gather of the two-pass
+// transform both read through this.
+__device__ __forceinline__ float resampleII_read(const float* __restrict__ in, double i, double k,
+                                                 double size, unsigned n)
+{
+    const unsigned idx = __double2uint_rn(i + i * k * (i - size));
+    return idx < n ? in[idx] : 0.0f;
+}
+
 // Read index of the centred resampler: k*((i-N/2)^2 - (N/2)^2).
 __device__ __forceinline__ unsigned long long resample_index(
     unsigned long long i, double k, double size_by_2)

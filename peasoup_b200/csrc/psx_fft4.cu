@@ -11,7 +11,7 @@
 //   pass 1 (k_fft4_cols): CTA = 8 columns c of the 1024 x C matrix
 //     z[r * C + c], 512 threads; each thread gathers 16 rows of its column
 //     straight from the dereddened series through the resample index (FP64,
-//     the same device function the resample kernel uses), then Stockham
+//     the same device function the resample kernel reads through), then Stockham
 //     stages of radix 16, 16 and 4 in registers with two exchanges through
 //     shared memory, the four-step twiddle W_M^(c k1), then y[k1 * C + c];
 //   pass 2 (k_fft4_rows): CTA = one row k1 (or 256/(C/16) rows) of y,
@@ -143,11 +143,14 @@ __global__ void __launch_bounds__(kColsW * 64, 2)
     float2 v[16];
     // stage 1 (radix 16, span 1): rows e = t + 64 q of column c, where
     // z[e C + c] = (x'[2m], x'[2m+1]); out[16 t + q]
+    const double i_first = 2.0 * ((double)t * (double)C + (double)c);
+    const double i_step = 128.0 * (double)C;
+    const unsigned n32 = (unsigned)n;
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-        const unsigned long long i0 = 2ull * ((unsigned long long)(t + 64 * q) * C + c);
-        v[q].x = gather_at(x, resampleII_index(i0, k, size), n);
-        v[q].y = gather_at(x, resampleII_index(i0 + 1, k, size), n);
+        const double i0 = i_first + (double)q * i_step;  // exact: integers < 2^26
+        v[q].x = resampleII_read(x, i0, k, size, n32);
+        v[q].y = resampleII_read(x, i0 + 1.0, k, size, n32);
     }
     dft<16>(v);
 #pragma unroll

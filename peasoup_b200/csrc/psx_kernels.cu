@@ -74,18 +74,19 @@ __global__ void __launch_bounds__(256) k_resample(const float* __restrict__ in,
             v.z = gather_at(in, resample_index(i0 + 2, k, s2), n);
             v.w = gather_at(in, resample_index(i0 + 3, k, s2), n);
         } else {
-            v.x = gather_at(in, resampleII_index(i0 + 0, k, size), n);
-            v.y = gather_at(in, resampleII_index(i0 + 1, k, size), n);
-            v.z = gather_at(in, resampleII_index(i0 + 2, k, size), n);
-            v.w = gather_at(in, resampleII_index(i0 + 3, k, size), n);
+            const double id = (double)i0;  // exact (n < 2^32)
+            v.x = resampleII_read(in, id, k, size, (unsigned)n);
+            v.y = resampleII_read(in, id + 1.0, k, size, (unsigned)n);
+            v.z = resampleII_read(in, id + 2.0, k, size, (unsigned)n);
+            v.w = resampleII_read(in, id + 3.0, k, size, (unsigned)n);
         }
         reinterpret_cast<float4*>(o)[q] = v;
     }
     // tail (n not a multiple of 4)
     if (blockIdx.x == 0 && threadIdx.x < (n & 3)) {
         const unsigned long long i = 4ull * n4 + threadIdx.x;
-        o[i] = gather_at(in, CENTRED ? resample_index(i, k, size * 0.5)
-                                     : resampleII_index(i, k, size), n);
+        o[i] = CENTRED ? gather_at(in, resample_index(i, k, size * 0.5), n)
+                       : resampleII_read(in, (double)i, k, size, (unsigned)n);
     }
 }
 
@@ -99,8 +100,8 @@ double accel_fact(float acc, float tsamp)
 int launch_resample(const float* d_in, float* d_out, size_t n, const double* d_ktab,
                     double k, int ntrials, size_t out_pitch, bool centred, cudaStream_t s)
 {
-    if (!d_in || !d_out || n == 0 || ntrials <= 0) {
-        set_error("resample: bad arguments");
+    if (!d_in || !d_out || n == 0 || n >= (size_t(1) << 32) || ntrials <= 0) {
+        set_error("resample: bad arguments (1 <= n < 2^32)");
         return PSX_ERR_INVALID;
     }
     const unsigned threads = 256;
