@@ -517,7 +517,9 @@ int psx_search_get_profile(psx_search* s, psx_search_profile* out, int reset);
    N as the reference leaves it) and, for trial `trial` of the last call,
    its resampled series (N floats) and normalised interbinned spectrum
    (N/2+1 floats), recomputed on the device through the instance's own
-   transform path (psx_search_info::fft_form).  Any pointer may be NULL. */
+   transform path (psx_search_info::fft_form; with the two-pass transform
+   the series is what its first pass gathers, dumped instead of
+   transformed).  Any pointer may be NULL. */
 int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
                          float* h_tim_r, float* h_pspec, float* h_norm2);
 

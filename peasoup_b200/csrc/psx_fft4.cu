@@ -130,6 +130,9 @@ __device__ __forceinline__ void dft(float2 (&v)[L])
 // exchange below.
 __device__ __forceinline__ unsigned swz_a(unsigned e) { return e ^ ((e >> 4) & 1u); }
 
+// DUMP: write the gathered pairs z[e C + c] (the resampled series as it is
+// read, interleaved) to y instead of transforming them (the debug tap).
+template <bool DUMP>
 __global__ void __launch_bounds__(kColsW * 64, 2)
     k_fft4_cols(const float* __restrict__ x, unsigned long long n, const double* __restrict__ ktab,
                 const float2* __restrict__ tab, unsigned offA2, unsigned offA3, unsigned offQ,
@@ -151,6 +154,12 @@ __global__ void __launch_bounds__(kColsW * 64, 2)
         const double i0 = i_first + (double)q * i_step;  // exact: integers < 2^26
         v[q].x = resampleII_read(x, i0, k, size, n32);
         v[q].y = resampleII_read(x, i0 + 1.0, k, size, n32);
+    }
+    if constexpr (DUMP) {
+        float2* yo = y + (size_t)blockIdx.y * ypitch;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) yo[(size_t)(t + 64 * q) * C + c] = v[q];
+        return;
     }
     dft<16>(v);
 #pragma unroll
@@ -484,7 +493,7 @@ int Fft4Plan::create(size_t n_)
     // (the default shared/L1 split: measured on B200, forcing the largest
     // shared carve-out slowed the gather of pass 1 and the twiddle reads of
     // pass 2, both served from L1)
-    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols,
+    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(kFft4Rows * kColsW * sizeof(float2))),
                         "fft4 column pass attribute"));
@@ -518,9 +527,23 @@ int Fft4Plan::exec_cols(const float* series, const double* ktab, int ntrials, fl
         return PSX_ERR_INVALID;
     }
     dim3 ga(C / kColsW, (unsigned)ntrials);
-    k_fft4_cols<<<ga, kColsW * 64, kFft4Rows * kColsW * sizeof(float2), s>>>(
+    k_fft4_cols<false><<<ga, kColsW * 64, kFft4Rows * kColsW * sizeof(float2), s>>>(
         series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
     return launch_status("fft4 column pass");
+}
+
+int Fft4Plan::dump_gather(const float* series, const double* ktab, float* out,
+                          cudaStream_t s) const
+{
+    if (!d_tab || !series || !ktab || !out) {
+        set_error("fft4 dump: bad arguments");
+        return PSX_ERR_INVALID;
+    }
+    dim3 ga(C / kColsW, 1);
+    k_fft4_cols<true><<<ga, kColsW * 64, 0, s>>>(series, (unsigned long long)n, ktab, d_tab,
+                                                 offA2, offA3, offQ, offP, C,
+                                                 reinterpret_cast<float2*>(out), n / 2);
+    return launch_status("fft4 gather dump");
 }
 
 int Fft4Plan::exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt, size_t zpitch,

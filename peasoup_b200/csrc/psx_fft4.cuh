@@ -40,6 +40,9 @@ struct Fft4Plan {
                   size_t ypitch, cudaStream_t s) const;
     int exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt, size_t zpitch,
                   cudaStream_t s) const;
+    // The N samples pass 1 gathers for one trial (ktab[0]), written to out
+    // in series order instead of being transformed (the debug tap).
+    int dump_gather(const float* series, const double* ktab, float* out, cudaStream_t s) const;
 
     // Real spectrum bins 0..M of each trial from zt, interbinned and
     // normalised with stat[3] (mean*N) and stat[4] (std*N), written at

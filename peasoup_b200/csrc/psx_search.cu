@@ -1666,8 +1666,12 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
             set_error("debug_tap: trial %d out of range", trial);
             return PSX_ERR_INVALID;
         }
-        PSX_TRY(launch_resample(sl.d_tim, s->d_tr, s->N, nullptr,
-                                accel_fact(accs[trial], s->cfg.tsamp), 1, s->N, false, s->st));
+        if (s->fft4())  // what the trials' own pass 1 gathers
+            PSX_TRY(s->f4.dump_gather(sl.d_tim, sl.d_ktab + trial, s->d_tr, s->st));
+        else
+            PSX_TRY(launch_resample(sl.d_tim, s->d_tr, s->N, nullptr,
+                                    accel_fact(accs[trial], s->cfg.tsamp), 1, s->N, false,
+                                    s->st));
         if (h_tim_r)
             PSX_CUDA(cudaMemcpyAsync(h_tim_r, s->d_tr, sizeof(float) * s->N,
                                      cudaMemcpyDeviceToHost, s->st));

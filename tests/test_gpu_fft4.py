@@ -94,3 +94,25 @@ def test_default_form_by_size(S):
                  per_dm=False)
         assert s.info()["fft_form"] == want, n
         s.close()
+
+
+@pytest.mark.parametrize("n", [1 << 19, 1 << 22])
+def test_gathered_series_bit_exact(S, oracle, n):
+    """What pass 1 gathers (dumped by the debug tap instead of transformed)
+    is the resampled series, bit for bit, against the oracle's FP64 index on
+    the product's own dereddened series."""
+    search, synth = S
+    ts = 64e-6
+    x = synth.make_series_np(synth.SeriesSpec(nsamps=n, tsamp=ts), 11)
+    s = search.AccelSearch(_params(S, n, ts, batch=4, acc_lo=-300.0, acc_hi=300.0,
+                                   nharmonics=2, min_snr=9.0))
+    s.search(x, 0.0, 0, per_dm=False)
+    assert s.info()["fft_form"] == 3
+    from peasoup_b200.transforms import AccelerationPlan
+    accs = AccelerationPlan(-300.0, 300.0, 1.10, 64e-6, n, ts, synth.CFREQ_HZ,
+                            synth.CH_BW_HZ).generate_accel_list(0.0, 0.0)
+    for t in sorted({0, len(accs) // 3, len(accs) - 1}):
+        tim, tr, ps, _ = s.debug_tap(t)
+        want = tim[oracle.resampleII_index(n, float(accs[t]), ts).astype(np.int64)]
+        assert np.array_equal(tr, want), t
+    s.close()
