@@ -405,8 +405,10 @@ typedef struct {
 } psx_search_config;
 
 /* Number of tile shapes of the fused harmonic-sum kernel (tile bins,
-   consumer threads, CTAs per SM, exact pass in or out of line). */
-#define PSX_HARM_SHAPES 5
+   consumer threads, CTAs per SM, exact pass in or out of line; shapes 6
+   and 7 stage each tile for 3 or 2 trials at once with 2D tensor copies
+   and need the batched mode with at least that many trials per group). */
+#define PSX_HARM_SHAPES 7
 
 /* Fills `cfg` with the reference's defaults (include/utils/cmdline.hpp:
    99-191) for a transform of `fft_size` samples of `tsamp` s. */

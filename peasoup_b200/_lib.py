@@ -25,7 +25,7 @@ PSX_ERR_BUSY = 8
 
 PSX_FFT_R2C = 0
 PSX_FFT_C2R = 1
-PSX_HARM_SHAPES = 5
+PSX_HARM_SHAPES = 7
 PSX_MODE_PLAIN = 0
 PSX_MODE_BATCHED = 1
 PSX_OUT_TRIAL = 0

@@ -23,6 +23,7 @@
 // the exact pass (reference scales, search ranges, one atomic per warp and
 // fold).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "psx_device.cuh"
@@ -349,12 +350,19 @@ __device__ __noinline__ void exact_pass_ool(const float* __restrict__ sm, unsign
 
 // Sums one staged item: the fast pass, then -- only in warps where some
 // output passes the vote -- the exact pass (inline or out of line).
-template <int F, int T, int NC, bool OOL>
+template <int F, int T, int NC, int ROWS>
+__device__ __noinline__ void exact_pass_rows_ool(const float* __restrict__ sm, unsigned i0,
+                                                 unsigned tid, unsigned rho, const PeakParams& pp,
+                                                 int trial, int4* __restrict__ rec,
+                                                 unsigned* __restrict__ counter, unsigned cap);
+
+template <int F, int T, int NC, bool OOL, int ROWS = 0>
 __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
                                          const unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1],
                                          const FoldScales& fs, unsigned i0, unsigned tid,
                                          const PeakParams& pp, int trial, int4* __restrict__ rec,
-                                         unsigned* __restrict__ counter, unsigned cap)
+                                         unsigned* __restrict__ counter, unsigned cap,
+                                         unsigned rho = 0)
 {
     constexpr int K = T / NC;
     float2 acc[K / 2];
@@ -370,7 +378,9 @@ __device__ __forceinline__ void sum_item(const float* __restrict__ sm,
 #pragma unroll
     for (int k = 0; k < K; ++k) over |= mx[k] > pp.vote;
     if (__any_sync(0xffffffffu, over)) {
-        if (OOL)
+        if constexpr (ROWS > 0)
+            exact_pass_rows_ool<F, T, NC, ROWS>(sm, i0, tid, rho, pp, trial, rec, counter, cap);
+        else if (OOL)
             exact_pass_ool<F, T, NC>(sm, i0, tid, pp, trial, rec, counter, cap);
         else
             exact_body<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
@@ -501,6 +511,211 @@ __global__ void __launch_bounds__(NC + 32, MINB) k_harm_tiles(const float* __res
     }
     // After an abort, copies the producer issued may still be landing in this
     // CTA's shared memory: wait for them (bounded) before the CTA exits.
+    __syncthreads();
+    if (abort_flag && threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s)
+            while (landed[s] < issued[s]) {
+                if (!mbar_wait_bounded(&full[s], landed[s] & 1u, kLimit)) break;
+                landed[s] += 1;
+            }
+    }
+    if ((!ok || abort_flag) && lane == 0) atomicExch(counter + 1, kHarmStagingTimeout);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-row staging: one work item is one tile of T output bins for ROWS
+// consecutive trials (rows of the spectrum buffer), and every window --
+// the tile and each fraction's -- arrives for all ROWS rows at once as one
+// 2D tensor copy (TMA) of a box [width, ROWS], so a CTA issues 2^F copies
+// per ROWS * T outputs instead of per T.  The tensor maps view the buffer
+// as rows of 8-byte elements (two floats), which keeps every window within
+// the 256-element box limit (widths 32 .. 512 floats in steps of 32, one
+// map each); window starts i0*m/2^h are multiples of 4 floats, i.e. 16
+// bytes.  Bins past the row's end and rows past the buffer arrive as zeros
+// (the maps' out-of-bounds fill), rows past the launch group's trials are
+// staged but not summed.
+constexpr int kHarmWidthClasses = 16;  // window widths 32 * (c + 1) floats
+
+struct HarmMaps {
+    CUtensorMap m[kHarmWidthClasses];
+};
+
+// Samples window q needs (q = -1: the tile) and its staged width.
+__host__ __device__ constexpr int win_need(int q, int T)
+{
+    return q < 0 ? T : (((T - 1) * frac_m(q) + (1 << (frac_h(q) - 1))) >> frac_h(q)) + 1;
+}
+__host__ __device__ constexpr int win_width(int q, int T) { return (win_need(q, T) + 31) / 32 * 32; }
+// Offset (floats) of window q's [ROWS][width] block in a stage; the tile's
+// [ROWS][T] block comes first.
+__host__ __device__ constexpr int rows_slot(int q, int T, int ROWS)
+{
+    int off = ROWS * T;
+    for (int r = 0; r < q; ++r) off += ROWS * win_width(r, T);
+    return q < 0 ? 0 : off;
+}
+__host__ __device__ constexpr int rows_stage_floats(int F, int T, int ROWS)
+{
+    return rows_slot(nfrac(F), T, ROWS);
+}
+
+// Offsets of fraction q's source for consumer `tid` of row `rho`, relative
+// to that row's tile (sm + rho * T).
+template <int F, int T, int ROWS>
+__device__ __forceinline__ void make_bases_rows(unsigned tid, unsigned rho,
+                                                unsigned (&base)[nfrac(F) > 0 ? nfrac(F) : 1])
+{
+#pragma unroll
+    for (int q = 0; q < nfrac(F); ++q) {
+        const unsigned hh = (unsigned)frac_h(q), mm = (unsigned)frac_m(q);
+        base[q] = (unsigned)rows_slot(q, T, ROWS) - rho * (unsigned)T +
+                  rho * (unsigned)win_width(q, T) + ((tid * mm + (1u << (hh - 1))) >> hh);
+    }
+}
+
+template <int F, int T, int NC, int ROWS>
+__device__ __noinline__ void exact_pass_rows_ool(const float* __restrict__ sm, unsigned i0,
+                                                 unsigned tid, unsigned rho, const PeakParams& pp,
+                                                 int trial, int4* __restrict__ rec,
+                                                 unsigned* __restrict__ counter, unsigned cap)
+{
+    unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
+    make_bases_rows<F, T, ROWS>(tid, rho, base);
+    const FoldScales fs;
+    exact_body<F, T, NC>(sm, base, fs, i0, tid, pp, trial, rec, counter, cap);
+}
+
+// 2D tensor copy of the box at element coordinates (x, y) of `map` into
+// this CTA's shared memory, completing as transaction bytes on `bar`.  Not
+// multicast.
+__device__ __forceinline__ void tensor_g2s_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                              uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y),
+          "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Persistent CTA (one per SM): warp 0 produces, ROWS * NC / 32 warps
+// consume (NC per row); two stages.  Same ring, bounded waits and abort
+// path as k_harm_tiles.
+template <int F, int T, int NC, int ROWS>
+__global__ void __launch_bounds__(ROWS * NC + 32, 1)
+    k_harm_rows(const __grid_constant__ HarmMaps maps, PeakParams pp, int trial0, int rows,
+                unsigned ntiles, int4* __restrict__ rec, unsigned* __restrict__ counter,
+                unsigned cap)
+{
+    static_assert(T % 128 == 0 && NC % 32 == 0 && T % (2 * NC) == 0 && T <= 512, "tile shape");
+    constexpr int STAGE = rows_stage_floats(F, T, ROWS);
+    constexpr int NW = nfrac(F) + 1;          // windows (tile + fractions)
+    constexpr unsigned NCW = ROWS * NC / 32;  // consumer warps
+    const unsigned kLimit = pp.wait_limit ? pp.wait_limit : kHarmWaitLimit;
+    extern __shared__ __align__(128) float4 smem4r[];
+    __shared__ __align__(8) uint64_t full[2], empty[2];
+    __shared__ volatile int abort_flag;
+    __shared__ unsigned issued[2], landed[2];
+    float* smem = reinterpret_cast<float*>(smem4r);
+    const unsigned ngroups = ((unsigned)rows + ROWS - 1) / ROWS;
+    const unsigned nitems = ntiles * ngroups;
+    if (blockIdx.x >= nitems) return;
+    const unsigned warp = threadIdx.x / 32, lane = threadIdx.x & 31u;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NCW);
+            issued[s] = 0;
+            landed[s] = 0;
+        }
+        abort_flag = 0;
+        mbar_init_fence();
+    }
+    __syncthreads();
+    bool ok = true;
+    unsigned grp = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+    const unsigned gstep_grp = gridDim.x / ntiles, gstep_tile = gridDim.x % ntiles;
+    auto advance = [&]() {
+        grp += gstep_grp;
+        tile += gstep_tile;
+        if (tile >= ntiles) {
+            tile -= ntiles;
+            ++grp;
+        }
+    };
+    if (warp == 0) {
+        // ---------------- producer: lane = window (0 the tile, q + 1 fraction q)
+        const bool active = lane < (unsigned)NW;
+        const int q = (int)lane - 1;
+        unsigned m = 1, h = 0, slot = 0, wcls = 0, bytes = 0;
+        if (active) {
+            if (q >= 0) {
+                m = (unsigned)frac_m(q);
+                h = (unsigned)frac_h(q);
+            }
+            slot = (unsigned)rows_slot(q, T, ROWS);
+            wcls = (unsigned)win_width(q, T) / 32u - 1u;
+            bytes = 4u * (unsigned)ROWS * (unsigned)win_width(q, T);
+        }
+        const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
+        const CUtensorMap* map = &maps.m[wcls];
+        for (unsigned j = 0; grp < ngroups; ++j, advance()) {
+            const unsigned s = j & 1u;
+            if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+            if (j >= 2) {
+                const bool got = mbar_wait_bounded(&empty[s], ((j >> 1) - 1) & 1u, kLimit);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    if (lane == 0) abort_flag = 1;
+                    break;
+                }
+            }
+            if (lane == 0) mbar_arrive_expect_tx(&full[s], total);
+            __syncwarp();
+            if (pp.flags & kHarmNoCopies) continue;
+            const unsigned i0 = pp.lo + tile * (unsigned)T;
+            // window start in floats, a multiple of 4 (i0 is a multiple of 128)
+            const unsigned a = (unsigned)(((unsigned long long)i0 * m) >> h);
+            if (active)
+                tensor_g2s_2d(smem + s * STAGE + slot, map, (int)(a >> 1), (int)(grp * ROWS),
+                              &full[s]);
+            if (lane == 0) issued[s] += 1;
+        }
+    } else {
+        // ---------------- consumers: ROWS groups of NC threads, one row each
+        const unsigned ct = threadIdx.x - 32;
+        const unsigned rho = ct / NC, tid = ct % NC;  // rho is warp-uniform
+        const FoldScales fs;
+        unsigned base[nfrac(F) > 0 ? nfrac(F) : 1];
+        make_bases_rows<F, T, ROWS>(tid, rho, base);
+        unsigned ph = 0;
+        for (;;) {
+#pragma unroll
+            for (unsigned s = 0; s < 2; ++s) {
+                if (grp >= ngroups || __any_sync(0xffffffffu, abort_flag != 0)) break;
+                const bool got = mbar_wait_bounded(&full[s], ph, kLimit);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    if (lane == 0) abort_flag = 1;
+                    break;
+                }
+                if (ct == 0) landed[s] += 1;
+                const unsigned row = grp * ROWS + rho;
+                if (row < (unsigned)rows)
+                    sum_item<F, T, NC, true, ROWS>(smem + s * STAGE + rho * T, base, fs,
+                                                   pp.lo + tile * (unsigned)T, tid, pp,
+                                                   trial0 + (int)row, rec, counter, cap, rho);
+                __syncwarp();
+                if (lane == 0)
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s]))
+                                 : "memory");
+                advance();
+            }
+            if (grp >= ngroups || __any_sync(0xffffffffu, abort_flag != 0)) break;
+            ph ^= 1u;
+        }
+    }
     __syncthreads();
     if (abort_flag && threadIdx.x == 0) {
         for (int s = 0; s < 2; ++s)

@@ -19,6 +19,8 @@
 //   (peakfinder.hpp:72-101), forms frequencies and distils them
 //   (distiller.hpp) while the GPU already runs the next DM (two record
 //   slots, psx_search_block).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
@@ -239,19 +241,24 @@ __global__ void __launch_bounds__(256) k_unpack_form_norm(const float* __restric
 // Persistent grid of MINB CTAs per SM, each one producer warp plus NC
 // consumer threads and kHarmStages shared stages of a T-bin tile and its
 // fractional windows.  The shapes below are the autotuner's choices
-// (psx_search_config::harm_shape); shape 4 is the default.
+// (psx_search_config::harm_shape); shape 4 is the default.  Shapes 6 and 7
+// stage every window for 3 or 2 trials at once with 2D tensor copies
+// (k_harm_rows, one CTA per SM, NC consumers per trial).
 constexpr int kHarmStages = 2;
 
 struct HarmShape {
     int T, NC, minb;
     bool ool;  // exact pass out of line
+    int rows;  // trials per item (multi-row kernel), 0 for k_harm_tiles
 };
 constexpr HarmShape kHarmShapes[] = {
-    {512, 128, 3, true},   // 1
-    {512, 256, 3, true},   // 2
-    {256, 128, 6, true},   // 3
-    {512, 256, 3, false},  // 4
-    {256, 128, 6, false},  // 5
+    {512, 128, 3, true, 0},   // 1
+    {512, 256, 3, true, 0},   // 2
+    {256, 128, 6, true, 0},   // 3
+    {512, 256, 3, false, 0},  // 4
+    {256, 128, 6, false, 0},  // 5
+    {512, 128, 1, true, 3},   // 6
+    {512, 128, 1, true, 2},   // 7
 };
 static_assert(sizeof(kHarmShapes) / sizeof(kHarmShapes[0]) == PSX_HARM_SHAPES, "shape table");
 constexpr int kHarmDefaultShape = 4;
@@ -283,10 +290,43 @@ struct HarmKernel {
     }
 };
 
+// The multi-row kernel (shapes 6 and 7): ROWS trials per item.
+template <int F, int SH>
+struct HarmRowsKernel {
+    static constexpr HarmShape S = kHarmShapes[SH];
+    static constexpr size_t smem_bytes()
+    {
+        return (size_t)kHarmStages * sizeof(float) * rows_stage_floats(F, S.T, S.rows);
+    }
+    static int configure()
+    {
+        return cuda_status(cudaFuncSetAttribute(k_harm_rows<F, S.T, S.NC, S.rows>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem_bytes()),
+                           "harmonic-sum kernel attribute");
+    }
+    static int launch(const HarmMaps* maps, const PeakParams& pp, int trial0, int rows, int4* rec,
+                      unsigned* counter, unsigned cap, cudaStream_t s)
+    {
+        if (!maps) {
+            set_error("harmonic-sum kernel: shape %d needs the instance's tensor maps", SH + 1);
+            return PSX_ERR_INVALID;
+        }
+        const unsigned ntiles = (pp.hi - pp.lo + S.T - 1) / S.T;
+        const unsigned items = ntiles * (((unsigned)rows + S.rows - 1) / S.rows);
+        const unsigned grid = std::min(items, (unsigned)sm_count());
+        k_harm_rows<F, S.T, S.NC, S.rows><<<grid, S.rows * S.NC + 32, smem_bytes(), s>>>(
+            *maps, pp, trial0, rows, ntiles, rec, counter, cap);
+        return launch_status("harmonic-sum kernel");
+    }
+};
+
 template <int F>
 static int configure_harm_f()
 {
     int rc = PSX_OK;
+    if (rc == PSX_OK) rc = HarmRowsKernel<F, 5>::configure();
+    if (rc == PSX_OK) rc = HarmRowsKernel<F, 6>::configure();
     if (rc == PSX_OK) rc = HarmKernel<F, 0>::configure();
     if (rc == PSX_OK) rc = HarmKernel<F, 1>::configure();
     if (rc == PSX_OK) rc = HarmKernel<F, 2>::configure();
@@ -312,9 +352,11 @@ static int configure_harm(int F)
 template <int F>
 static int launch_harm_f(int shape, const float* p, size_t ppitch, unsigned row_len,
                          const PeakParams& pp, int trial0, int rows, int4* rec, unsigned* counter,
-                         unsigned cap, cudaStream_t s)
+                         unsigned cap, cudaStream_t s, const HarmMaps* maps)
 {
     switch (shape) {
+    case 6: return HarmRowsKernel<F, 5>::launch(maps, pp, trial0, rows, rec, counter, cap, s);
+    case 7: return HarmRowsKernel<F, 6>::launch(maps, pp, trial0, rows, rec, counter, cap, s);
     case 2: return HarmKernel<F, 1>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
     case 3: return HarmKernel<F, 2>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
     case 4: return HarmKernel<F, 3>::launch(p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
@@ -325,19 +367,61 @@ static int launch_harm_f(int shape, const float* p, size_t ppitch, unsigned row_
 
 static int launch_harm(int F, int shape, const float* p, size_t ppitch, unsigned row_len,
                        const PeakParams& pp, int trial0, int rows, int4* rec, unsigned* counter,
-                       unsigned cap, cudaStream_t s)
+                       unsigned cap, cudaStream_t s, const HarmMaps* maps = nullptr)
 {
     switch (F) {
-    case 0: return launch_harm_f<0>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 1: return launch_harm_f<1>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 2: return launch_harm_f<2>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 3: return launch_harm_f<3>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    case 4: return launch_harm_f<4>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
-    default: return launch_harm_f<5>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s);
+    case 0: return launch_harm_f<0>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s, maps);
+    case 1: return launch_harm_f<1>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s, maps);
+    case 2: return launch_harm_f<2>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s, maps);
+    case 3: return launch_harm_f<3>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s, maps);
+    case 4: return launch_harm_f<4>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s, maps);
+    default: return launch_harm_f<5>(shape, p, ppitch, row_len, pp, trial0, rows, rec, counter, cap, s, maps);
     }
 }
 
 constexpr int kDeviceBaselinePasses = 4;
+
+// Tensor maps of a spectrum buffer of `rows` rows of `pitch` floats for
+// the multi-row harmonic kernel: the rows as 8-byte elements, one map per
+// window width 32 (c + 1) floats, boxes [width, box_rows]; out-of-bounds
+// elements read as zero.  cuTensorMapEncodeTiled comes from the driver
+// through the runtime's entry-point query.
+static int encode_harm_maps(const float* buf, size_t pitch, int rows, int box_rows, HarmMaps* out)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            (void)cudaGetLastError();
+            set_error("cuTensorMapEncodeTiled is not available from the driver");
+            return PSX_ERR_CUDA;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if ((pitch & 3) || (reinterpret_cast<uintptr_t>(buf) & 15) || rows < 1) {
+        set_error("harmonic maps: pitch must be a multiple of 4 floats and the buffer 16-byte aligned");
+        return PSX_ERR_INVALID;
+    }
+    for (int c = 0; c < kHarmWidthClasses; ++c) {
+        const cuuint64_t dims[2] = {(cuuint64_t)(pitch / 2), (cuuint64_t)rows};
+        const cuuint64_t strides[1] = {(cuuint64_t)(pitch * sizeof(float))};
+        const cuuint32_t box[2] = {(cuuint32_t)(16 * (c + 1)), (cuuint32_t)box_rows};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = encode(&out->m[c], CU_TENSOR_MAP_DATA_TYPE_INT64, 2,
+                                  const_cast<float*>(buf), dims, strides, box, estr,
+                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            set_error("cuTensorMapEncodeTiled failed (%d) for the harmonic maps", (int)r);
+            return PSX_ERR_CUDA;
+        }
+    }
+    return PSX_OK;
+}
 
 }  // namespace psx
 
@@ -436,6 +520,7 @@ struct psx_search {
     float* d_trl[2] = {nullptr, nullptr};
     float* d_Xl[2] = {nullptr, nullptr};
     float* d_pl[2] = {nullptr, nullptr};
+    HarmMaps hmaps[2] = {};  // per lane: the spectra as boxes of the multi-row shape's rows
     float* d_tr = nullptr;
     float* d_X = nullptr;
     float* d_p = nullptr;
@@ -784,7 +869,7 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 2], ls));
         if (span) {
             PSX_TRY(launch_harm(F, harm_shape, pp, Bp, (unsigned)Bp, pk, t0, b, s.d_rec,
-                                s.d_count, (unsigned)s.rec_cap, ls));
+                                s.d_count, (unsigned)s.rec_cap, ls, &hmaps[lane]));
             ++s.launches;
         }
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 3], ls));
@@ -1144,6 +1229,8 @@ void psx_search_config_defaults(psx_search_config* c, size_t fft_size, float tsa
     c->fft_form = 0;
 }
 
+static int effective_batch(const psx_search_config* c);
+
 static int check_config(const psx_search_config* c)
 {
     if (!c) {
@@ -1186,6 +1273,13 @@ static int check_config(const psx_search_config* c)
     }
     if (c->harm_shape < 0 || c->harm_shape > PSX_HARM_SHAPES) {
         set_error("search: harm_shape must be 0..%d", PSX_HARM_SHAPES);
+        return PSX_ERR_INVALID;
+    }
+    if (c->harm_shape > 0 && kHarmShapes[c->harm_shape - 1].rows > 0 &&
+        (c->mode != PSX_MODE_BATCHED || effective_batch(c) < kHarmShapes[c->harm_shape - 1].rows)) {
+        set_error("search: harm_shape %d stages %d trials per tile and needs the batched mode "
+                  "with at least that many trials per launch group",
+                  c->harm_shape, kHarmShapes[c->harm_shape - 1].rows);
         return PSX_ERR_INVALID;
     }
     if (c->nbirdies && (!c->birdie_freqs || !c->birdie_widths)) {
@@ -1351,6 +1445,11 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->d_tr = s->d_trl[0];
     s->d_X = s->d_Xl[0];
     s->d_p = s->d_pl[0];
+    if (kHarmShapes[s->harm_shape - 1].rows > 0)
+        for (int l = 0; l < s->lanes; ++l)
+            if ((rc = encode_harm_maps(s->d_pl[l], Bp, (int)b, kHarmShapes[s->harm_shape - 1].rows,
+                                       &s->hmaps[l])) != PSX_OK)
+                return fail(rc);
     ALLOC(s->d_kbatch, sizeof(double) * b);
     for (Slot& sl : s->slot) {
         ALLOC(sl.d_count, sizeof(unsigned) * 16);

@@ -98,7 +98,10 @@ extern "C" int psx_autotune(psx_search_config* cfg, const int* h_batches, int nb
             if (psx_search_footprint(&c) < free_b / 10 * 8) {
                 psx_search* s = nullptr;
                 rc = psx_search_create(&c, &s);
-                if (rc == PSX_OK) {
+                if (rc == PSX_ERR_INVALID) {  // a shape this batch cannot use: skip it
+                    clear_error();
+                    rc = PSX_OK;
+                } else if (rc == PSX_OK) {
                     size_t n = 0;
                     // one DM to warm up (plans, graph capture), then `reps`
                     // DMs through the pipelined block call, timed on the host

@@ -121,3 +121,10 @@ def test_server_needs_a_device(psx):
     assert psx.psx_server_create(C.byref(cfg), C.byref(h)) == PSX_ERR_CUDA
     bad = ServerConfig(device=0, hbm_budget=0, max_active=0, max_queue=0)
     assert psx.psx_server_create(C.byref(bad), C.byref(h)) == 1
+
+
+def test_binding_constants_match_header():
+    import re
+    hdr = open(os.path.join(os.path.dirname(_lib.LIB_PATH), "..", "include",
+                            "peasoup_b200.h")).read()
+    assert int(re.search(r"#define PSX_HARM_SHAPES (\d+)", hdr).group(1)) == _lib.PSX_HARM_SHAPES
