@@ -755,7 +755,7 @@ def run_psx(args, ws, rank, local):
         "harm": 4.0 * B,                  # read the normalised spectrum once
     }
     stage_kernels = {"resample": "k_resample", "fft": "cuFFT", "form": "k_unpack_form_norm",
-                     "harm": "k_harm_tiles"}
+                     "harm": "k_harm_rows" if shape_used >= 6 else "k_harm_tiles"}
     if form_used == 3:
         # the two-pass transform: pass 1 (timed as "resample") gathers the
         # series (4N bytes) and writes the column transforms (M complex =
