@@ -772,7 +772,8 @@ def run_psx(args, ws, rank, local):
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tp):
         tj = json.load(open(tp))
-        traffic = (tj.get("two_pass", {}) if form_used == 3 else tj).get(dom)
+        tkey = "harm_rows" if (dom == "harm" and shape_used >= 6) else dom
+        traffic = (tj.get("two_pass", {}) if form_used == 3 else tj).get(tkey)
     stages = {}
     for k, ms in stage_ms.items():
         sec = ms / 1e3 / trials_prof
