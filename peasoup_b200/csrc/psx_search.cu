@@ -784,6 +784,18 @@ int psx_search::prologue(Slot& s)
     return PSX_OK;
 }
 
+// Trials of the launch group starting at t0: `batch` while that many are
+// left; the rest as one group with the two-pass transform (any group size
+// works there), else in power-of-two groups (the cuFFT plans exist for
+// powers of two only).
+static int group_size(int nacc, int t0, int batch, bool any_size)
+{
+    int b = batch;
+    if (any_size) return std::min(b, nacc - t0);
+    while (b > nacc - t0) b >>= 1;
+    return b;
+}
+
 // Enqueues every acceleration trial of the DM (k factors already in
 // s.d_ktab) plus the reset of the record counter.
 int psx_search::trials_enqueue(Slot& s, int nacc)
@@ -821,8 +833,7 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
         if (fft4()) {
             // resample gather + transform in two passes; the profile times
             // the first pass (which does the gather) as the resample stage
-            b = batch;
-            while (b > nacc - t0) b >>= 1;
+            b = group_size(nacc, t0, batch, true);
             PSX_TRY(f4.exec_cols(s.d_tim, s.d_ktab + t0, b, reinterpret_cast<float2*>(tr), N / 2,
                                  ls));
             if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], ls));
@@ -884,14 +895,12 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
     return PSX_OK;
 }
 
-static int count_groups(int nacc, bool batched, int batch)
+static int count_groups(int nacc, bool batched, int batch, bool any_size)
 {
     if (!batched) return nacc;
     int t0 = 0, g = 0;
     while (t0 < nacc) {
-        int b = batch;
-        while (b > nacc - t0) b >>= 1;
-        t0 += b;
+        t0 += group_size(nacc, t0, batch, any_size);
         ++g;
     }
     return g;
@@ -902,7 +911,7 @@ int psx_search::run_trials(Slot& s, int nacc)
     // events recorded inside a graph carry no timestamps: profiling runs
     // the schedule without capture
     const bool graph = batched() && cfg.use_graph && !s.profiled;
-    if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
+    if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch, fft4())));
     if (!graph) return trials_enqueue(s, nacc);
     // One lane: the graph holds the counter reset and the full launch groups
     // and is keyed by their number, which neighbouring DM trials share (the
@@ -919,12 +928,14 @@ int psx_search::run_trials(Slot& s, int nacc)
     };
     if (it == graphs.end() && capture_failures[key] >= 2) return trials_enqueue(s, nacc);
     if (it == graphs.end()) {
-        // plans must exist before capture (creation allocates)
-        for (int l = 0; l < lanes; ++l)
-            for (int b = batch; b >= 1; b >>= 1) {
-                FftPlan* p = nullptr;
-                PSX_TRY(get_plan(b, &p, l));
-            }
+        // cuFFT plans must exist before capture (creation allocates); the
+        // two-pass transform has none
+        if (!fft4())
+            for (int l = 0; l < lanes; ++l)
+                for (int b = batch; b >= 1; b >>= 1) {
+                    FftPlan* p = nullptr;
+                    PSX_TRY(get_plan(b, &p, l));
+                }
         const int l0 = s.launches, f0 = s.ffts;
         PSX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int rc = trials_enqueue(s, upto);
@@ -981,7 +992,7 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
     const int nacc = (int)s.accs.size();
     PSX_TRY(grow_ktab(s, (size_t)nacc));
     for (int t = 0; t < nacc; ++t) s.h_ktab[t] = accel_fact(s.accs[t], c.tsamp);
-    if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch)));
+    if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch, fft4())));
     PSX_TRY(prologue(s));
     PSX_CUDA(cudaStreamWaitEvent(st, s.ready, 0));
     PSX_CUDA(cudaMemcpyAsync(s.d_ktab, s.h_ktab, sizeof(double) * nacc, cudaMemcpyHostToDevice, st));
@@ -1335,9 +1346,13 @@ size_t psx_search_footprint(const psx_search_config* c)
     bytes += L * sizeof(float) * Bp * b;              // normalised spectra, per lane
     bytes += 2 * sizeof(int4) * ((size_t)1 << 20);    // two initial record slots
     // cuFFT work areas: about one transform's worth per batched plan size and
-    // lane, plus the batch-1 plans of the two slots' prologues and the plain path
-    bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
-    if (effective_form(c) == 3) bytes += sizeof(float2) * (2400 + 82 * (N / 2048));  // twiddles
+    // lane (none with the two-pass transform, which has twiddle tables
+    // instead), plus the batch-1 plans of the two slots' prologues and the
+    // plain path
+    if (effective_form(c) == 3)
+        bytes += sizeof(float) * 2 * Bp * 6 + sizeof(float2) * (2400 + 82 * (N / 2048));
+    else
+        bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
     return bytes;
 }
 

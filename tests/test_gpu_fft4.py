@@ -116,3 +116,35 @@ def test_gathered_series_bit_exact(S, oracle, n):
         want = tim[oracle.resampleII_index(n, float(accs[t]), ts).astype(np.int64)]
         assert np.array_equal(tr, want), t
     s.close()
+
+
+def test_padding_zap_lanes_graphs(S):
+    """The two-pass path on a series shorter than the transform (zero
+    padding) with a birdie list: one or two lanes, with or without graph
+    capture, give bit-identical candidates (the same kernels in the same
+    order), and those equal the plain path's (the reference's real
+    transform), S/N within 1e-5."""
+    search, synth = S
+    n, ts = 1 << 19, 76e-6
+    plan = synth.survey_plan(ndm=1, nsamps=n - 20000, tsamp=ts, seed=5, npulsars=2, nbirdies=5)
+    for ps in plan.pulsars:
+        ps.amp = 30.0
+    x = synth.survey_series_np(plan, 0, seed=5)
+    assert x.size == n - 20000
+    kw = dict(acc_lo=-100.0, acc_hi=100.0, nharmonics=5, min_snr=6.0,
+              birdie_freqs=plan.birdie_freqs, birdie_widths=plan.birdie_widths)
+    outs = []
+    for lanes, graph in ((1, True), (2, True), (2, False)):
+        s = search.AccelSearch(_params(S, n, ts, batch=4, lanes=lanes, graph=graph, **kw))
+        c = s.search(x, float(plan.dms[0]), 0, per_dm=False)[0]
+        assert s.info()["fft_form"] == 3
+        outs.append(c)
+        s.close()
+    assert len(outs[0]) > 3
+    for c in outs[1:]:
+        assert np.array_equal(c, outs[0])
+    p = search.AccelSearch(_params(S, n, ts, mode="plain", **kw))
+    cp = p.search(x, float(plan.dms[0]), 0, per_dm=False)[0]
+    p.close()
+    nm, ua, ub, worst = match_candidates(outs[0], cp, 6.0, margin=1e-4)
+    assert nm > 3 and not ua and not ub and worst < 1e-5, (ua[:3], ub[:3], worst)
