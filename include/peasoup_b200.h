@@ -383,7 +383,9 @@ typedef struct {
     const float* birdie_widths;
     size_t nbirdies;
     int mode;                  /* PSX_MODE_* */
-    int batch;                 /* trials per launch (batched); 0 = tuned */
+    int batch;                 /* trials per launch (batched; rounded down to a
+                                  power of two unless the two-pass transform
+                                  carries the trials); 0 = default */
     int use_fft_callback;      /* batched: fuse the resample into cuFFT */
     int use_graph;             /* batched: capture the trial schedule */
     int harm_shape;            /* harmonic-kernel tile shape 1..PSX_HARM_SHAPES;

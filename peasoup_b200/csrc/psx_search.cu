@@ -1304,10 +1304,16 @@ static int check_config(const psx_search_config* c)
     return PSX_OK;
 }
 
+static int effective_form(const psx_search_config* c);
+
+// Trials per launch group: the configured count (or the default), rounded
+// down to a power of two where cuFFT plans carry the trials (they exist for
+// powers of two only); the two-pass transform takes any count.
 static int effective_batch(const psx_search_config* c)
 {
     if (c->mode != PSX_MODE_BATCHED) return 1;
     int b = c->batch ? c->batch : default_batch(c->fft_size);
+    if (effective_form(c) == 3) return b;
     int p = 1;
     while (p * 2 <= b) p *= 2;
     return p;
