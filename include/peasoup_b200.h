@@ -473,7 +473,9 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
    footprint exceeds 80 % of the free device memory are skipped.  Writes
    the fastest pair into cfg->batch and cfg->harm_shape; h_ms (may be NULL)
    receives nbatch * PSX_HARM_SHAPES milliseconds per DM trial, batch-major
-   (-1 for a skipped pair).  Results never depend on the pair chosen. */
+   (-1 for a skipped pair: one that does not fit, or that the configuration
+   cannot use, e.g. a multi-trial harmonic shape with fewer trials per
+   group).  Results never depend on the pair chosen. */
 int psx_autotune(psx_search_config* cfg, const int* h_batches, int nbatch,
                  int reps, int max_trials, double* h_ms);
 
