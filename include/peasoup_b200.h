@@ -39,7 +39,7 @@ enum {
     PSX_ERR_CUFFT = 3,       /* cuFFT error */
     PSX_ERR_ALLOC = 4,       /* device or host allocation failed */
     PSX_ERR_OVERFLOW = 5,    /* caller buffer too small; *n_out has the need */
-    PSX_ERR_UNSUPPORTED = 6, /* valid request this build does not support */
+    PSX_ERR_UNSUPPORTED = 6, /* valid request the library does not support */
     PSX_ERR_IO = 7,          /* file could not be read (zap list) */
     PSX_ERR_BUSY = 8         /* served loop: admission refused / queue full */
 };
