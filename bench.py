@@ -631,7 +631,7 @@ def run_psx(args, ws, rank, local):
     batch, shape = args.batch, args.harm_shape
     if not args.batch:
         t0 = time.perf_counter()
-        tune = search.autotune(make_params(plan, "batched"), batches=(16, 32, 48, 63, 64, 96),
+        tune = search.autotune(make_params(plan, "batched"), batches=(16, 32, 48, 63, 64, 96, 128),
                                reps=2)
         batch, shape = tune["batch"], tune["harm_shape"]
         log(f"[rank {rank}] autotune: batch {batch}, harmonic shape {shape} "

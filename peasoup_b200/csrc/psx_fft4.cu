@@ -289,16 +289,20 @@ __device__ __forceinline__ float2 zt_at(const float2* __restrict__ z, unsigned C
     return z[(size_t)(idx & (kFft4Rows - 1)) * C + (idx >> 10)];
 }
 
-// X[j] and X[M-j] of the real series from Z[j] = a and Z[M-j] = w, with
-// (cs, sn) = (cos, sin)(pi j / M) (the split step of a real transform
-// computed as a half-length complex one).
+// 2 X[j] and 2 X[M-j] of the real series from Z[j] = a and Z[M-j] = w,
+// with (cs, sn) = (cos, sin)(pi j / M) (the split step of a real transform
+// computed as a half-length complex one).  The factor 2 is kept: the
+// interbinned amplitude of 2X is exactly twice that of X (a power-of-two
+// scale commutes with rounding, square root included), and normalising
+// with twice the mean and twice the deviation gives exactly the same value,
+// so the four halvings per pair are not needed.
 __device__ __forceinline__ void unpack_one(float2 a, float2 w, float cs, float sn, float2& lo,
                                            float2& hi)
 {
     const float ar = a.x + w.x, ai = a.y - w.y, br = a.x - w.x, bi = a.y + w.y;
     const float u = cs * bi - sn * br, v = sn * bi + cs * br;
-    lo = make_float2(0.5f * (ar + u), 0.5f * (ai - v));
-    hi = make_float2(0.5f * (ar - u), 0.5f * (-ai - v));
+    lo = make_float2(ar + u, ai - v);
+    hi = make_float2(ar - u, -ai - v);
 }
 
 // Grid (ceil(1024/30) * C/64, trials), 256 threads.  CTA (wk, g): rows
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     const int k1v = v0 + (int)lane;
     const float2 tv = __ldg(rv + (k1v + 1));
-    const float meanN = stat[3], stdN = stat[4];
+    const float meanN = 2.0f * stat[3], stdN = 2.0f * stat[4];  // of 2X (exact)
     const bool out = lane >= 1 && lane <= 30 && k1v < (int)R;
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
