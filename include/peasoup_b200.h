@@ -516,6 +516,16 @@ typedef struct {
     int last_event_error;   /* cudaError_t of the last such pair */
 } psx_search_profile;
 
+/* Scheduling hint for a server running several instances on one device
+   (no counterpart in the reference, which runs one search per GPU): with
+   `high` set, the instance's kernels go to streams of the device's greatest
+   priority, so that, where two searches share the GPU, its CTAs are
+   scheduled first.  Takes effect at the next DM trial the instance starts;
+   applies to instances on their own streams (not after
+   psx_search_set_stream).  Safe to call from another thread while a search
+   runs. */
+int psx_search_set_priority(psx_search* s, int high);
+
 int psx_search_set_profile(psx_search* s, int on);
 int psx_search_get_profile(psx_search* s, psx_search_profile* out, int reset);
 

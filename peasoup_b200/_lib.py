@@ -163,6 +163,7 @@ SIGNATURES = {
                               C.POINTER(_sz)]),
     "psx_search_last_info": (_i, [_vp, C.POINTER(SearchInfo)]),
     "psx_search_set_profile": (_i, [_vp, _i]),
+    "psx_search_set_priority": (_i, [_vp, _i]),
     "psx_search_get_profile": (_i, [_vp, C.POINTER(SearchProfile), _i]),
     "psx_search_debug_tap": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "psx_autotune": (_i, [C.POINTER(SearchConfig), _vp, _i, _i, _i, _vp]),

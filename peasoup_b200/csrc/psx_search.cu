@@ -509,6 +509,15 @@ struct psx_search {
     cudaStream_t cst = nullptr;  // record copies
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool own_stream = false;
+    // Scheduling priority (a server's hint, psx_search_set_priority): set 0
+    // holds the streams made at creation, set 1 the same streams at the
+    // device's greatest priority (made on first use); the set in use is
+    // swapped at a DM boundary, the new streams waiting for the old ones.
+    cudaStream_t set_st[2] = {nullptr, nullptr}, set_st2[2] = {nullptr, nullptr};
+    cudaStream_t set_pst[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    cudaEvent_t ev_switch[4] = {nullptr, nullptr, nullptr, nullptr};
+    int prio_cur = 0;
+    std::atomic<int> prio_want{0};
     double bin_width = 0.0;
     float bin_width_f = 0.f;
     float tobs = 0.f;
@@ -555,8 +564,29 @@ struct psx_search {
         graphs.clear();
     }
 
+    int apply_priority();
+
     void release()
     {
+        if (prio_cur == 1) {  // back to the creation streams, then drop set 1
+            for (cudaStream_t q : {st, st2, slot[0].pst, slot[1].pst})
+                if (q) cudaStreamSynchronize(q);
+            st = set_st[0];
+            st2 = set_st2[0];
+            slot[0].pst = set_pst[0][0];
+            slot[1].pst = set_pst[0][1];
+            prio_cur = 0;
+        }
+        for (cudaStream_t q : {set_st[1], set_st2[1], set_pst[1][0], set_pst[1][1]})
+            if (q) {
+                cudaStreamSynchronize(q);
+                cudaStreamDestroy(q);
+            }
+        set_st[1] = set_st2[1] = set_pst[1][0] = set_pst[1][1] = nullptr;
+        for (cudaEvent_t& e : ev_switch) {
+            if (e) cudaEventDestroy(e);
+            e = nullptr;
+        }
         if (st) cudaStreamSynchronize(st);
         if (cst) cudaStreamSynchronize(cst);
         drop_graphs();
@@ -655,6 +685,39 @@ int psx_search::get_plan(int b, FftPlan** out, int lane)
     }
     r2cb[lane][b] = p;
     *out = p;
+    return PSX_OK;
+}
+
+// Swaps in the stream set of the wanted priority (at a DM boundary): the
+// new streams first wait for everything queued on the old ones.  Only for
+// an instance that owns its streams.
+int psx_search::apply_priority()
+{
+    const int want = prio_want.load(std::memory_order_relaxed) ? 1 : 0;
+    if (want == prio_cur || !own_stream) return PSX_OK;
+    if (!set_st[1]) {
+        int pri_lo = 0, pri_hi = 0;
+        PSX_CUDA(cudaDeviceGetStreamPriorityRange(&pri_lo, &pri_hi));
+        PSX_CUDA(cudaStreamCreateWithPriority(&set_st[1], cudaStreamNonBlocking, pri_hi));
+        if (set_st2[0])
+            PSX_CUDA(cudaStreamCreateWithPriority(&set_st2[1], cudaStreamNonBlocking, pri_hi));
+        for (int k = 0; k < 2; ++k)
+            PSX_CUDA(cudaStreamCreateWithPriority(&set_pst[1][k], cudaStreamNonBlocking, pri_hi));
+        for (cudaEvent_t& e : ev_switch)
+            if (!e) PSX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t from[4] = {st, st2, slot[0].pst, slot[1].pst};
+    cudaStream_t to[4] = {set_st[want], set_st2[want], set_pst[want][0], set_pst[want][1]};
+    for (int k = 0; k < 4; ++k) {
+        if (!from[k] || !to[k]) continue;
+        PSX_CUDA(cudaEventRecord(ev_switch[k], from[k]));
+        PSX_CUDA(cudaStreamWaitEvent(to[k], ev_switch[k], 0));
+    }
+    st = set_st[want];
+    st2 = set_st2[want];
+    slot[0].pst = set_pst[want][0];
+    slot[1].pst = set_pst[want][1];
+    prio_cur = want;
     return PSX_OK;
 }
 
@@ -978,6 +1041,7 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
                         int dm_idx)
 {
     const psx_search_config& c = cfg;
+    PSX_TRY(apply_priority());
     s.series = series;
     s.nsamps = nsamps;
     s.on_device = on_device;
@@ -1544,6 +1608,9 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->info.harm_shape = s->harm_shape;
     s->info.fft_callback = cb ? 1 : 0;
     s->info.fft_form = effective_form(cfg);
+    s->set_st[0] = s->st;
+    s->set_st2[0] = s->st2;
+    for (int k = 0; k < 2; ++k) s->set_pst[0][k] = s->slot[k].pst;
     *out = s;
     return PSX_OK;
 }
@@ -1666,10 +1733,21 @@ int psx_search_set_stream(psx_search* s, psx_stream_t stream)
 {
     clear_error();
     if (!s) return PSX_ERR_INVALID;
+    // the creation streams first (priorities apply to owned streams only)
+    s->prio_want.store(0);
+    PSX_TRY(s->apply_priority());
     PSX_CUDA(cudaStreamSynchronize(s->st));
     if (s->own_stream) cudaStreamDestroy(s->st);
     s->own_stream = false;
     s->st = cs(stream);
+    s->set_st[0] = s->st;
+    return PSX_OK;
+}
+
+int psx_search_set_priority(psx_search* s, int high)
+{
+    if (!s) return PSX_ERR_INVALID;
+    s->prio_want.store(high ? 1 : 0, std::memory_order_relaxed);
     return PSX_OK;
 }
 

@@ -94,6 +94,19 @@ struct psx_server {
     long long next_id = 1;
     bool stop = false;
     std::vector<std::thread> workers;
+    // Requests running on the device, by admission order: the oldest runs
+    // at the higher stream priority, so a request shares the GPU with a
+    // later one without being slowed by it beyond the gaps it leaves.
+    std::map<long long, psx_search*> running;
+    long long admit_seq = 0;
+    void reprioritise()  // under `mu`
+    {
+        bool first = true;
+        for (auto& r : running) {
+            psx_search_set_priority(r.second, first ? 1 : 0);
+            first = false;
+        }
+    }
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
     void worker();
@@ -158,6 +171,7 @@ void psx_server::worker()
         std::shared_ptr<Request> r;
         Engine eng;
         std::vector<Engine> evict;
+        long long my_seq = 0;
         {
             std::unique_lock<std::mutex> lock(mu);
             for (;;) {
@@ -168,7 +182,10 @@ void psx_server::worker()
                 if (a == 2) continue;
                 cv_work.wait(lock);
             }
-            if (r) r->st.t_admit = now();
+            if (r) {
+                r->st.t_admit = now();
+                my_seq = ++admit_seq;
+            }
         }
         for (Engine& e : evict) psx_search_destroy(e.s);
         evict.clear();
@@ -187,6 +204,11 @@ void psx_server::worker()
             }
         }
         if (!eng.s) rc = psx_search_create(&r->cfg, &eng.s);
+        if (rc == PSX_OK) {
+            std::lock_guard<std::mutex> lock(mu);
+            running[my_seq] = eng.s;
+            reprioritise();
+        }
         if (rc == PSX_OK) {
             psx_search_info info{};
             size_t cap = (size_t)4096 * r->dms.size(), n = 0;
@@ -211,6 +233,8 @@ void psx_server::worker()
         if (rc != PSX_OK) r->error = psx_last_error();
         {
             std::lock_guard<std::mutex> lock(mu);
+            if (running.erase(my_seq)) reprioritise();
+            if (eng.s) psx_search_set_priority(eng.s, 0);  // pooled at the normal level
             if (eng.s) {
                 idle.push_back(eng);
             } else {
