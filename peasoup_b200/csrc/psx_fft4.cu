@@ -1,14 +1,15 @@
 // psx_fft4.cu -- the batched search's forward transform, written for
 // sm_100a: per acceleration trial the complex DFT of length M = N/2 of
 // z[m] = x'[2m] + i x'[2m+1] (x' the resampled series) as a four-step
-// transform M = 1024 * C in two passes over HBM, then the real-spectrum
+// transform M = R * C (R = 1024, or 768 for lengths 3 * 2^k) in two passes
+// over HBM, then the real-spectrum
 // unpack fused with interbinning and normalisation.
 //
 // It replaces, on the batched path, the reference's resample kernel
 // (src/kernels.cu:364-380), its cuFFT R2C call (include/transforms/
 // ffter.hpp:23-53) and the spectrum forming and normalising kernels
 // (src/kernels.cu:238-259, :496-507) with three launches:
-//   pass 1 (k_fft4_cols): CTA = 8 columns c of the 1024 x C matrix
+//   pass 1 (k_fft4_cols): CTA = 8 columns c of the R x C matrix
 //     z[r * C + c], 512 threads; each thread gathers 16 rows of its column
 //     straight from the dereddened series through the resample index (FP64,
 //     the same device function the resample kernel reads through), then Stockham
@@ -17,7 +18,7 @@
 //   pass 2 (k_fft4_rows): CTA = one row k1 (or 256/(C/16) rows) of y,
 //     radix-16 Stockham stages (one radix 2/4/8 stage where C is not a
 //     power of 16) through padded shared memory, written in natural order
-//     as zt[k1 * C + k2] = Z[k1 + 1024 k2];
+//     as zt[k1 * C + k2] = Z[k1 + R k2];
 //   unpack (k_unpack_form_norm_t): a CTA stages a 32-row x 32-column tile of
 //     zt and the tile of its mirror bins through shared memory with
 //     coalesced loads; then lanes take consecutive k1 (30 output lanes and
@@ -123,6 +124,20 @@ __device__ __forceinline__ void dft(float2 (&v)[L])
     unscramble(v, std::make_integer_sequence<int, L>{});
 }
 
+// Forward DFT of length 3: with W = exp(-2 pi i / 3) = -1/2 - i s, s = sqrt(3)/2,
+// X1,2 = a - (b + c)/2 -/+ i s (b - c).
+__device__ __forceinline__ void dft3(float2& a, float2& b, float2& c)
+{
+    constexpr float s3 = 0.866025403784438646763723f;
+    const float2 t1 = make_float2(b.x + c.x, b.y + c.y);
+    const float2 t2 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+    const float2 d = make_float2(b.x - c.x, b.y - c.y);
+    const float2 m = make_float2(s3 * d.y, -s3 * d.x);
+    a = make_float2(a.x + t1.x, a.y + t1.y);
+    b = make_float2(t2.x + m.x, t2.y + m.y);
+    c = make_float2(t2.x - m.x, t2.y - m.y);
+}
+
 // ------------------------------------------------------------- pass 1
 // Shared layout [e][col], e the row index 0..1023; a row of 8 columns is 64
 // bytes.  Flipping bit 0 of e by bit 4 spreads the four rows a warp touches
@@ -130,68 +145,85 @@ __device__ __forceinline__ void dft(float2 (&v)[L])
 // exchange below.
 __device__ __forceinline__ unsigned swz_a(unsigned e) { return e ^ ((e >> 4) & 1u); }
 
+// Column length R = 1024 (stages of radix 16, 16, 4) or 768 (16, 16, 3, for
+// transform lengths 3 * 2^k); 64 threads per column, of which R/16 take the
+// radix-16 stages and all take 4 butterflies of the last stage.
 // DUMP: write the gathered pairs z[e C + c] (the resampled series as it is
 // read, interleaved) to y instead of transforming them (the debug tap).
-template <bool DUMP>
+template <int R, bool DUMP>
 __global__ void __launch_bounds__(kColsW * 64, 2)
     k_fft4_cols(const float* __restrict__ x, unsigned long long n, const double* __restrict__ ktab,
                 const float2* __restrict__ tab, unsigned offA2, unsigned offA3, unsigned offQ,
                 unsigned offP, unsigned C, float2* __restrict__ y, size_t ypitch)
 {
+    static_assert(R == 1024 || R == 768, "column length");
     constexpr int W = kColsW;
+    constexpr int J = R / 16;   // radix-16 butterflies per column and stage
+    constexpr int R3 = R / 256;  // radix of the last stage
     extern __shared__ float2 sm_a[];
     const unsigned col = threadIdx.x % W, t = threadIdx.x / W;  // t in [0, 64)
     const unsigned c = blockIdx.x * W + col;
     const double k = ktab[blockIdx.y], size = (double)n;
     float2 v[16];
-    // stage 1 (radix 16, span 1): rows e = t + 64 q of column c, where
+    // stage 1 (radix 16, span 1): rows e = t + J q of column c, where
     // z[e C + c] = (x'[2m], x'[2m+1]); out[16 t + q]
-    const double i_first = 2.0 * ((double)t * (double)C + (double)c);
-    const double i_step = 128.0 * (double)C;
-    const unsigned n32 = (unsigned)n;
+    if (J == 64 || t < (unsigned)J) {  // every thread when R = 1024
+        const double i_first = 2.0 * ((double)t * (double)C + (double)c);
+        const double i_step = 2.0 * J * (double)C;
+        const unsigned n32 = (unsigned)n;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        const double i0 = i_first + (double)q * i_step;  // exact: integers < 2^26
-        v[q].x = resampleII_read(x, i0, k, size, n32);
-        v[q].y = resampleII_read(x, i0 + 1.0, k, size, n32);
+        for (int q = 0; q < 16; ++q) {
+            const double i0 = i_first + (double)q * i_step;  // exact: integers < 2^26
+            v[q].x = resampleII_read(x, i0, k, size, n32);
+            v[q].y = resampleII_read(x, i0 + 1.0, k, size, n32);
+        }
+        if constexpr (DUMP) {
+            float2* yo = y + (size_t)blockIdx.y * ypitch;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) yo[(size_t)(t + J * q) * C + c] = v[q];
+        } else {
+            dft<16>(v);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) sm_a[swz_a(16 * t + q) * W + col] = v[q];
+        }
     }
-    if constexpr (DUMP) {
-        float2* yo = y + (size_t)blockIdx.y * ypitch;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) yo[(size_t)(t + 64 * q) * C + c] = v[q];
-        return;
-    }
-    dft<16>(v);
-#pragma unroll
-    for (int q = 0; q < 16; ++q) sm_a[swz_a(16 * t + q) * W + col] = v[q];
+    if constexpr (DUMP) return;
     __syncthreads();
-    // stage 2 (radix 16, span 16): in[t + 64 q] * W_256^((t mod 16) q),
+    // stage 2 (radix 16, span 16): in[t + J q] * W_256^((t mod 16) q),
     // out[(t / 16) 256 + t mod 16 + 16 q]
+    if (J == 64 || t < (unsigned)J) {  // every thread when R = 1024
 #pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = sm_a[swz_a(t + 64 * q) * W + col];
+        for (int q = 0; q < 16; ++q) v[q] = sm_a[swz_a(t + J * q) * W + col];
+    }
     __syncthreads();
+    if (J == 64 || t < (unsigned)J) {  // every thread when R = 1024
 #pragma unroll
-    for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], __ldg(tab + offA2 + q * 16 + (t & 15)));
-    dft<16>(v);
-    const unsigned base2 = (t >> 4) * 256 + (t & 15);
+        for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], __ldg(tab + offA2 + q * 16 + (t & 15)));
+        dft<16>(v);
+        const unsigned base2 = (t >> 4) * 256 + (t & 15);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) sm_a[swz_a(base2 + 16 * q) * W + col] = v[q];
+        for (int q = 0; q < 16; ++q) sm_a[swz_a(base2 + 16 * q) * W + col] = v[q];
+    }
     __syncthreads();
-    // stage 3 (radix 4, span 256): butterflies j = t + 64 u, in[j + 256 q]
-    // * W_1024^(j q), out[j + 256 q] = row k1 = t + 64 (u + 4 q)
+    // stage 3 (radix R3, span 256): butterflies j = t + 64 u, in[j + 256 q]
+    // * W_R^(j q), out[j + 256 q] = row k1 = t + 64 (u + 4 q)
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) v[4 * u + q] = sm_a[swz_a(t + 64 * u + 256 * q) * W + col];
+        for (int q = 0; q < R3; ++q) v[4 * u + q] = sm_a[swz_a(t + 64 * u + 256 * q) * W + col];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
         float2 b[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < R3; ++q)
             b[q] = q ? cmul(v[4 * u + q], __ldg(tab + offA3 + q * 256 + t + 64 * u)) : v[4 * u];
-        dft<4>(b);
+        if constexpr (R3 == 4) {
+            dft<4>(b);
+        } else {
+            dft3(b[0], b[1], b[2]);
+        }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) v[4 * u + q] = b[q];
+        for (int q = 0; q < R3; ++q) v[4 * u + q] = b[q];
     }
     // four-step twiddle W_M^(c k1), k1 = t + 64 w (w = u + 4 q):
     // W_M^(c t) * W_M^(64 c w)
@@ -200,7 +232,7 @@ __global__ void __launch_bounds__(kColsW * 64, 2)
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < R3; ++q) {
             const unsigned w = u + 4 * q;
             const float2 tw = w ? cmul(wt, __ldg(tab + offP + (size_t)w * C + c)) : wt;
             yo[(size_t)(t + 64 * w) * C + c] = cmul(v[4 * u + q], tw);
@@ -284,9 +316,10 @@ __global__ void __launch_bounds__(RowShape<LOGC>::THREADS, 1024 / RowShape<LOGC>
 }
 
 // ------------------------------------------------------------- unpack
+template <unsigned R>
 __device__ __forceinline__ float2 zt_at(const float2* __restrict__ z, unsigned C, unsigned idx)
 {
-    return z[(size_t)(idx & (kFft4Rows - 1)) * C + (idx >> 10)];
+    return z[(size_t)(idx % R) * C + (idx / R)];
 }
 
 // 2 X[j] and 2 X[M-j] of the real series from Z[j] = a and Z[M-j] = w,
@@ -305,10 +338,11 @@ __device__ __forceinline__ void unpack_one(float2 a, float2 w, float cs, float s
     hi = make_float2(ar - u, -ai - v);
 }
 
-// Grid (ceil(1024/30) * C/64, trials), 256 threads.  CTA (wk, g): rows
-// k1 = 30 wk - 1 + r, r < 32 ("virtual" rows -1 and >= 1024 continue into
+// Grid (ceil(R/30) * C/64, trials), 256 threads, R the row count of the
+// four-step split (1024 or 768).  CTA (wk, g): rows
+// k1 = 30 wk - 1 + r, r < 32 ("virtual" rows -1 and >= R continue into
 // the neighbouring columns), columns k2 = 32 g .. 32 g + 31 < C/2: the bins
-// j = k1 + 1024 k2 < M/2 and their mirrors M - j.  Both 32 x 32 tiles are
+// j = k1 + R k2 < M/2 and their mirrors M - j.  Both 32 x 32 tiles are
 // loaded coalesced (a warp reads 32 consecutive columns of a row) into
 // padded shared memory; warp w then takes columns 32 g + 4 w .. + 3 with
 // lane = r, and lanes 1..30 write bin j (interbinned with lane-1's X[j-1])
@@ -316,13 +350,13 @@ __device__ __forceinline__ void unpack_one(float2 a, float2 w, float cs, float s
 // block 0.  The split-step rotation (cos, sin)(pi j / M) is the product of
 // tabulated (cos, sin)(pi k1 / M) (k1 = -1 .. 1055, rv[k1 + 1]) and
 // (cos, sin)(pi k2 / C) (rk[k2]).
+template <unsigned R>
 __global__ void __launch_bounds__(256)
     k_unpack_form_norm_t(const float2* __restrict__ zt, size_t zpitch, unsigned C,
-                         float* __restrict__ p, size_t ppitch, float inv_m,
+                         float* __restrict__ p, size_t ppitch,
                          const float2* __restrict__ rv, const float2* __restrict__ rk,
                          const float* __restrict__ stat)
 {
-    constexpr unsigned R = kFft4Rows;
     __shared__ float2 lo_t[32][33], mi_t[32][33];
     const unsigned M = R * C;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -348,8 +382,8 @@ __global__ void __launch_bounds__(256)
         float2 a = make_float2(0.f, 0.f), w = a;  // X[-1] := 0
         if (j >= 0) {
             const unsigned jj = (unsigned)j;
-            a = zt_at(z, C, jj);
-            w = zt_at(z, C, jj ? M - jj : 0u);
+            a = zt_at<R>(z, C, jj);
+            w = zt_at<R>(z, C, jj ? M - jj : 0u);
         }
         lo_t[r][lane] = a;
         mi_t[r][lane] = w;
@@ -378,13 +412,12 @@ __global__ void __launch_bounds__(256)
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // bin M/2 with bin M/2 - 1
+        // (cos, sin)(pi/2) = (0, 1); (cos, sin)(pi/2 - pi/M) = (sin, cos)(pi/M)
         const unsigned jh = M / 2;
+        const float2 r1 = __ldg(rv + 2);  // (cos, sin)(pi / M)
         float2 x0, x1, unused;
-        float s, c;
-        sincospif((float)jh * inv_m, &s, &c);
-        unpack_one(zt_at(z, C, jh), zt_at(z, C, M - jh), c, s, x0, unused);
-        sincospif((float)(jh - 1) * inv_m, &s, &c);
-        unpack_one(zt_at(z, C, jh - 1), zt_at(z, C, M - jh + 1), c, s, x1, unused);
+        unpack_one(zt_at<R>(z, C, jh), zt_at<R>(z, C, M - jh), 0.0f, 1.0f, x0, unused);
+        unpack_one(zt_at<R>(z, C, jh - 1), zt_at<R>(z, C, M - jh + 1), r1.y, r1.x, x1, unused);
         o[jh] = normalise(interbin(x0.x, x0.y, x1.x, x1.y), meanN, stdN);
     }
 }
@@ -401,11 +434,11 @@ int configure_rows()
 }
 
 template <int LOGC>
-int launch_rows(const float2* y, size_t ypitch, float2* zt, size_t zpitch, const float2* tw,
-                int ntrials, cudaStream_t s)
+int launch_rows(unsigned nrows, const float2* y, size_t ypitch, float2* zt, size_t zpitch,
+                const float2* tw, int ntrials, cudaStream_t s)
 {
     using S = RowShape<LOGC>;
-    dim3 grid(kFft4Rows / S::RPC, (unsigned)ntrials);
+    dim3 grid(nrows / S::RPC, (unsigned)ntrials);
     k_fft4_rows<LOGC><<<grid, S::THREADS, S::SMEM, s>>>(y, ypitch, zt, zpitch, tw);
     return launch_status("fft4 row pass");
 }
@@ -429,7 +462,9 @@ void row_stages(int logc, std::vector<std::pair<int, int>>& out)
 
 bool Fft4Plan::supported(size_t n)
 {
-    return n >= (size_t(1) << 19) && n <= (size_t(1) << 25) && (n & (n - 1)) == 0;
+    auto pow2 = [](size_t v) { return v && (v & (v - 1)) == 0; };
+    if (pow2(n)) return n >= (size_t(1) << 19) && n <= (size_t(1) << 25);
+    return n % 3 == 0 && pow2(n / 3) && n / 3 >= (size_t(1) << 17) && n / 3 <= (size_t(1) << 23);
 }
 
 void Fft4Plan::destroy()
@@ -444,11 +479,13 @@ int Fft4Plan::create(size_t n_)
 {
     destroy();
     if (!supported(n_)) {
-        set_error("fft4: unsupported length %zu (powers of two 2^19 .. 2^25)", n_);
+        set_error("fft4: unsupported length %zu (2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23)", n_);
         return PSX_ERR_INVALID;
     }
     const unsigned long long M = n_ / 2;
-    const unsigned Cn = (unsigned)(M / kFft4Rows);
+    const unsigned Rn = (n_ % 3 == 0) ? 768u : 1024u;
+    const unsigned R3 = Rn / 256;
+    const unsigned Cn = (unsigned)(M / Rn);
     const double two_pi = 6.283185307179586476925286766559;
     // W_L^e = exp(-2 pi i e / L), rounded once from double
     auto W = [&](unsigned long long e, unsigned long long L) {
@@ -461,14 +498,14 @@ int Fft4Plan::create(size_t n_)
     offA2 = 0;  // [q * 16 + m] = W_256^(m q)
     for (unsigned q = 0; q < 16; ++q)
         for (unsigned m = 0; m < 16; ++m) h.push_back(W((unsigned long long)m * q, 256));
-    offA3 = (unsigned)h.size();  // [q * 256 + j] = W_1024^(j q)
-    for (unsigned q = 0; q < 4; ++q)
-        for (unsigned j = 0; j < 256; ++j) h.push_back(W((unsigned long long)j * q, 1024));
+    offA3 = (unsigned)h.size();  // [q * 256 + j] = W_R^(j q)
+    for (unsigned q = 0; q < R3; ++q)
+        for (unsigned j = 0; j < 256; ++j) h.push_back(W((unsigned long long)j * q, Rn));
     offQ = (unsigned)h.size();  // [t * C + c] = W_M^(c t)
     for (unsigned t = 0; t < 64; ++t)
         for (unsigned c = 0; c < Cn; ++c) h.push_back(W((unsigned long long)c * t, M));
     offP = (unsigned)h.size();  // [w * C + c] = W_M^(64 c w)
-    for (unsigned w = 0; w < 16; ++w)
+    for (unsigned w = 0; w < 4 * R3; ++w)
         for (unsigned c = 0; c < Cn; ++c) h.push_back(W(64ull * c * w, M));
     // unpack rotations (cos, sin)(pi k1 / M), k1 = -1 .. 1055, and (pi k2 / C)
     const double pi = two_pi / 2;
@@ -493,13 +530,18 @@ int Fft4Plan::create(size_t n_)
     PSX_CUDA(cudaMemcpy(d_tab, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
     n = n_;
     C = Cn;
+    R = Rn;
     logc = lc;
     // (the default shared/L1 split: measured on B200, forcing the largest
     // shared carve-out slowed the gather of pass 1 and the twiddle reads of
     // pass 2, both served from L1)
-    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<false>,
+    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<1024, false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(kFft4Rows * kColsW * sizeof(float2))),
+                                             (int)(1024 * kColsW * sizeof(float2))),
+                        "fft4 column pass attribute"));
+    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<768, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(768 * kColsW * sizeof(float2))),
                         "fft4 column pass attribute"));
 
     switch (logc) {
@@ -531,8 +573,12 @@ int Fft4Plan::exec_cols(const float* series, const double* ktab, int ntrials, fl
         return PSX_ERR_INVALID;
     }
     dim3 ga(C / kColsW, (unsigned)ntrials);
-    k_fft4_cols<false><<<ga, kColsW * 64, kFft4Rows * kColsW * sizeof(float2), s>>>(
-        series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
+    if (R == 768)
+        k_fft4_cols<768, false><<<ga, kColsW * 64, 768 * kColsW * sizeof(float2), s>>>(
+            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
+    else
+        k_fft4_cols<1024, false><<<ga, kColsW * 64, 1024 * kColsW * sizeof(float2), s>>>(
+            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
     return launch_status("fft4 column pass");
 }
 
@@ -544,9 +590,14 @@ int Fft4Plan::dump_gather(const float* series, const double* ktab, float* out,
         return PSX_ERR_INVALID;
     }
     dim3 ga(C / kColsW, 1);
-    k_fft4_cols<true><<<ga, kColsW * 64, 0, s>>>(series, (unsigned long long)n, ktab, d_tab,
-                                                 offA2, offA3, offQ, offP, C,
-                                                 reinterpret_cast<float2*>(out), n / 2);
+    if (R == 768)
+        k_fft4_cols<768, true><<<ga, kColsW * 64, 0, s>>>(
+            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C,
+            reinterpret_cast<float2*>(out), n / 2);
+    else
+        k_fft4_cols<1024, true><<<ga, kColsW * 64, 0, s>>>(
+            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C,
+            reinterpret_cast<float2*>(out), n / 2);
     return launch_status("fft4 gather dump");
 }
 
@@ -560,13 +611,13 @@ int Fft4Plan::exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt,
     }
     const float2* tw = d_tab + offB;
     switch (logc) {
-    case 8: return launch_rows<8>(y, ypitch, zt, zpitch, tw, ntrials, s);
-    case 9: return launch_rows<9>(y, ypitch, zt, zpitch, tw, ntrials, s);
-    case 10: return launch_rows<10>(y, ypitch, zt, zpitch, tw, ntrials, s);
-    case 11: return launch_rows<11>(y, ypitch, zt, zpitch, tw, ntrials, s);
-    case 12: return launch_rows<12>(y, ypitch, zt, zpitch, tw, ntrials, s);
-    case 13: return launch_rows<13>(y, ypitch, zt, zpitch, tw, ntrials, s);
-    case 14: return launch_rows<14>(y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 8: return launch_rows<8>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 9: return launch_rows<9>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 10: return launch_rows<10>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 11: return launch_rows<11>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 12: return launch_rows<12>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 13: return launch_rows<13>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
+    case 14: return launch_rows<14>(R, y, ypitch, zt, zpitch, tw, ntrials, s);
     default: break;
     }
     set_error("fft4: row length 2^%d out of range", logc);
@@ -581,11 +632,14 @@ int Fft4Plan::form(const float2* zt, size_t zpitch, int ntrials, float* p, size_
         set_error("fft4 form: bad arguments");
         return PSX_ERR_INVALID;
     }
-    const unsigned nck = (kFft4Rows + 29) / 30;
+    const unsigned nck = (R + 29) / 30;
     dim3 grid(nck * (C / 64), (unsigned)ntrials);
-    const float inv_m = 1.0f / (float)(n / 2);
-    k_unpack_form_norm_t<<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, inv_m, d_tab + offRv,
-                                              d_tab + offRk, stat);
+    if (R == 768)
+        k_unpack_form_norm_t<768><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch,
+                                                       d_tab + offRv, d_tab + offRk, stat);
+    else
+        k_unpack_form_norm_t<1024><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch,
+                                                        d_tab + offRv, d_tab + offRk, stat);
     return launch_status("fft4 unpack kernel");
 }
 

@@ -1,27 +1,27 @@
 // psx_fft4.cuh -- the batched search's own forward transform: for each
 // acceleration trial, the complex DFT of length M = N/2 of the resampled
 // series read as interleaved pairs, z[m] = x'[2m] + i x'[2m+1], in two
-// passes over HBM (four-step split M = 1024 * C), with the resample gather
-// done by the first pass's loads; and the unpack + interbin + normalise
-// pass that reads its transposed output.
+// passes over HBM (four-step split M = R * C, R = 1024 or 768), with the
+// resample gather done by the first pass's loads; and the unpack +
+// interbin + normalise pass that reads its transposed output.
 #pragma once
 #include <cuda_runtime.h>
 #include <cstddef>
 
 namespace psx {
 
-// Rows of the four-step split (the first pass's column length).
-constexpr unsigned kFft4Rows = 1024;
 
 struct Fft4Plan {
     size_t n = 0;      // real samples N
-    unsigned C = 0;    // row length of the second pass (M / 1024)
+    unsigned R = 1024; // rows of the four-step split: 1024, or 768 for 3 * 2^k
+    unsigned C = 0;    // row length of the second pass (M / R)
     int logc = 0;
     float2* d_tab = nullptr;  // twiddle tables (offsets below, in float2)
     size_t tab_len = 0;
     unsigned offA2 = 0, offA3 = 0, offQ = 0, offP = 0, offB = 0, offRv = 0, offRk = 0;
 
-    // N = 2^19 .. 2^25 (C = 2^8 .. 2^14).
+    // N = 2^19 .. 2^25 (R = 1024) or 3 * 2^17 .. 3 * 2^23 (R = 768), i.e.
+    // C = 2^8 .. 2^14.
     static bool supported(size_t n);
     int create(size_t n);
     void destroy();
@@ -30,7 +30,7 @@ struct Fft4Plan {
     // ntrials transforms: trial t gathers series[resampleII index of
     // ktab[t]] (the resampleII read index in FP64, as the resample kernel
     // forms it) and leaves Z = DFT_M(z) transposed:
-    //   zt[t * zpitch + k1 * C + k2] = Z[k1 + 1024 * k2].
+    //   zt[t * zpitch + k1 * C + k2] = Z[k1 + R * k2].
     // y (ypitch complex elements per trial, >= M) holds the intermediate.
     int exec(const float* series, const double* ktab, int ntrials, float2* y, size_t ypitch,
              float2* zt, size_t zpitch, cudaStream_t s) const;

@@ -1339,7 +1339,7 @@ static int check_config(const psx_search_config* c)
     if (c->fft_form == 3 && (c->mode != PSX_MODE_BATCHED || c->use_fft_callback ||
                              !Fft4Plan::supported(c->fft_size))) {
         set_error("search: fft_form 3 needs the batched mode without the cuFFT callback and "
-                  "fft_size a power of two from 2^19 to 2^25");
+                  "fft_size 2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23");
         return PSX_ERR_INVALID;
     }
     if (c->lanes < 0 || c->lanes > 2) {

@@ -52,8 +52,10 @@ def test_invalid_arguments_fail_loudly(psx):
     cfg.nharmonics = 6
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
     assert b"nharmonics" in psx.psx_last_error()
-    # the library's own transform: batched, no cuFFT callback, 2^19 .. 2^25 points
-    for n, mode, cb in ((1 << 16, _lib.PSX_MODE_BATCHED, 0), (3 << 18, _lib.PSX_MODE_BATCHED, 0),
+    # the library's own transform: batched, no cuFFT callback, 2^19 .. 2^25 or
+    # 3 * 2^17 .. 3 * 2^23 points
+    for n, mode, cb in ((1 << 16, _lib.PSX_MODE_BATCHED, 0), (3 << 16, _lib.PSX_MODE_BATCHED, 0),
+                        (3 << 24, _lib.PSX_MODE_BATCHED, 0),
                         (1 << 26, _lib.PSX_MODE_BATCHED, 0), (1 << 20, _lib.PSX_MODE_PLAIN, 0),
                         (1 << 20, _lib.PSX_MODE_BATCHED, 1)):
         psx.psx_search_config_defaults(C.byref(cfg), n, 64e-6)

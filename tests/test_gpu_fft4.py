@@ -5,7 +5,7 @@ interleaved pairs, then the unpack + interbin + normalise kernel):
   * the normalised interbinned spectrum of tapped trials against FP64
     (numpy's real transform of the same resampled series) within 1e-5
     relative, |a - b| <= 1e-5 (|b| + RMS), at every row length the two
-    passes support;
+    passes support and for both row counts (1024, and 768 for 3 * 2^k);
   * candidate lists identical to cuFFT's complex transform (fft_form 1) and
     to the reference's real transform (plain mode), S/N within 1e-5.
 """
@@ -40,10 +40,12 @@ def _fp64_spectrum(tim, idx, norm2):
     return (amp - float(norm2[0])) / float(norm2[1])
 
 
-@pytest.mark.parametrize("logn", [19, 20, 21, 22, 23, 24, 25])
-def test_spectrum_vs_fp64(S, oracle, logn):
+@pytest.mark.parametrize("n", [1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25,
+                               3 << 17, 3 << 20, 3 << 23])
+def test_spectrum_vs_fp64(S, oracle, n):
     search, synth = S
-    n, ts = 1 << logn, 64e-6
+    ts = 64e-6
+    logn = n.bit_length()
     x = synth.make_series_np(synth.SeriesSpec(
         nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(4.1e-3, 35.0, 0.04, 0.5)]), logn)
     s = search.AccelSearch(_params(S, n, ts, batch=4, acc_lo=-40.0, acc_hi=40.0,
@@ -62,7 +64,7 @@ def test_spectrum_vs_fp64(S, oracle, logn):
     s.close()
 
 
-@pytest.mark.parametrize("n", [1 << 20, 1 << 22])
+@pytest.mark.parametrize("n", [1 << 20, 1 << 22, 3 << 20])
 def test_candidates_match_cufft_paths(S, n):
     search, synth = S
     ts = 64e-6
@@ -87,7 +89,7 @@ def test_candidates_match_cufft_paths(S, n):
 def test_default_form_by_size(S):
     search, synth = S
     ts = 64e-6
-    for n, want in ((1 << 16, 1), (3 << 18, 1), (1 << 19, 3)):
+    for n, want in ((1 << 16, 1), (3 << 16, 1), (1 << 19, 3), (3 << 17, 3)):
         s = search.AccelSearch(_params(S, n, ts, batch=2, acc_lo=-1.0, acc_hi=1.0,
                                        nharmonics=1, min_snr=9.0))
         s.search(synth.make_series_np(synth.SeriesSpec(nsamps=n, tsamp=ts), 2), 0.0, 0,
@@ -96,7 +98,7 @@ def test_default_form_by_size(S):
         s.close()
 
 
-@pytest.mark.parametrize("n", [1 << 19, 1 << 22])
+@pytest.mark.parametrize("n", [1 << 19, 1 << 22, 3 << 19])
 def test_gathered_series_bit_exact(S, oracle, n):
     """What pass 1 gathers (dumped by the debug tap instead of transformed)
     is the resampled series, bit for bit, against the oracle's FP64 index on
