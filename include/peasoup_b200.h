@@ -403,7 +403,8 @@ typedef struct {
                                   3 = the library's own two-pass transform of
                                   the interleaved pairs with the resample
                                   gather in its first pass, then the unpack
-                                  kernel (fft_size 2^19 .. 2^25) */
+                                  kernel (fft_size 2^19 .. 2^25 or
+                                  3 * 2^17 .. 3 * 2^23) */
 } psx_search_config;
 
 /* Number of tile shapes of the fused harmonic-sum kernel (tile bins,

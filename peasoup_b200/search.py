@@ -58,7 +58,7 @@ class SearchParams:
     graph: bool = True             # batched: CUDA-graph trial schedule
     harm_shape: int = 0            # harmonic-kernel tile shape (0 = default)
     lanes: int = 0                 # batched: streams the launch groups alternate over (0 = 1)
-    fft_form: int = 0              # batched: 0 default (3 for 2^19..2^25 points, else 1),
+    fft_form: int = 0              # batched: 0 default (3 for 2^19..2^25, 3*2^17..3*2^23, else 1),
                                    # 1 cuFFT complex transform + fused unpack/interbin,
                                    # 2 the reference's real transform + interbin,
                                    # 3 the library's two-pass transform (resample in pass 1)
