@@ -130,3 +130,26 @@ def test_binding_constants_match_header():
     hdr = open(os.path.join(os.path.dirname(_lib.LIB_PATH), "..", "include",
                             "peasoup_b200.h")).read()
     assert int(re.search(r"#define PSX_HARM_SHAPES (\d+)", hdr).group(1)) == _lib.PSX_HARM_SHAPES
+
+
+def test_two_pass_transform_lengths(psx):
+    """Host rule of the two-pass transform (fft_form 3): batched mode,
+    2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23 points; a configuration outside it
+    has no footprint (it is rejected before any device work)."""
+    cfg = _lib.SearchConfig()
+    ok = [1 << 19, 1 << 23, 1 << 25, 3 << 17, 3 << 20, 3 << 23]
+    bad = [1 << 18, 1 << 26, 3 << 16, 3 << 24, 5 << 20, 1000]
+    for n in ok + bad:
+        psx.psx_search_config_defaults(C.byref(cfg), n, 64e-6)
+        cfg.mode, cfg.fft_form = _lib.PSX_MODE_BATCHED, 3
+        fp = psx.psx_search_footprint(C.byref(cfg))
+        assert (fp > 0) == (n in ok), (n, fp)
+    # the default form picks it where it applies, and the footprint then has
+    # no batched cuFFT work areas
+    psx.psx_search_config_defaults(C.byref(cfg), 1 << 23, 64e-6)
+    cfg.mode, cfg.batch = _lib.PSX_MODE_BATCHED, 32
+    cfg.fft_form = 0
+    own = psx.psx_search_footprint(C.byref(cfg))
+    cfg.fft_form = 1
+    lib = psx.psx_search_footprint(C.byref(cfg))
+    assert 0 < own < lib
