@@ -142,8 +142,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase)
 }
 
 // Global -> shared bulk copy of `bytes` (multiple of 16, both addresses
-// 16-byte aligned), completing as transaction bytes on `bar`.  Not
-// multicast: the destination is this CTA's own shared memory.
+// 16-byte aligned), completing as transaction bytes on `bar`.  The
+// destination is this CTA's own shared memory only.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
                                          uint64_t* bar)
 {
@@ -586,8 +586,8 @@ __device__ __noinline__ void exact_pass_rows_ool(const float* __restrict__ sm, u
 }
 
 // 2D tensor copy of the box at element coordinates (x, y) of `map` into
-// this CTA's shared memory, completing as transaction bytes on `bar`.  Not
-// multicast.
+// this CTA's own shared memory only, completing as transaction bytes on
+// `bar`.
 __device__ __forceinline__ void tensor_g2s_2d(void* dst, const CUtensorMap* map, int x, int y,
                                               uint64_t* bar)
 {
