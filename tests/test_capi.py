@@ -64,6 +64,7 @@ def test_invalid_arguments_fail_loudly(psx):
         assert b"fft_form 3" in psx.psx_last_error()
     cfg.fft_form = 4
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
+    assert psx.psx_search_set_priority(None, 1) == _lib.PSX_ERR_INVALID
 
 
 def test_no_cpu_fallback_without_device(psx):
