@@ -196,59 +196,128 @@ def make_params(plan, mode="batched", batch=0, harm_shape=0):
 
 
 # ----------------------------------------------------------------- reference
+def _standalone(name):
+    """peasoup_b200/<name>.py loaded as a module of its own, without the
+    package (whose library the reference arm must not load).  Used for the
+    pure numpy/torch modules: the synthetic workload and the DM schedule."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        f"_bench_{name}", os.path.join(ROOT, "peasoup_b200", f"{name}.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _mapped_native_libraries():
+    """Shared libraries of this repository mapped into the process."""
+    seen = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.startswith(ROOT) and ".so" in path:
+                    seen.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(seen)
+
+
 def run_reference(args, ws, rank):
+    """The reference's own implementation of the path on the same workload:
+    its src/kernels.cu, transform classes and unmodified Worker::start,
+    built for sm_100a into oracle/_ref, over exactly the DM trials and
+    series of the --impl psx arm's timed steps (same seeds, same schedule,
+    same zap list).  As in the reference's program, one Worker searches the
+    whole DM list (its set-up of plans and buffers once, then DM trial by
+    DM trial, host->device copy of each series included); the time is that
+    of Worker::start.  Trials are counted with the reference's own
+    AccelerationPlan (oracle/_ref host build).  Nothing of this
+    repository's library is loaded in this process."""
     if rank != 0:
         return 0
     from oracle import oracle as O
-    if not os.path.exists(O.REF_GPU_PATH):
+    if not (os.path.exists(O.REF_GPU_PATH) and os.path.exists(O.REF_HOST_PATH)):
         print(json.dumps({"impl": "reference", "metric": METRIC,
-                          "unavailable": "oracle/_ref/libpeasoup_ref_gpu.so not built "
-                                         "(build() compiles it where the reference sources "
+                          "unavailable": "oracle/_ref libraries not built "
+                                         "(build() compiles them where the reference sources "
                                          "exist)"}), flush=True)
         return 0
+    import ctypes as C
     import torch
-    from peasoup_b200 import synth
+    synth = _standalone("synth")
+    repl = _standalone("replicas")
+    S = args.dms_per_step
     plan = synth.survey_plan(ndm=NDM, nsamps=N_FFT, tsamp=TSAMP)
-    sched = dm_schedule(0, 1, args.warmup + args.steps, 1)
-    dmsel = sorted({d for st in sched for d in st})
-    block = synth.survey_block_torch(plan, dm_indices=dmsel)
-    host = {d: block[i].cpu().numpy() for i, d in enumerate(dmsel)}
-    del block
-    torch.cuda.empty_cache()
+    # the schedule and the synthesis calls of the psx arm at one rank
+    warm = repl.dm_schedule(NDM, 0, 1, args.warmup, S, args.steps)
+    timed = repl.dm_schedule(NDM, 0, 1, args.steps, S)
+    need = sorted({d for st in warm + timed for d in st})
+    block = synth.survey_block_torch(plan, dm_indices=need)
+    row = {d: i for i, d in enumerate(need)}
     p = O.SearchParams(fft_size=N_FFT, tsamp=TSAMP, acc_lo=-ACC, acc_hi=ACC, nharmonics=NFOLDS,
                        cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ)
+    warm_dms = [d for st in warm for d in st]
+    timed_dms = [d for st in timed for d in st]
+    L = O.ref_gpu()
+    L.ref_worker_search_timed.restype = C.c_int
+    a = O._RefArgs(p.cdm, p.acc_lo, p.acc_hi, p.acc_tol, p.acc_pulse_width * 1e6, p.cfreq,
+                   p.ch_bw, p.nharmonics, p.min_snr, p.min_freq, p.max_freq, int(p.max_harm),
+                   p.freq_tol, b"")
     fd, zap = tempfile.mkstemp(suffix=".txt")
     with os.fdopen(fd, "w") as f:
         f.write(plan.zaplist_text())
+    a.zapfile = zap.encode()
+
+    def worker(dm_list):
+        rows = torch.stack([block[row[d]] for d in dm_list]).cpu().numpy()
+        cap = 1 << 20
+        out = np.zeros(cap, O.CAND_DTYPE)
+        na = np.zeros(cap, np.int32)
+        n = C.c_size_t()
+        sec = C.c_double()
+        dms = np.ascontiguousarray(plan.dms[dm_list], np.float32)
+        rc = L.ref_worker_search_timed(rows.ctypes.data_as(C.c_void_p), C.c_size_t(len(dm_list)),
+                                       C.c_size_t(N_FFT), C.c_float(TSAMP),
+                                       dms.ctypes.data_as(C.c_void_p), C.c_size_t(N_FFT),
+                                       C.byref(a), out.ctypes.data_as(C.c_void_p),
+                                       na.ctypes.data_as(C.c_void_p), C.c_size_t(cap),
+                                       C.byref(n), C.byref(sec))
+        if rc != 0:
+            raise RuntimeError(f"reference Worker failed with status {rc}")
+        return sec.value, int(n.value)
+
     try:
-        for st in sched[:args.warmup]:
-            d = st[0]
-            O.ref_worker_search(host[d][None, :], TSAMP, plan.dms[d:d + 1], N_FFT, p, zap)
+        worker(warm_dms)
         torch.cuda.synchronize()
-        ntr = 0
-        t0 = time.perf_counter()
-        for st in sched[args.warmup:]:
-            d = st[0]
-            O.ref_worker_search(host[d][None, :], TSAMP, plan.dms[d:d + 1], N_FFT, p, zap)
-            ntr += trials_of(plan, [d])
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
+        dt, ncand = worker(timed_dms)
     finally:
         os.unlink(zap)
+    ntr = 0
+    for d in timed_dms:
+        ntr += len(O.ref_accel_list(-ACC, ACC, 1.10, 64e-6, N_FFT, TSAMP, synth.CFREQ_HZ,
+                                    synth.CH_BW_HZ, float(plan.dms[d]), 0.0))
     v = ntr / dt
-    sample = (f"{args.steps} DM trials of the survey workload (one per step, "
-              f"{ntr} acceleration trials), reference kernels.cu + unmodified Worker on the GPU")
+    loaded = _mapped_native_libraries()
+    sample = (f"{len(timed_dms)} DM trials of the survey workload ({ntr} acceleration trials; "
+              f"the --impl psx arm's timed DM trials), the reference's kernels.cu + transforms + "
+              f"unmodified Worker::start built for sm_100a, one host thread driving cuda:0 (the "
+              f"reference has no CPU implementation of this path)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "trials/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dt / max(1, args.steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "survey-2^23 (256 DM x 2^23, tsamp 76us, acc +-100, 5 folds, "
-                               "20 birdies)", "dms_per_step": 1},
+        "config": {"workload": "survey-2^23: 256 DM trials x 2^23 samples, tsamp 76us, "
+                               "acc -100..100, 5 folds, S/N 9, 20 birdies zapped",
+                   "dms_per_step": S, "dm_trials": timed_dms[:1] + timed_dms[-1:],
+                   "same_config_as_psx_arm": True,
+                   "l2": "inputs larger than L2 (32 MB series per DM trial)"},
+        "trials": ntr, "candidates": ncand,
         "cpu_baseline": {"value": v, "unit": "trials/s", "cores": 1, "kind": "reference",
-                         "sample": sample},
+                         "runs_on": "cuda:0", "sample": sample},
         "e2e": {"value": v, "unit": "trials/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "native_libraries_loaded": loaded,
     }), flush=True)
     return 0
 
@@ -847,6 +916,37 @@ def run_psx(args, ws, rank, local):
     return 0
 
 
+# ----------------------------------------------------------- profiling case
+def run_case(args):
+    """A small search case for profiler captures (not a benchmark): the
+    first --ndm (default 2) DM trials of the survey workload, searched one
+    DM trial per call by the batched engine with CUDA events around every
+    launch group (so no graph capture: each kernel is an ordinary stream
+    launch), --batch / --harm-shape / --fft-form as given.  Two DM trials
+    hold about 1.5 GB on the device, so a capture of any of its kernels
+    stays small while every buffer a kernel streams exceeds the 126 MB L2.
+    Prints one JSON line with the engine's counters and stage times."""
+    import torch
+    from peasoup_b200 import search, synth
+    from peasoup_b200.build import build
+    build()
+    ndm = args.ndm or 2
+    plan = synth.survey_plan(ndm=NDM, nsamps=N_FFT, tsamp=TSAMP)
+    block = synth.survey_block_torch(plan, dm_indices=list(range(ndm)))
+    pr = make_params(plan, "batched", args.batch, args.harm_shape)
+    pr.fft_form = args.fft_form
+    s = search.AccelSearch(pr)
+    s.set_profile(True)
+    counts = []
+    for d in range(ndm):
+        counts.append(len(s.search(block[d], float(plan.dms[d]), d)[0]))
+    torch.cuda.synchronize()
+    print(json.dumps({"workload": "case", "ndm": ndm, "candidates": counts, "info": s.info(),
+                      "profile": s.profile()}), flush=True)
+    s.close()
+    return 0
+
+
 # ----------------------------------------------------------- dedispersion
 DD_NCHANS = 64
 DD_NBITS = 8
@@ -1013,16 +1113,20 @@ def main():
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
                     help="2: the headline survey workload; 3 and 5: the other throughput "
                          "configurations (one JSON line each)")
-    ap.add_argument("--ndm", type=int, default=0, help="configs 3/5: DM trials to time")
+    ap.add_argument("--ndm", type=int, default=0,
+                    help="configs 3/5: DM trials to time; --workload case: DM trials searched")
     ap.add_argument("--plain-sample", type=int, default=128,
                     help="config 3: DM trials searched by the plain path")
-    ap.add_argument("--workload", default="search", choices=["search", "dedisp"],
-                    help="dedisp: the dedispersion producer instead of the search")
+    ap.add_argument("--workload", default="search", choices=["search", "dedisp", "case"],
+                    help="dedisp: the dedispersion producer instead of the search; case: a "
+                         "small search case for profiler captures (--ndm DM trials, default 2)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_init()
     try:
-        if args.workload == "dedisp":
+        if args.workload == "case":
+            rc = run_case(args)
+        elif args.workload == "dedisp":
             if args.impl == "reference":
                 if rank == 0:
                     print(json.dumps({"impl": "reference", "unavailable": (

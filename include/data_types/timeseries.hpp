@@ -87,7 +87,7 @@ class ReusableDeviceTimeSeries : public DeviceTimeSeries<OnDeviceType> {
 public:
     explicit ReusableDeviceTimeSeries(std::size_t n) : DeviceTimeSeries<OnDeviceType>(n), staging(nullptr)
     {
-        if (sizeof(OnHostType) != sizeof(OnDeviceType) &&
+        if (!std::is_same<OnHostType, OnDeviceType>::value &&
             cudaMalloc(&staging, sizeof(OnHostType) * (n ? n : 1)) != cudaSuccess)
             ErrorChecker::throw_error("ReusableDeviceTimeSeries: cudaMalloc failed");
     }
@@ -100,22 +100,27 @@ public:
     {
         const std::size_t n = host.get_nsamps() < this->nsamps ? host.get_nsamps() : this->nsamps;
         this->tsamp = host.get_tsamp();
-        if (sizeof(OnHostType) == sizeof(OnDeviceType)) {
+        if constexpr (std::is_same<OnHostType, OnDeviceType>::value) {
             if (cudaMemcpy(this->data_ptr, host.get_data(), sizeof(OnHostType) * n,
                            cudaMemcpyHostToDevice) != cudaSuccess)
                 ErrorChecker::throw_error("copy_from_host: cudaMemcpy failed");
-            return;
+        } else {
+            // the reference converts after the copy (conversion_kernel,
+            // src/kernels.cu:1171-1200) for its 8-bit host types only
+            static_assert(std::is_same<OnDeviceType, float>::value && sizeof(OnHostType) == 1 &&
+                              std::is_integral<OnHostType>::value,
+                          "host series are float (copied) or 8-bit integers (converted)");
+            if (cudaMemcpy(staging, host.get_data(), n, cudaMemcpyHostToDevice) != cudaSuccess)
+                ErrorChecker::throw_error("copy_from_host: cudaMemcpy failed");
+            int rc;
+            if (std::is_signed<OnHostType>::value)
+                rc = psx_convert_i8_f32((const int8_t*)staging, (float*)this->data_ptr, n,
+                                        nullptr);
+            else
+                rc = psx_convert_u8_f32((const uint8_t*)staging, (float*)this->data_ptr, n,
+                                        nullptr);
+            ErrorChecker::check(rc, "copy_from_host");
         }
-        static_assert(sizeof(OnHostType) == 1 || sizeof(OnHostType) == 4, "uint8/int8/float hosts");
-        if (cudaMemcpy(staging, host.get_data(), sizeof(OnHostType) * n, cudaMemcpyHostToDevice) !=
-            cudaSuccess)
-            ErrorChecker::throw_error("copy_from_host: cudaMemcpy failed");
-        int rc;
-        if (std::is_signed<OnHostType>::value)
-            rc = psx_convert_i8_f32((const int8_t*)staging, (float*)this->data_ptr, n, nullptr);
-        else
-            rc = psx_convert_u8_f32((const uint8_t*)staging, (float*)this->data_ptr, n, nullptr);
-        ErrorChecker::check(rc, "copy_from_host");
     }
 };
 

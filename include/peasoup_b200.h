@@ -183,9 +183,12 @@ int psx_find_peaks(const float* d_spec, int n, int start, float thresh,
    which every GPU that loads the library holds until exit.  Limit:
    n - start <= 2^28 bins; larger requests fail with PSX_ERR_INVALID.
    The first call on each device looks up the array's device address with
-   that device current; make that first call before any stream capture.
-   All calls share the array: calls whose GPU work overlaps (different
-   streams or host threads) race and give wrong results. */
+   that device current and keeps it for the life of the process; make that
+   first call before any stream capture.  A cudaDeviceReset invalidates
+   the kept address: do not call this entry point in a process after a
+   reset of the device.  All calls share the array: calls whose GPU work
+   overlaps (different streams or host threads) race and give wrong
+   results. */
 int psx_find_peaks_noalloc(const float* d_spec, int n, int start, float thresh,
                            int* d_idx, float* d_val, int cap, int* h_count,
                            psx_stream_t stream);
@@ -215,15 +218,23 @@ int psx_harmonic_peaks(const float* d_spec, size_t pitch, size_t nbins, int rows
 /* ------------------------------------------------------------------ */
 
 typedef struct psx_fft_plan psx_fft_plan;
-enum { PSX_FFT_R2C = 0, PSX_FFT_C2R = 1 };
+enum { PSX_FFT_R2C = 0, PSX_FFT_C2R = 1, PSX_FFT_C2C = 2 };
 
 /* Unnormalised R2C / C2R plan of length `size`, `batch` transforms with
-   input/output distances size and size/2+1.  Replaces CuFFTerR2C /
-   CuFFTerC2R (include/transforms/ffter.hpp:90-146). */
+   input/output distances size and size/2+1, or (PSX_FFT_C2C) a complex
+   plan of `batch` transforms of length `size`, distance size.  Replaces
+   CuFFTerR2C / CuFFTerC2R (include/transforms/ffter.hpp:54-110) and
+   CuFFTerC2C (ffter.hpp:33-53). */
 int psx_fft_plan_create(psx_fft_plan** plan, size_t size, long long batch,
                         int kind);
+/* Executes an R2C or C2R plan. */
 int psx_fft_exec(psx_fft_plan* plan, const void* d_in, void* d_out,
                  psx_stream_t stream);
+/* Executes a PSX_FFT_C2C plan in `direction` -1 (forward, CUFFT_FORWARD)
+   or +1 (inverse, CUFFT_INVERSE), unnormalised; in place when d_in ==
+   d_out.  Replaces CuFFTerC2C::execute (ffter.hpp:43-47). */
+int psx_fft_exec_c2c(psx_fft_plan* plan, const void* d_in, void* d_out, int direction,
+                     psx_stream_t stream);
 int psx_fft_plan_destroy(psx_fft_plan* plan);
 
 /* ------------------------------------------------------------------ */
@@ -250,12 +261,12 @@ int psx_accel_list(float acc_lo, float acc_hi, float tol, float pulse_width_s,
                    float dm, float cdm, float* h_out, size_t cap, size_t* n);
 
 /* Search range [*start, *end) and frequency factor of a spectrum with
-   harmonic number nh.  Restates peakfinder.hpp:123-134. */
+   harmonic number nh.  Restates peakfinder.hpp:78-91. */
 int psx_peak_range(unsigned nbins, double bin_width, int nh, float min_freq,
                    float max_freq, int* start, int* end, float* factor);
 
 /* Cluster sorted above-threshold bins (min_gap rule of
-   PeakFinder::identify_unique_peaks, peakfinder.hpp:72-101). */
+   PeakFinder::identify_unique_peaks, peakfinder.hpp:72-94). */
 size_t psx_identify_unique_peaks(const int* idx, const float* snr,
                                  size_t count, int min_gap, int* out_idx,
                                  float* out_snr);
@@ -386,7 +397,12 @@ typedef struct {
     int batch;                 /* trials per launch (batched; rounded down to a
                                   power of two unless the two-pass transform
                                   carries the trials); 0 = default */
-    int use_fft_callback;      /* batched: fuse the resample into cuFFT */
+    int use_fft_callback;      /* must be 0: the resample inside cuFFT needs LTO
+                                  load callbacks, which cuFFT 11.4 (CUDA 12.9)
+                                  cannot plan on sm_100; a non-zero value is
+                                  refused with PSX_ERR_UNSUPPORTED.  The
+                                  two-pass transform (fft_form 3) does that
+                                  fusion itself */
     int use_graph;             /* batched: capture the trial schedule */
     int harm_shape;            /* harmonic-kernel tile shape 1..PSX_HARM_SHAPES;
                                   0 = default (psx_autotune picks one) */
@@ -486,7 +502,7 @@ typedef struct {
     int kernel_launches;  /* kernels this library launched */
     int fft_launches;     /* cuFFT executions */
     long long above_threshold; /* (bin, fold) pairs above threshold */
-    int fft_callback;     /* 1 if the resample ran inside cuFFT */
+    int fft_callback;     /* always 0 (see use_fft_callback) */
     int graph;            /* 1 if the trial schedule ran as a CUDA graph */
     int batch;            /* trials per launch used */
     int baseline_passes;  /* mean-removal passes of the last DM (-1: host loop) */
@@ -541,7 +557,7 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
                          float* h_tim_r, float* h_pspec, float* h_norm2);
 
 /* Reuses an instance for another request with the same transform length,
-   folds, mode, batch, harmonic shape and callback setting (the things its
+   folds, mode, batch, harmonic shape and lanes (the things its
    buffers and plans depend on): acceleration range, tsamp, thresholds,
    frequency limits and birdies may all change.  Waits for the instance's
    queued work first.  No counterpart in the reference (whose Worker builds

@@ -1,6 +1,6 @@
-// ffter.hpp -- unnormalised real transforms of the drop-in API (reference
-// include/transforms/ffter.hpp:43-146: CuFFTer, CuFFTerR2C, CuFFTerC2R)
-// over psx_fft_plan_*.
+// ffter.hpp -- unnormalised transforms of the drop-in API (reference
+// include/transforms/ffter.hpp: CuFFTer :8-31, CuFFTerC2C :33-53,
+// CuFFTerR2C :54-80, CuFFTerC2R :82-110) over psx_fft_plan_*.
 #pragma once
 #include <cufft.h>
 #include "peasoup_b200.h"
@@ -26,6 +26,21 @@ public:
     }
     CuFFTer(const CuFFTer&) = delete;
     CuFFTer& operator=(const CuFFTer&) = delete;
+};
+
+class CuFFTerC2C : public CuFFTer {
+public:
+    explicit CuFFTerC2C(unsigned int n, unsigned int batch = 1, psx_stream_t s = nullptr)
+        : CuFFTer(n, batch, PSX_FFT_C2C, s)
+    {
+    }
+    unsigned int get_output_size() override { return size; }
+    // direction CUFFT_FORWARD or CUFFT_INVERSE, unnormalised, as cufftExecC2C
+    void execute(cufftComplex* input, cufftComplex* output, int direction)
+    {
+        ErrorChecker::check(psx_fft_exec_c2c(plan, input, output, direction, stream),
+                            "CuFFTerC2C::execute");
+    }
 };
 
 class CuFFTerR2C : public CuFFTer {

@@ -1,5 +1,5 @@
 // peakfinder.hpp -- PeakFinder of the drop-in API (reference
-// include/transforms/peakfinder.hpp:56-140): threshold, order-preserving
+// include/transforms/peakfinder.hpp:11-95): threshold, order-preserving
 // compaction on the device, min-gap clustering and frequency assignment.
 #pragma once
 #include <cuda_runtime.h>

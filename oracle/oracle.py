@@ -570,6 +570,21 @@ def ref_resampleII(x, acc, tsamp):
     return out
 
 
+def ref_copy_from_host_8bit(x) -> np.ndarray:
+    """The reference's ReusableDeviceTimeSeries<float, unsigned char | char>
+    ::copy_from_host of a uint8 or int8 host array (its conversion_kernel)."""
+    x = np.ascontiguousarray(x)
+    if x.dtype not in (np.uint8, np.int8):
+        raise TypeError("uint8 or int8 samples")
+    out = np.zeros(x.size, np.float32)
+    L = ref_gpu()
+    fn = L.ref_copy_from_host_u8 if x.dtype == np.uint8 else L.ref_copy_from_host_i8
+    fn.restype = C.c_int
+    _chk(fn(x.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p), C.c_size_t(x.size)),
+         "copy_from_host")
+    return out
+
+
 def ref_resample(x, acc, tsamp):
     x = np.ascontiguousarray(x, np.float32)
     out = np.zeros_like(x)

@@ -5,7 +5,7 @@
  * the checker that the parity tests and the CPU baseline run against.
  *
  * The reference performs its transforms with cuFFT (include/transforms/
- * ffter.hpp:90-146: an unnormalised forward R2C of length N and an
+ * ffter.hpp:54-110: an unnormalised forward R2C of length N and an
  * unnormalised inverse C2R of length N).  This file restates those two
  * transforms in double precision with published methods:
  *

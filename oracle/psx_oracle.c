@@ -353,10 +353,10 @@ int orc_harmonic_sums(const double* in, size_t n, int nfolds, double* out)
 }
 
 /* ------------------------------------------------------------------ */
-/* Peak finding (peakfinder.hpp:72-139)                                */
+/* Peak finding (peakfinder.hpp:72-94)                                */
 /* ------------------------------------------------------------------ */
 
-/* peakfinder.hpp:123-134, with the reference's types: nyquist and factor
+/* peakfinder.hpp:78-91, with the reference's types: nyquist and factor
    are floats, orig_size an int, the power of two a double. */
 void orc_peak_range(unsigned nbins, double bin_width, int nh, float min_freq,
                     float max_freq, int* start, int* end, float* factor)
@@ -372,7 +372,7 @@ void orc_peak_range(unsigned nbins, double bin_width, int nh, float min_freq,
     *factor = (float)(1.0 / size * (double)nyquist / pow(2.0, (double)(float)nh));
 }
 
-/* peakfinder.hpp:72-101: a cluster starts at an above-threshold bin and
+/* peakfinder.hpp:72-94: a cluster starts at an above-threshold bin and
    absorbs following bins while they lie closer than min_gap to the bin
    that currently holds the cluster maximum; each cluster yields its
    maximum. */

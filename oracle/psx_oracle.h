@@ -70,7 +70,7 @@ int orc_remove_baseline(double* x, size_t n);
 int orc_harmonic_sums(const double* in, size_t n, int nfolds,
                       double* out /* nfolds*n */);
 
-/* ---- peak finding (peakfinder.hpp:72-139) ---- */
+/* ---- peak finding (peakfinder.hpp:72-94) ---- */
 void orc_peak_range(unsigned nbins, double bin_width, int nh, float min_freq,
                     float max_freq, int* start, int* end, float* factor);
 size_t orc_identify_unique_peaks(const int* idx, const double* snr,

@@ -22,6 +22,7 @@
 #include <iostream>
 #include <sstream>
 #include <map>
+#include <chrono>
 #include <thrust/device_vector.h>
 #include <data_types/fourierseries.hpp>
 #include <data_types/timeseries.hpp>
@@ -58,6 +59,21 @@ int guarded(const std::function<void()>& f)
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
 
+/* ReusableDeviceTimeSeries<float, X>::copy_from_host (timeseries.hpp:
+   352-361): the host->device copy of n 8-bit samples and the reference's
+   conversion_kernel (src/kernels.cu:1171-1200); X = unsigned char or char,
+   the two 8-bit types the reference instantiates. */
+template <class X>
+int copy_from_host_8bit(const X* in, float* out, size_t n)
+{
+    return guarded([&] {
+        ReusableDeviceTimeSeries<float, X> d(n);
+        TimeSeries<X> host(const_cast<X*>(in), n, 64e-6f);
+        d.copy_from_host(host);
+        cudaMemcpy(out, d.get_data(), sizeof(float) * n, cudaMemcpyDeviceToHost);
+    });
+}
+
 }  // namespace
 
 extern "C" {
@@ -84,6 +100,16 @@ int ref_resampleII(const float* in, float* out, size_t n, float acc, float tsamp
     });
 }
 
+int ref_copy_from_host_u8(const unsigned char* in, float* out, size_t n)
+{
+    return copy_from_host_8bit<unsigned char>(in, out, n);
+}
+
+int ref_copy_from_host_i8(const char* in, float* out, size_t n)
+{
+    return copy_from_host_8bit<char>(in, out, n);
+}
+
 /* TimeDomainResampler::resample (resampler.hpp:19-24). */
 int ref_resample(const float* in, float* out, size_t n, float acc, float tsamp)
 {
@@ -97,7 +123,7 @@ int ref_resample(const float* in, float* out, size_t n, float acc, float tsamp)
     });
 }
 
-/* CuFFTerR2C::execute (ffter.hpp:90-116). */
+/* CuFFTerR2C::execute (ffter.hpp:54-80). */
 int ref_fft_r2c(const float* in, size_t n, float* out_c)
 {
     return guarded([&] {
@@ -116,7 +142,7 @@ int ref_fft_r2c(const float* in, size_t n, float* out_c)
     });
 }
 
-/* CuFFTerC2R::execute (ffter.hpp:118-146). */
+/* CuFFTerC2R::execute (ffter.hpp:82-110). */
 int ref_fft_c2r(const float* in_c, size_t n, float* out)
 {
     return guarded([&] {
@@ -241,7 +267,7 @@ int ref_harmonic_sums(const float* in, size_t n, int nfolds, float* out)
 }
 
 /* PeakFinder::find_candidates on one spectrum with harmonic number nh
-   (peakfinder.hpp:72-139). */
+   (peakfinder.hpp:72-94). */
 int ref_find_candidates(const float* spec, size_t nbins, double bin_width, int nh,
                         float thresh, float min_freq, float max_freq, int min_gap,
                         float* snr, float* freq, size_t cap, size_t* n)
@@ -290,7 +316,7 @@ static void flatten_tree(Candidate& c, std::vector<ref_candidate>& out, std::vec
 static int worker_search(const float* series, size_t ndm, size_t nsamps, float tsamp,
                          const float* dms, size_t fft_size, const ref_search_args* a,
                          ref_candidate* out, int* nassoc, int* sizes_out, size_t cap,
-                         size_t* n_out)
+                         size_t* n_out, double* start_seconds = nullptr)
 {
     return guarded([&] {
         DispersionTrials<float> trials(tsamp);
@@ -318,7 +344,11 @@ static int worker_search(const float* series, size_t ndm, size_t nsamps, float t
                               args.acc_pulse_width * 1e-6, fft_size, tsamp,
                               a->cfreq_hz, a->ch_bw_hz);
         Worker w(trials, dispenser, plan, args, (unsigned)fft_size, 0);
+        const auto t0 = std::chrono::steady_clock::now();
         w.start();
+        if (start_seconds)
+            *start_seconds =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::vector<Candidate>& c = w.dm_trial_cands.cands;
         if (sizes_out) {
             // the candidates with their association trees, as a forest
@@ -346,6 +376,22 @@ int ref_worker_search(const float* series, size_t ndm, size_t nsamps, float tsam
 {
     return worker_search(series, ndm, nsamps, tsamp, dms, fft_size, a, out, nassoc, nullptr, cap,
                          n_out);
+}
+
+/* The same run, also returning the wall time of Worker::start alone (the
+   worker's own set-up of transforms and plans, every DM trial's host->device
+   copy, prologue and acceleration trials; every launch there is followed by
+   a device synchronisation, so wall time is device time).  The staging copy
+   of the series into the reference's DispersionTrials container is outside
+   it: in the reference's program that container is the dedisperser's
+   output. */
+int ref_worker_search_timed(const float* series, size_t ndm, size_t nsamps, float tsamp,
+                            const float* dms, size_t fft_size, const ref_search_args* a,
+                            ref_candidate* out, int* nassoc, size_t cap, size_t* n_out,
+                            double* start_seconds)
+{
+    return worker_search(series, ndm, nsamps, tsamp, dms, fft_size, a, out, nassoc, nullptr, cap,
+                         n_out, start_seconds);
 }
 
 /* The same run; its per-DM candidates with their association trees as a

@@ -25,6 +25,7 @@ PSX_ERR_BUSY = 8
 
 PSX_FFT_R2C = 0
 PSX_FFT_C2R = 1
+PSX_FFT_C2C = 2
 PSX_HARM_SHAPES = 7
 PSX_MODE_PLAIN = 0
 PSX_MODE_BATCHED = 1
@@ -147,6 +148,7 @@ SIGNATURES = {
                                 C.c_uint, C.c_uint, _vp]),
     "psx_fft_plan_create": (_i, [C.POINTER(_vp), _sz, C.c_longlong, _i]),
     "psx_fft_exec": (_i, [_vp, _vp, _vp, _vp]),
+    "psx_fft_exec_c2c": (_i, [_vp, _vp, _vp, _i, _vp]),
     "psx_fft_plan_destroy": (_i, [_vp]),
     "psx_accel_list": (_i, [_f, _f, _f, _f, _sz, _f, _f, _f, _f, _f, _vp, _sz, C.POINTER(_sz)]),
     "psx_peak_range": (_i, [C.c_uint, C.c_double, _i, _f, _f, C.POINTER(_i), C.POINTER(_i),

@@ -2,9 +2,8 @@
 
     python -m peasoup_b200.build          # or peasoup_b200.build.build()
 
-Steps: the cuFFT load callback is compiled to LTO IR and embedded as a
-byte array; the CUDA and C++ sources are compiled with nvcc/g++ for
-sm_100a; everything is linked against cuFFT into
+Steps: the CUDA and C++ sources are compiled with nvcc/g++ for sm_100a;
+everything is linked against cuFFT into
 peasoup_b200/libpeasoup_b200.so.  Objects go to peasoup_b200/_build/.
 """
 from __future__ import annotations
@@ -57,16 +56,6 @@ def _run(cmd):
     return r
 
 
-def _embed(fatbin: str, inc: str, name: str) -> None:
-    data = open(fatbin, "rb").read()
-    lines = [f"// generated from {os.path.basename(fatbin)}; do not edit",
-             f"alignas(16) static const unsigned char {name}[] = {{"]
-    for i in range(0, len(data), 16):
-        lines.append("  " + ", ".join(str(b) for b in data[i:i + 16]) + ",")
-    lines.append("};")
-    open(inc, "w").write("\n".join(lines) + "\n")
-
-
 def build(verbose: bool = False, force: bool = False) -> str:
     """Compile and link the library if any source is newer; returns its path."""
     if not os.path.exists(NVCC):
@@ -74,23 +63,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in _headers()] + [os.path.join(INCLUDE, "peasoup_b200.h")]
 
-    # 1. LTO callback for cuFFT, embedded as a byte array
-    cb_src = os.path.join(CSRC, "psx_fft_cb.cu")
-    cb_fat = os.path.join(BUILD, "psx_fft_cb.fatbin")
-    cb_inc = os.path.join(BUILD, "psx_fft_cb_fatbin.inc")
-    if force or _newer(cb_inc, [cb_src] + hdrs):
-        _run([NVCC, "-gencode", "arch=compute_100a,code=lto_100a", "-dc", "-fatbin",
-              "-std=c++17", f"-I{INCLUDE}", f"-I{CSRC}", cb_src, "-o", cb_fat])
-        _embed(cb_fat, cb_inc, "psx_fft_cb_fatbin")
-
-    # 2. objects
+    # 1. objects
     jobs = []
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
-        if force or _newer(o, [s, cb_inc] + hdrs):
+        if force or _newer(o, [s] + hdrs):
             jobs.append([NVCC, "-c", *NVCC_FLAGS, s, "-o", o])
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
@@ -106,7 +86,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 if verbose:
                     sys.stdout.write(r.stdout + r.stderr)
 
-    # 3. link
+    # 2. link
     if force or jobs or _newer(LIB, objs):
         tmp = LIB + ".tmp"
         _run([NVCC, "-shared", *ARCH, *objs, "-lcufft", "-o", tmp])

@@ -1,17 +1,12 @@
 // psx_fft.cu -- cuFFT plans for the search: plain R2C/C2R plans (the
-// drop-in CuFFTerR2C / CuFFTerC2R) and batched R2C plans whose load
-// callback performs the acceleration resample (LTO callback, compiled from
-// psx_fft_cb.cu and embedded at build time).
+// drop-in CuFFTerR2C / CuFFTerC2R), batched R2C plans and the complex
+// transforms of the batched trials.
 #include <cufft.h>
 #include <cufftXt.h>
 #include <cuda_runtime.h>
 #include <cstring>
 #include "psx_common.cuh"
 #include "psx_fft.cuh"
-#include "psx_fft_cb.h"
-
-// Generated by the build: const unsigned char psx_fft_cb_fatbin[]; size.
-#include "psx_fft_cb_fatbin.inc"
 
 namespace psx {
 
@@ -46,8 +41,7 @@ bool fft_size_supported(size_t n)
     return m == 1 || m == 3;
 }
 
-int FftPlan::create(size_t n_, long long batch_, int kind_, size_t in_dist, size_t out_dist,
-                    bool resample_callback)
+int FftPlan::create(size_t n_, long long batch_, int kind_, size_t in_dist, size_t out_dist)
 {
     destroy();
     if (!fft_size_supported(n_) || batch_ < 1) {
@@ -62,19 +56,6 @@ int FftPlan::create(size_t n_, long long batch_, int kind_, size_t in_dist, size
     const size_t nb = n / 2 + 1;
     if (in_dist == 0) in_dist = kind == PSX_FFT_R2C ? n : kind == kFftC2C ? n : nb;
     if (out_dist == 0) out_dist = kind == PSX_FFT_R2C ? nb : n;
-    if (resample_callback) {
-        if (kind != PSX_FFT_R2C) {
-            set_error("fft plan: the resample callback needs an R2C plan");
-            return PSX_ERR_INVALID;
-        }
-        PSX_CUDA(cudaMalloc(&d_cbinfo, sizeof(psx_resample_cb_info)));
-        void* info = d_cbinfo;
-        PSX_TRY(fft_status(cufftXtSetJITCallback(h, "psx_resample_load", psx_fft_cb_fatbin,
-                                                 sizeof(psx_fft_cb_fatbin), CUFFT_CB_LD_REAL,
-                                                 &info),
-                           "cufftXtSetJITCallback"));
-        callback = true;
-    }
     long long dims[1] = {(long long)n};
     long long inembed[1] = {(long long)in_dist};
     long long onembed[1] = {(long long)out_dist};
@@ -89,34 +70,6 @@ void FftPlan::destroy()
 {
     if (have) cufftDestroy(h);
     have = false;
-    if (d_cbinfo) cudaFree(d_cbinfo);
-    d_cbinfo = nullptr;
-    callback = false;
-}
-
-int FftPlan::set_resample(const float* d_series, const double* d_ktab, cudaStream_t s)
-{
-    if (!callback) {
-        set_error("fft plan has no resample callback");
-        return PSX_ERR_INVALID;
-    }
-    psx_resample_cb_info info;
-    info.series = d_series;
-    info.ktab = d_ktab;
-    info.n = n;
-    info.size = (double)n;
-    unsigned sh = 0;
-    size_t m = n;
-    while ((m & 1) == 0) {
-        m >>= 1;
-        ++sh;
-    }
-    info.shift = sh;
-    info.three = m == 3 ? 1u : 0u;
-    // Stream-ordered: executions already queued keep the previous block.
-    host_info = info;
-    return cuda_status(cudaMemcpyAsync(d_cbinfo, &host_info, sizeof info, cudaMemcpyHostToDevice, s),
-                       "fft callback info copy");
 }
 
 int FftPlan::exec(const void* in, void* out, cudaStream_t s)
@@ -137,6 +90,22 @@ int FftPlan::exec(const void* in, void* out, cudaStream_t s)
                       "cufftExecC2R");
 }
 
+int FftPlan::exec_c2c(const void* in, void* out, int direction, cudaStream_t s)
+{
+    if (!have || kind != kFftC2C) {
+        set_error("fft exec_c2c: not a complex plan");
+        return PSX_ERR_INVALID;
+    }
+    if (direction != CUFFT_FORWARD && direction != CUFFT_INVERSE) {
+        set_error("fft exec_c2c: direction must be -1 (forward) or +1 (inverse)");
+        return PSX_ERR_INVALID;
+    }
+    PSX_TRY(fft_status(cufftSetStream(h, s), "cufftSetStream"));
+    return fft_status(cufftExecC2C(h, (cufftComplex*)const_cast<void*>(in), (cufftComplex*)out,
+                                   direction),
+                      "cufftExecC2C");
+}
+
 }  // namespace psx
 
 struct psx_fft_plan {
@@ -148,14 +117,15 @@ extern "C" {
 int psx_fft_plan_create(psx_fft_plan** plan, size_t size, long long batch, int kind)
 {
     psx::clear_error();
-    if (!plan || (kind != PSX_FFT_R2C && kind != PSX_FFT_C2R)) {
+    if (!plan || (kind != PSX_FFT_R2C && kind != PSX_FFT_C2R && kind != PSX_FFT_C2C)) {
         psx::set_error("fft_plan_create: bad arguments");
         return PSX_ERR_INVALID;
     }
     *plan = nullptr;
     psx_fft_plan* p = new (std::nothrow) psx_fft_plan;
     if (!p) return PSX_ERR_ALLOC;
-    int rc = p->p.create(size, batch, kind, 0, 0, false);
+    int rc = kind == PSX_FFT_C2C ? p->p.create(size, batch, psx::kFftC2C, size, size)
+                                 : p->p.create(size, batch, kind, 0, 0);
     if (rc != PSX_OK) {
         delete p;
         return rc;
@@ -171,7 +141,22 @@ int psx_fft_exec(psx_fft_plan* plan, const void* d_in, void* d_out, psx_stream_t
         psx::set_error("fft_exec: bad arguments");
         return PSX_ERR_INVALID;
     }
+    if (plan->p.kind == psx::kFftC2C) {
+        psx::set_error("fft_exec: a complex plan needs psx_fft_exec_c2c (a direction)");
+        return PSX_ERR_INVALID;
+    }
     return plan->p.exec(d_in, d_out, psx::cs(stream));
+}
+
+int psx_fft_exec_c2c(psx_fft_plan* plan, const void* d_in, void* d_out, int direction,
+                     psx_stream_t stream)
+{
+    psx::clear_error();
+    if (!plan || !d_in || !d_out) {
+        psx::set_error("fft_exec_c2c: bad arguments");
+        return PSX_ERR_INVALID;
+    }
+    return plan->p.exec_c2c(d_in, d_out, direction, psx::cs(stream));
 }
 
 int psx_fft_plan_destroy(psx_fft_plan* plan)

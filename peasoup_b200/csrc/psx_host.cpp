@@ -48,7 +48,7 @@ std::vector<float> accel_list(float acc_lo, float acc_hi, float tol, float pulse
     return out;
 }
 
-// include/transforms/peakfinder.hpp:123-134.
+// include/transforms/peakfinder.hpp:78-91.
 void peak_range(unsigned nbins, double bin_width, int nh, float min_freq, float max_freq,
                 int* start, int* end, float* factor)
 {
@@ -63,7 +63,7 @@ void peak_range(unsigned nbins, double bin_width, int nh, float min_freq, float 
     *factor = (float)(1.0 / size * (double)nyquist / std::pow(2.0, (double)(float)nh));
 }
 
-// include/transforms/peakfinder.hpp:72-101: a cluster absorbs bins closer
+// include/transforms/peakfinder.hpp:72-94: a cluster absorbs bins closer
 // than min_gap to the bin holding its current maximum.
 size_t unique_peaks(const int* idx, const float* snr, size_t count, int min_gap, int* oi,
                     float* os)

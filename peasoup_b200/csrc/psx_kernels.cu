@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(256) k_sum_partials(Src src, size_t first, siz
 // Adds `nparts` partials (one warp, fixed order); writes the totals to sums[0..1]
 // and, when stat != nullptr, the reference's float statistics
 // {mean, rms, std, mean*scale, std*scale} computed exactly as its host
-// code does (stats.hpp:160-173 and src/kernels.cu:443,458), without
+// code does (stats.hpp:20-31 and src/kernels.cu:443,458), without
 // contraction.
 __global__ void k_finish_stats(const double2* __restrict__ partials, int nparts, double count,
                                double* __restrict__ sums, float* __restrict__ stat, float scale)

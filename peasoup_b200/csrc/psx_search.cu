@@ -9,14 +9,14 @@
 //   birdie zapping -> interbin statistics (device-resident mean*N, std*N)
 //   -> C2R into the resident dereddened series.
 // Per acceleration trial (the hot loop), in launch groups of `batch`:
-//   resample gather -> R2C (one batched cuFFT, or with the resample inside
-//   cuFFT through a load callback where cuFFT supports it) -> k_form_norm
+//   resample gather -> R2C (one batched cuFFT; by default the library's
+//   two-pass transform with the gather in its first pass) -> k_form_norm
 //   (interbin + normalise in one pass) -> k_harm_tiles (fractional harmonic
 //   sums + threshold + warp-aggregated compaction of every (trial, fold,
 //   bin, S/N) above threshold).  The trial schedule of a DM can be captured
 //   as one CUDA graph.  Nothing per trial goes to the host: the records of
 //   a DM come back in one copy, and the host clusters them
-//   (peakfinder.hpp:72-101), forms frequencies and distils them
+//   (peakfinder.hpp:72-94), forms frequencies and distils them
 //   (distiller.hpp) while the GPU already runs the next DM (two record
 //   slots, psx_search_block).
 #include <cuda.h>
@@ -536,7 +536,6 @@ struct psx_search {
     float* d_bf = nullptr;
     float* d_bw = nullptr;
     size_t bird_cap = 0;  // entries d_bf / d_bw hold
-    double* d_kbatch = nullptr;
     float* h_mean = nullptr;
     TwSteps tw_steps{};  // unit rotations of the fused unpack kernel
 
@@ -596,8 +595,7 @@ struct psx_search {
             m.clear();
         }
         r2c1.destroy();
-        void* dev[] = {d_trl[0], d_Xl[0], d_pl[0], d_trl[1], d_Xl[1], d_pl[1], d_bf, d_bw,
-                       d_kbatch};
+        void* dev[] = {d_trl[0], d_Xl[0], d_pl[0], d_trl[1], d_Xl[1], d_pl[1], d_bf, d_bw};
         for (void* q : dev)
             if (q) cudaFree(q);
         for (int l = 0; l < 2; ++l) d_trl[l] = d_Xl[l] = d_pl[l] = nullptr;
@@ -605,7 +603,6 @@ struct psx_search {
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         ev_fork = ev_join = nullptr;
-        d_kbatch = nullptr;
         if (call_start) cudaEventDestroy(call_start);
         call_start = nullptr;
         if (h_mean) cudaFreeHost(h_mean);
@@ -641,12 +638,11 @@ struct psx_search {
     }
 
     bool batched() const { return cfg.mode == PSX_MODE_BATCHED; }
-    bool callback() const { return batched() && cfg.use_fft_callback; }
     // batched trials through the hand-written two-pass transform (resample
     // gather in its first pass) + the unpack kernel of its transposed output
     bool fft4() const { return use_f4; }
     // batched trials through cuFFT's complex transform + fused unpack kernel
-    bool fused_form() const { return batched() && !callback() && cfg.fft_form != 2 && !use_f4; }
+    bool fused_form() const { return batched() && cfg.fft_form != 2 && !use_f4; }
 
     int get_plan(int b, FftPlan** out, int lane = 0);
     int grow_records(Slot& s, size_t need);
@@ -676,9 +672,8 @@ int psx_search::get_plan(int b, FftPlan** out, int lane)
     if (!p) return PSX_ERR_ALLOC;
     // fused form: a complex transform of length N/2 over the series read as
     // interleaved pairs (row distances in complex elements)
-    int rc = fused_form() ? p->create(N / 2, b, kFftC2C, N / 2, Bp, false)
-                          : p->create(N, b, PSX_FFT_R2C, N, Bp, callback());
-    if (rc == PSX_OK && callback()) rc = p->set_resample(slot[0].d_tim, d_kbatch, st);
+    int rc = fused_form() ? p->create(N / 2, b, kFftC2C, N / 2, Bp)
+                          : p->create(N, b, PSX_FFT_R2C, N, Bp);
     if (rc != PSX_OK) {
         delete p;
         return rc;
@@ -908,14 +903,8 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
             while (b > nacc - t0) b >>= 1;
             FftPlan* plan = nullptr;
             PSX_TRY(get_plan(b, &plan, lane));
-            if (callback()) {
-                PSX_TRY(plan->set_resample(s.d_tim, d_kbatch, ls));
-                PSX_CUDA(cudaMemcpyAsync(d_kbatch, s.d_ktab + t0, sizeof(double) * b,
-                                         cudaMemcpyDeviceToDevice, ls));
-            } else {
-                PSX_TRY(launch_resample(s.d_tim, tr, N, s.d_ktab + t0, 0.0, b, N, false, ls));
-                ++s.launches;
-            }
+            PSX_TRY(launch_resample(s.d_tim, tr, N, s.d_ktab + t0, 0.0, b, N, false, ls));
+            ++s.launches;
             if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g], ls));
             PSX_TRY(plan->exec(tr, X, ls));
             ++s.ffts;
@@ -1098,7 +1087,7 @@ void psx_search::read_profile(Slot& s)
 
 // Host side of one DM: bucket the records by (trial, fold), order each
 // bucket by bin (the order the reference's copy_if leaves them in),
-// cluster (peakfinder.hpp:72-101), form candidate frequencies, distil per
+// cluster (peakfinder.hpp:72-94), form candidate frequencies, distil per
 // trial (pipeline_multi.cu:283-289) and optionally per DM (:294).
 void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candidate>& out,
                          std::vector<int>& nassoc, std::vector<int>& trial_of)
@@ -1328,6 +1317,12 @@ static int check_config(const psx_search_config* c)
         set_error("search: unknown mode %d", c->mode);
         return PSX_ERR_INVALID;
     }
+    if (c->use_fft_callback) {
+        set_error("search: the resample inside cuFFT (use_fft_callback) is not available: cuFFT "
+                  "11.4 of CUDA 12.9 cannot plan LTO load callbacks on sm_100; the two-pass "
+                  "transform (fft_form 3) gathers the resampled series in its first pass");
+        return PSX_ERR_UNSUPPORTED;
+    }
     if (c->batch < 0 || c->batch > 1024) {
         set_error("search: batch must be 0..1024");
         return PSX_ERR_INVALID;
@@ -1336,9 +1331,8 @@ static int check_config(const psx_search_config* c)
         set_error("search: fft_form must be 0..3");
         return PSX_ERR_INVALID;
     }
-    if (c->fft_form == 3 && (c->mode != PSX_MODE_BATCHED || c->use_fft_callback ||
-                             !Fft4Plan::supported(c->fft_size))) {
-        set_error("search: fft_form 3 needs the batched mode without the cuFFT callback and "
+    if (c->fft_form == 3 && (c->mode != PSX_MODE_BATCHED || !Fft4Plan::supported(c->fft_size))) {
+        set_error("search: fft_form 3 needs the batched mode and "
                   "fft_size 2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23");
         return PSX_ERR_INVALID;
     }
@@ -1385,10 +1379,10 @@ static int effective_batch(const psx_search_config* c)
 
 // Transform path of the trials: 3 = the hand-written two-pass transform,
 // 1 = cuFFT's complex transform + the fused unpack kernel, 2 = the
-// reference's real transform (also plain mode and the cuFFT callback).
+// reference's real transform (also plain mode).
 static int effective_form(const psx_search_config* c)
 {
-    if (c->mode != PSX_MODE_BATCHED || c->use_fft_callback || c->fft_form == 2) return 2;
+    if (c->mode != PSX_MODE_BATCHED || c->fft_form == 2) return 2;
     if (c->fft_form == 3 || (c->fft_form == 0 && Fft4Plan::supported(c->fft_size))) return 3;
     return 1;
 }
@@ -1407,11 +1401,10 @@ size_t psx_search_footprint(const psx_search_config* c)
     const size_t N = c->fft_size, B = N / 2 + 1, Bp = round_up(B, 64);
     const size_t b = (size_t)effective_batch(c);
     const size_t L = (size_t)effective_lanes(c);
-    const bool cb = c->mode == PSX_MODE_BATCHED && c->use_fft_callback;
     size_t bytes = 0;
     bytes += 2 * sizeof(float) * (N + 2 * Bp);        // per slot: series, prologue spectrum
     bytes += 2 * median_scratch_bytes(B);
-    bytes += L * sizeof(float) * N * (cb ? 1 : b);    // resampled series, per lane
+    bytes += L * sizeof(float) * N * b;               // resampled series, per lane
     bytes += L * sizeof(float) * 2 * Bp * b;          // complex spectra, per lane
     bytes += L * sizeof(float) * Bp * b;              // normalised spectra, per lane
     bytes += 2 * sizeof(int4) * ((size_t)1 << 20);    // two initial record slots
@@ -1429,7 +1422,7 @@ size_t psx_search_footprint(const psx_search_config* c)
 // Host-side state of an instance derived from its configuration: the
 // birdie list, transform sizes, tobs and bin width (floats, as at
 // pipeline_multi.cu:126-128), the search ranges of every fold
-// (peakfinder.hpp:123-128) and the fast-pass vote level.  Shared by
+// (peakfinder.hpp:78-83) and the fast-pass vote level.  Shared by
 // psx_search_create and psx_search_retarget.
 static void host_setup(psx_search* s, const psx_search_config* cfg)
 {
@@ -1462,7 +1455,7 @@ static void host_setup(psx_search* s, const psx_search_config* cfg)
     s->tobs = (float)s->N * cfg->tsamp;
     s->bin_width_f = (float)(1.0 / (double)s->tobs);
     s->bin_width = (double)s->bin_width_f;
-    // search ranges of every fold (peakfinder.hpp:123-128)
+    // search ranges of every fold (peakfinder.hpp:78-83)
     unsigned lo = 0xffffffffu, hi = 0;
     for (int h = 0; h <= 5; ++h) {
         int st, en;
@@ -1516,14 +1509,13 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
         return fail(rc);
     const size_t N = s->N, Bp = s->Bp;
     const size_t b = (size_t)s->batch;
-    const bool cb = s->callback();
     const int nb = reduction_blocks();
 #define ALLOC(ptr, bytes)                                                        \
     if ((rc = cuda_status(cudaMalloc((void**)&(ptr), (bytes)), "cudaMalloc")) != \
         PSX_OK)                                                                  \
         return fail(rc == PSX_ERR_CUDA ? PSX_ERR_ALLOC : rc);
     for (int l = 0; l < s->lanes; ++l) {
-        ALLOC(s->d_trl[l], sizeof(float) * N * (cb ? 1 : b));
+        ALLOC(s->d_trl[l], sizeof(float) * N * b);
         ALLOC(s->d_Xl[l], sizeof(float) * 2 * Bp * b);
         ALLOC(s->d_pl[l], sizeof(float) * Bp * b);
     }
@@ -1535,7 +1527,6 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
             if ((rc = encode_harm_maps(s->d_pl[l], Bp, (int)b, kHarmShapes[s->harm_shape - 1].rows,
                                        &s->hmaps[l])) != PSX_OK)
                 return fail(rc);
-    ALLOC(s->d_kbatch, sizeof(double) * b);
     for (Slot& sl : s->slot) {
         ALLOC(sl.d_count, sizeof(unsigned) * 16);
         ALLOC(sl.d_tim, sizeof(float) * N);
@@ -1566,8 +1557,8 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
         sl.r2c = new (std::nothrow) FftPlan;
         sl.c2r = new (std::nothrow) FftPlan;
         if (!sl.r2c || !sl.c2r) return fail(PSX_ERR_ALLOC);
-        if ((rc = sl.r2c->create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
-        if ((rc = sl.c2r->create(N, 1, PSX_FFT_C2R, 0, 0, false)) != PSX_OK) return fail(rc);
+        if ((rc = sl.r2c->create(N, 1, PSX_FFT_R2C, 0, 0)) != PSX_OK) return fail(rc);
+        if ((rc = sl.c2r->create(N, 1, PSX_FFT_C2R, 0, 0)) != PSX_OK) return fail(rc);
         if ((rc = s->grow_records(sl, (size_t)1 << 20)) != PSX_OK) return fail(rc);
         if ((rc = s->grow_ktab(sl, 1024)) != PSX_OK) return fail(rc);
     }
@@ -1588,13 +1579,12 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
             cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
             return fail(PSX_ERR_CUDA);
     }
-    cudaMemsetAsync(s->d_kbatch, 0, sizeof(double) * b, s->st);
     for (Slot& sl : s->slot) {
         cudaMemsetAsync(sl.d_Xp, 0, sizeof(float) * 2 * Bp, s->st);
     }
     if (cudaEventCreateWithFlags(&s->call_start, cudaEventDisableTiming) != cudaSuccess)
         return fail(PSX_ERR_CUDA);
-    if ((rc = s->r2c1.create(N, 1, PSX_FFT_R2C, 0, 0, false)) != PSX_OK) return fail(rc);
+    if ((rc = s->r2c1.create(N, 1, PSX_FFT_R2C, 0, 0)) != PSX_OK) return fail(rc);
     if (s->fft4()) {
         if ((rc = s->f4.create(N)) != PSX_OK) return fail(rc);
     } else if (s->batched()) {
@@ -1606,7 +1596,7 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
         return fail(rc);
     s->info.batch = s->batch;
     s->info.harm_shape = s->harm_shape;
-    s->info.fft_callback = cb ? 1 : 0;
+    s->info.fft_callback = 0;
     s->info.fft_form = effective_form(cfg);
     s->set_st[0] = s->st;
     s->set_st2[0] = s->st2;
@@ -1694,13 +1684,12 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     }
     PSX_TRY(check_config(cfg));
     const int shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
-    const bool cb = cfg->mode == PSX_MODE_BATCHED && cfg->use_fft_callback;
     if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
-        effective_batch(cfg) != s->batch || shape != s->harm_shape || cb != s->callback() ||
+        effective_batch(cfg) != s->batch || shape != s->harm_shape ||
         effective_lanes(cfg) != s->lanes ||
         effective_form(cfg) != effective_form(&s->cfg)) {
-        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, callback, "
-                  "lanes and transform path must match the instance");
+        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, lanes and "
+                  "transform path must match the instance");
         return PSX_ERR_INVALID;
     }
     PSX_CUDA(cudaSetDevice(s->device));

@@ -50,10 +50,10 @@ class SearchParams:
     birdie_widths: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
     mode: str = "batched"          # "plain": one trial per launch
     batch: int = 0                 # 0: chosen from the transform length
-    # batched: resample inside cuFFT through an LTO load callback.  Off by
-    # default: the cuFFT 11.4 library of CUDA 12.9 fails plan creation for
-    # LTO callbacks on sm_100 (CUFFT_INTERNAL_ERROR), so the resample runs as
-    # its own kernel.
+    # resample inside cuFFT through an LTO load callback: refused
+    # (PSX_ERR_UNSUPPORTED), since the cuFFT 11.4 library of CUDA 12.9 fails
+    # plan creation for LTO callbacks on sm_100; the two-pass transform
+    # (fft_form 3) gathers the resampled series in its first pass instead.
     fft_callback: bool = False
     graph: bool = True             # batched: CUDA-graph trial schedule
     harm_shape: int = 0            # harmonic-kernel tile shape (0 = default)

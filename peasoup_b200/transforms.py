@@ -24,7 +24,8 @@ from ._lib import PsxError, check, load
 
 __all__ = [
     "PsxError", "DeviceTimeSeries", "DeviceFourierSeries", "DevicePowerSpectrum",
-    "HarmonicSums", "TimeDomainResampler", "CuFFTerR2C", "CuFFTerC2R", "SpectrumFormer",
+    "HarmonicSums", "TimeDomainResampler", "CuFFTerC2C", "CuFFTerR2C", "CuFFTerC2R",
+    "SpectrumFormer",
     "Dereddener", "Zapper", "stats", "normalise", "SpectrumNormaliser", "HarmonicFolder",
     "PeakFinder", "Candidate", "CandidateCollection", "SpectrumCandidates",
     "HarmonicDistiller", "AccelerationDistiller", "DMDistiller", "AccelerationPlan",
@@ -209,8 +210,23 @@ class _CuFFTer:
             pass
 
 
+class CuFFTerC2C(_CuFFTer):
+    """include/transforms/ffter.hpp:33-53: unnormalised complex transform;
+    direction -1 (CUFFT_FORWARD) or +1 (CUFFT_INVERSE) per call."""
+    kind = _lib.PSX_FFT_C2C
+
+    def get_output_size(self) -> int:
+        return self.size
+
+    def execute(self, input, output, direction: int) -> None:
+        a = input.get_data() if hasattr(input, "get_data") else input
+        b = output.get_data() if hasattr(output, "get_data") else output
+        check(load().psx_fft_exec_c2c(self._plan, _ptr(a), _ptr(b), int(direction), _stream()),
+              "CuFFTerC2C::execute")
+
+
 class CuFFTerR2C(_CuFFTer):
-    """include/transforms/ffter.hpp:90-116: unnormalised R2C."""
+    """include/transforms/ffter.hpp:54-80: unnormalised R2C."""
     kind = _lib.PSX_FFT_R2C
 
     def execute(self, tim, fseries) -> None:
@@ -220,7 +236,7 @@ class CuFFTerR2C(_CuFFTer):
 
 
 class CuFFTerC2R(_CuFFTer):
-    """include/transforms/ffter.hpp:118-146: unnormalised C2R."""
+    """include/transforms/ffter.hpp:82-110: unnormalised C2R."""
     kind = _lib.PSX_FFT_C2R
 
     def get_output_size(self) -> int:

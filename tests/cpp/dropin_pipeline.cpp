@@ -8,6 +8,8 @@
 //
 // usage: dropin_pipeline series.f32 nsamps fft_size tsamp dm acc_lo acc_hi
 //                        nharm min_snr zapfile|- out.bin
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -28,6 +30,40 @@
 #include "transforms/spectrumnormaliser.hpp"
 #include "utils/stats.hpp"
 #include "utils/utils.hpp"
+
+// The other classes a reference translation unit may name: CuFFTerC2C
+// (a forward and inverse round trip gives n times the input) and the
+// 8-bit host series of ReusableDeviceTimeSeries (converted exactly).
+// Returns 0 when both hold.
+static int check_other_classes()
+{
+    const unsigned n = 1024;
+    std::vector<cufftComplex> z(n), back(n);
+    for (unsigned i = 0; i < n; ++i) z[i] = cufftComplex{std::sin(0.37f * i), std::cos(1.3f * i)};
+    cufftComplex* d = nullptr;
+    if (cudaMalloc(&d, sizeof(cufftComplex) * n) != cudaSuccess) return 5;
+    cudaMemcpy(d, z.data(), sizeof(cufftComplex) * n, cudaMemcpyHostToDevice);
+    {
+        CuFFTerC2C c2c(n);
+        c2c.execute(d, d, CUFFT_FORWARD);
+        c2c.execute(d, d, CUFFT_INVERSE);
+    }
+    cudaMemcpy(back.data(), d, sizeof(cufftComplex) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    for (unsigned i = 0; i < n; ++i)
+        if (std::fabs(back[i].x - n * z[i].x) > 1e-3f * n || std::fabs(back[i].y - n * z[i].y) > 1e-3f * n)
+            return 6;
+    std::vector<uint8_t> u8(n);
+    for (unsigned i = 0; i < n; ++i) u8[i] = (uint8_t)(i * 37u);
+    TimeSeries<uint8_t> host_u8(u8.data(), n, 64e-6f);
+    ReusableDeviceTimeSeries<float, uint8_t> d_u8(n);
+    d_u8.copy_from_host(host_u8);
+    std::vector<float> f(n);
+    cudaMemcpy(f.data(), d_u8.get_data(), sizeof(float) * n, cudaMemcpyDeviceToHost);
+    for (unsigned i = 0; i < n; ++i)
+        if (f[i] != (float)u8[i]) return 7;
+    return 0;
+}
 
 int main(int argc, char** argv)
 {
@@ -50,6 +86,10 @@ int main(int argc, char** argv)
         if (!f) return 3;
     }
     try {
+        if (int rc = check_other_classes()) {
+            std::fprintf(stderr, "drop-in class check failed (%d)\n", rc);
+            return rc;
+        }
         // set-up, as the worker thread does once
         const float tobs = size * tsamp;
         const float bin_width = 1.0 / tobs;

@@ -52,16 +52,21 @@ def test_invalid_arguments_fail_loudly(psx):
     cfg.nharmonics = 6
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
     assert b"nharmonics" in psx.psx_last_error()
-    # the library's own transform: batched, no cuFFT callback, 2^19 .. 2^25 or
-    # 3 * 2^17 .. 3 * 2^23 points
-    for n, mode, cb in ((1 << 16, _lib.PSX_MODE_BATCHED, 0), (3 << 16, _lib.PSX_MODE_BATCHED, 0),
-                        (3 << 24, _lib.PSX_MODE_BATCHED, 0),
-                        (1 << 26, _lib.PSX_MODE_BATCHED, 0), (1 << 20, _lib.PSX_MODE_PLAIN, 0),
-                        (1 << 20, _lib.PSX_MODE_BATCHED, 1)):
+    # the library's own transform: batched, 2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23
+    # points
+    for n, mode in ((1 << 16, _lib.PSX_MODE_BATCHED), (3 << 16, _lib.PSX_MODE_BATCHED),
+                    (3 << 24, _lib.PSX_MODE_BATCHED),
+                    (1 << 26, _lib.PSX_MODE_BATCHED), (1 << 20, _lib.PSX_MODE_PLAIN)):
         psx.psx_search_config_defaults(C.byref(cfg), n, 64e-6)
-        cfg.mode, cfg.use_fft_callback, cfg.fft_form = mode, cb, 3
+        cfg.mode, cfg.fft_form = mode, 3
         assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
         assert b"fft_form 3" in psx.psx_last_error()
+    # the resample inside cuFFT (LTO load callbacks) is refused, not emulated
+    psx.psx_search_config_defaults(C.byref(cfg), 1 << 20, 64e-6)
+    cfg.use_fft_callback = 1
+    assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_UNSUPPORTED
+    assert b"use_fft_callback" in psx.psx_last_error()
+    cfg.use_fft_callback = 0
     cfg.fft_form = 4
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
     assert psx.psx_search_set_priority(None, 1) == _lib.PSX_ERR_INVALID

@@ -5,8 +5,9 @@ channels than a packed 16-bit accumulator holds (4096 at 8 bits, 4400 at
 4 bits, where bytes are first summed as they stand), DM counts that do
 not fill a CTA, a single output sample, host and device input; then the
 Dedisperser class on a file, and the whole program (run) on a synthetic
-tutorial-shaped filterbank: its pulsar is found at its DM, and its
-candidates equal a search of the oracle's dedispersed block."""
+tutorial-shaped filterbank and on the reference's own example filterbank:
+the pulsars are found, and the candidates equal a search of the oracle's
+dedispersed block."""
 import ctypes as C
 import os
 
@@ -193,6 +194,53 @@ def test_whole_program_on_synthetic_tutorial(psx, cuda, oracle, tmp_path):
     assert fast
     best = max(fast, key=lambda c: c["snr"])
     assert abs(best["dm"] - 30.0) <= 7.0, (best["dm"], best["snr"], best["freq"])
+
+
+TUTORIAL = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle",
+                        "_ref", "tutorial.fil")
+
+
+@pytest.mark.skipif(not os.path.exists(TUTORIAL),
+                    reason="the reference's example filterbank is staged by the oracle's build")
+def test_whole_program_on_tutorial_filterbank(psx, cuda, oracle, tmp_path):
+    """The reference's example data (example_data/tutorial.fil: 2-bit, 64
+    channels, 320 us, 187,520 samples, source "P: 250 ms, DM: 30") through
+    the whole program as the reference's main runs it (header, segment,
+    DM list 0..60, dedispersion into device memory, search, distillers,
+    outputs): the candidates equal a search of the oracle's dedispersion of
+    the same file, and the 4 Hz family is among the top candidates, its
+    strongest detection at a DM trial near 30."""
+    from peasoup_b200 import output, pipeline
+    from peasoup_b200.search import SearchParams
+    opts = pipeline.Options(TUTORIAL, outdir=str(tmp_path / "out"), dm_start=0.0, dm_end=60.0,
+                            min_snr=8.0)
+    nodes, sizes, scores, offsets, timers = pipeline.run(opts)
+    assert os.path.getsize(os.path.join(opts.outdir, "candidates.peasoup")) > 0
+    fb = sigproc.SigprocFilterbank(TUTORIAL)
+    h = oracle.parse_sigproc_header(TUTORIAL)
+    rows = np.fromfile(TUTORIAL, np.uint8, offset=h["header_size"]).reshape(-1, 16)
+    ts = np.float32(h["tsamp"])
+    dms = oracle.dm_list(64, ts, h["fch1"], h["foff"], 0.0, 60.0, 64.0, 1.11)
+    delays = oracle.delay_table(64, ts, h["fch1"], h["foff"])
+    block = oracle.dedisperse(rows, 2, 64, delays, dms)
+    size = sigproc.prev_power_of_two(fb.get_effective_nsamps())
+    cf = fb.get_cfreq()
+    foff = float(np.float32(h["foff"]))
+    params = SearchParams(fft_size=size, tsamp=float(ts),
+                          cfreq_hz=float(np.float32(float(np.float32(cf)) * 1e6)),
+                          ch_bw_hz=float(np.float32(foff * 1e6)),
+                          min_snr=8.0, acc_pulse_width=float(np.float32(64.0 * 1e-6)))
+    n2, s2, _, _, _ = pipeline.search_to_outputs(
+        block, dms, params, str(tmp_path / "out2"), foff_mhz=foff, nchans=64, cfreq_mhz=cf,
+        dm_chunk=len(dms))
+    assert np.array_equal(nodes, n2) and np.array_equal(sizes, s2)
+    top = nodes[output.roots(sizes)]
+    fam = [c for c in top if _family(float(c["freq"]), 4.0)]
+    print("tutorial: %d top candidates, 4 Hz family:" % len(top),
+          [(float(c["dm"]), float(c["freq"]), float(c["snr"])) for c in fam[:8]])
+    assert fam
+    best = max(fam, key=lambda c: c["snr"])
+    assert abs(best["dm"] - 30.0) <= 10.0, (best["dm"], best["snr"], best["freq"])
 
 
 @pytest.mark.parametrize("nchans,nbits", [(64, 8), (4096, 8), (64, 2), (32, 16)])

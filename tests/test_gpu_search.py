@@ -7,7 +7,7 @@
     spectrum of a tapped trial are checked stage by stage (resampled
     series bit-exact against the oracle's FP64 index on the product's own
     dereddened series; spectra within 1e-5 of FP64);
-  * plain (one trial per launch), batched and batched-with-callback
+  * plain (one trial per launch), batched and graph-captured batched
     schedules must give identical candidate lists;
   * against the reference's unmodified Worker (oracle/_ref) on the same
     series: the per-DM acceleration-distilled lists must match in the same
@@ -85,49 +85,39 @@ def test_tap_resampled_series_bit_exact(S, oracle):
 
 
 @pytest.mark.parametrize("n", [1 << 16, 3 << 15])
-def test_plain_batched_callback_identical(S, n):
+def test_plain_batched_graph_identical(S, n):
     search, synth = S
     ts = 64e-6
     x = synth.make_series_np(synth.SeriesSpec(
         nsamps=n, tsamp=ts, pulsars=[synth.Pulsar(3.1e-3, -20.0, 0.05, 0.8)]), 1)
     kw = dict(acc_lo=-200.0, acc_hi=200.0, nharmonics=5, min_snr=6.0)
     outs = []
-    for mode, cb, graph, batch in (("plain", False, False, 0), ("batched", False, False, 4),
-                                   ("batched", False, True, 8), ("batched", False, True, 1)):
-        s = search.AccelSearch(_params(S, n, ts, mode=mode, fft_callback=cb, graph=graph,
-                                       batch=batch, **kw))
+    for mode, graph, batch in (("plain", False, 0), ("batched", False, 4),
+                               ("batched", True, 8), ("batched", True, 1)):
+        s = search.AccelSearch(_params(S, n, ts, mode=mode, graph=graph, batch=batch, **kw))
         c, na, tr = s.search(x, 1.5, 3, per_dm=False)
         info = s.info()
         assert info["graph"] == int(graph and mode == "batched")
-        outs.append((mode, cb, c, info))
+        outs.append((mode, graph, c, info))
         s.close()
     base = outs[0][2]
-    for mode, cb, c, info in outs[1:]:
+    for mode, graph, c, info in outs[1:]:
         nm, ua, ub, worst = match_candidates(c, base, 6.0, margin=0.0)
         exact = len(c) == len(base) and np.array_equal(c, base)
-        assert exact or (not ua and not ub and worst < 1e-5), (mode, cb, ua[:3], ub[:3], worst)
+        assert exact or (not ua and not ub and worst < 1e-5), (mode, graph, ua[:3], ub[:3], worst)
 
 
-def test_fft_callback_path_fails_cleanly_or_matches(S):
+def test_fft_callback_refused(S):
     """The resample-in-cuFFT path needs LTO callbacks, which cuFFT rejects
-    on sm_100 in this toolkit; creation must then fail with a cuFFT status
-    (never fall back silently).  Where it works it must match the default."""
+    on sm_100 in this toolkit; asking for it is refused with a status
+    (never a silent fallback)."""
     search, synth = S
-    from peasoup_b200._lib import PSX_ERR_CUFFT, PsxError
+    from peasoup_b200._lib import PSX_ERR_UNSUPPORTED, PsxError
     n, ts = 1 << 16, 64e-6
-    x = synth.make_series_np(synth.SeriesSpec(nsamps=n, tsamp=ts), 3)
-    kw = dict(acc_lo=-100.0, acc_hi=100.0, nharmonics=3, min_snr=6.0)
-    try:
-        s = search.AccelSearch(_params(S, n, ts, fft_callback=True, batch=4, **kw))
-    except PsxError as e:
-        assert e.status == PSX_ERR_CUFFT
-        return
-    c = s.search(x)[0]
-    assert s.info()["fft_callback"] == 1
-    s.close()
-    ref = search.AccelSearch(_params(S, n, ts, batch=4, **kw))
-    nm, ua, ub, worst = match_candidates(c, ref.search(x)[0], 6.0, margin=0.0)
-    assert not ua and not ub and worst < 1e-5
+    with pytest.raises(PsxError) as e:
+        search.AccelSearch(_params(S, n, ts, fft_callback=True, batch=4, acc_lo=-100.0,
+                                   acc_hi=100.0, nharmonics=3, min_snr=6.0))
+    assert e.value.status == PSX_ERR_UNSUPPORTED
 
 
 def test_block_equals_single_dm_calls(S):

@@ -107,6 +107,28 @@ def test_fft_r2c_c2r_vs_oracle(T, oracle, n):
     assert err_vs_rms(back, n * x.astype(np.float64)) < 1e-5
 
 
+@pytest.mark.parametrize("n,batch", [(1 << 12, 3), (3 << 10, 1)])
+def test_fft_c2c_both_directions(T, n, batch):
+    """CuFFTerC2C (ffter.hpp:33-53): the forward transform against FP64
+    numpy (within 1e-5 of the RMS), and forward then inverse gives n times
+    the input (unnormalised, as cufftExecC2C)."""
+    rng = np.random.default_rng(n + batch)
+    z = (rng.standard_normal((batch, n)) + 1j * rng.standard_normal((batch, n))).astype(
+        np.complex64)
+    fft = T.CuFFTerC2C(n, batch)
+    assert fft.get_output_size() == n
+    a, b = _dev(z.view(np.float32)), _dev(np.zeros((batch, 2 * n), np.float32))
+    fft.execute(a, b, -1)
+    got = _host(b).view(np.complex64)
+    want = np.fft.fft(z.astype(np.complex128), axis=1)
+    assert err_vs_rms(got, want) < 1e-5
+    fft.execute(b, b, +1)   # in place
+    assert err_vs_rms(_host(b).view(np.complex64), n * z.astype(np.complex128)) < 1e-5
+    from peasoup_b200._lib import PsxError
+    with pytest.raises(PsxError):
+        fft.execute(a, b, 0)
+
+
 def test_fft_vs_reference(T, ref_gpu):
     rng = np.random.default_rng(3)
     n = 1 << 16
@@ -305,3 +327,29 @@ def test_batched_resample_matches_single(psx, cuda):
         assert psx.psx_resampleII(C.c_void_p(x.data_ptr()), C.c_void_p(one.data_ptr()), n,
                                   float(a), float(TS), None) == 0
         assert torch.equal(one, out[t])
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.int8])
+@pytest.mark.parametrize("n", [1, 1000, (1 << 20) + 3])
+def test_convert_8bit_vs_reference(T, psx, ref_gpu, dtype, n):
+    """psx_convert_u8_f32 / psx_convert_i8_f32 (the conversion after the
+    host->device copy of 8-bit series) against numpy's cast and against the
+    reference's own ReusableDeviceTimeSeries::copy_from_host
+    (conversion_kernel, src/kernels.cu:1171-1200): exact, the edge values
+    0, 127, -128 (int8) and 255 (uint8) included."""
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(n)
+    info = np.iinfo(dtype)
+    x = rng.integers(info.min, int(info.max) + 1, n, dtype=np.int64).astype(dtype)
+    edges = np.array([0, 127, info.min, info.max, 1, info.max - 1], np.int64).astype(dtype)
+    x[:min(n, edges.size)] = edges[:min(n, edges.size)]
+    d_in = _dev(x)
+    d_out = torch.full((n,), -1.0, dtype=torch.float32, device="cuda")
+    fn = psx.psx_convert_u8_f32 if dtype == np.uint8 else psx.psx_convert_i8_f32
+    rc = fn(C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), C.c_size_t(n),
+            C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, psx.psx_last_error()
+    got = _host(d_out)
+    assert np.array_equal(got, x.astype(np.float32))
+    assert np.array_equal(got, ref_gpu.ref_copy_from_host_8bit(x))

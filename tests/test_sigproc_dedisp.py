@@ -12,7 +12,10 @@ import pytest
 
 from peasoup_b200 import _lib, sigproc
 
-TUTORIAL = "/root/reference/example_data/tutorial.fil"
+# The reference's example filterbank (250 ms pulsar at DM 30), as the
+# oracle's build stages it beside the reference's built libraries.
+TUTORIAL = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle",
+                        "_ref", "tutorial.fil")
 
 
 def _hdr_dict(h):
