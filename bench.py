@@ -204,6 +204,7 @@ def _standalone(name):
     spec = importlib.util.spec_from_file_location(
         f"_bench_{name}", os.path.join(ROOT, "peasoup_b200", f"{name}.py"))
     mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod   # dataclasses look their module up there
     spec.loader.exec_module(mod)
     return mod
 
