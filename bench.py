@@ -23,11 +23,13 @@ workload (Poisson arrivals of uneven segmented searches through the C++
 server, p50/p95/p99 latency from arrival and from admission, each request
 also run alone for the ratios); `roofline` = the
 dominant stage's achieved HBM bytes/s against the measured copy bandwidth;
-`cpu_baseline` = the FP64 CPU oracle on a bounded sample.
+`cpu_baseline` = an FP32 C++ rendering of the same stages (MKL FFT through
+libtorch) on one whole DM trial, on every host core.
 
 `--impl reference` times the reference's own implementation of the path
-(its src/kernels.cu, transforms and unmodified Worker, built for sm_100a
-into oracle/_ref) on the same workload, one DM trial per step.
+(its src/kernels.cu, transforms and unmodified Worker::start, built for
+sm_100a into oracle/_ref) over the same DM trials of the same series, one
+Worker for the whole list as the reference's program runs it.
 """
 from __future__ import annotations
 
@@ -324,30 +326,9 @@ def run_reference(args, ws, rank):
 
 
 # ----------------------------------------------------------------- CPU baseline
-def _oracle_params(plan, dm, lo, hi):
-    from peasoup_b200 import synth
-    return dict(fft_size=N_FFT, tsamp=TSAMP, dm=float(dm), acc_lo=lo, acc_hi=hi,
-                nharmonics=NFOLDS, cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ,
-                birdie_freqs=np.asarray(plan.birdie_freqs), birdie_widths=np.asarray(plan.birdie_widths))
-
-
-def _oracle_init():
-    from oracle import oracle as O
-    O.lib()
-
-
-def _oracle_job(job):
-    """One oracle DM search (run in a spawned worker); its own elapsed time."""
-    x, kw = job
-    from oracle import oracle as O
-    t0 = time.perf_counter()
-    O.search_dm(x, O.SearchParams(**kw))
-    return time.perf_counter() - t0
-
-
 def _cpu_workers():
-    """Host threads for the parallel sample: every core, bounded by memory
-    (about 1.5 GB per FP64 2^23 search) and by 32."""
+    """Spawned processes for the dedispersion CPU sample: every core,
+    bounded by memory (about 1.5 GB each) and by 32."""
     n = os.cpu_count() or 1
     try:
         with open("/proc/meminfo") as f:
@@ -358,27 +339,30 @@ def _cpu_workers():
     return max(1, min(n, 32))
 
 
+def _cpu_threads():
+    """Host threads for the CPU baseline: every core, at most 64."""
+    return max(1, min(os.cpu_count() or 1, 64))
+
+
 def cpu_baseline(plan, block_row, dm):
-    """FP64 oracle on a bounded sample: one DM trial with 1 and with 3
-    acceleration trials on one core separates the per-trial and per-DM
-    costs; the 3-trial search run on every worker at once (spawned
-    processes, one per core) gives the parallel efficiency.  Throughput is
-    extrapolated to the workload's trials per DM."""
-    import multiprocessing as mp
-    from concurrent.futures import ProcessPoolExecutor
+    """The FP32 CPU rendering of the same stages (oracle/cpu_render.cpp:
+    the per-trial loop in FP32 with libtorch's MKL-backed FFT, FFTW being
+    absent here; trials spread over one thread per core) on one whole DM
+    trial of the workload, every acceleration trial of it included.
+    Returns (trials per second, threads, trials, seconds)."""
+    from oracle import oracle as O
+    from peasoup_b200 import synth
+    p = O.SearchParams(fft_size=N_FFT, tsamp=TSAMP, dm=float(dm), acc_lo=-ACC, acc_hi=ACC,
+                       nharmonics=NFOLDS, cfreq=synth.CFREQ_HZ, ch_bw=synth.CH_BW_HZ,
+                       birdie_freqs=np.asarray(plan.birdie_freqs),
+                       birdie_widths=np.asarray(plan.birdie_widths))
+    ntr = len(O.accel_list(-ACC, ACC, 1.10, 64e-6, N_FFT, TSAMP, synth.CFREQ_HZ,
+                           synth.CH_BW_HZ, float(dm), 0.0))
+    threads = _cpu_threads()
     x = np.ascontiguousarray(block_row, np.float32)
-    t1 = _oracle_job((x, _oracle_params(plan, dm, 0.0, 0.0)))
-    t3 = _oracle_job((x, _oracle_params(plan, dm, -1.0, 1.0)))   # {-1, 0, 1}: three trials
-    per_trial = max(1e-9, (t3 - t1) / 2.0)
-    per_dm = max(0.0, t1 - per_trial)
-    cores = _cpu_workers()
-    par = [t3]
-    if cores > 1:
-        with ProcessPoolExecutor(cores, mp_context=mp.get_context("spawn"),
-                                 initializer=_oracle_init) as ex:
-            par = list(ex.map(_oracle_job, [(x, _oracle_params(plan, dm, -1.0, 1.0))] * cores))
-    eff = t3 / (sum(par) / len(par))
-    return per_trial, per_dm, cores, eff, t1 + t3 + max(par)
+    _, _, sec = O.cpu_search_dm(x, p, threads)
+    return ntr / sec, threads, ntr, sec
+
 
 # ----------------------------------------------------------------- served
 def _pct(v, q):
@@ -511,6 +495,61 @@ def _pulse_block_torch(ndm, n, ts, seed, pulsar=(5.7e-3, 12.0, 0.05, 0.3), sigma
     return out
 
 
+def stage_roofline(prof, n, form_used, shape_used, peak, peak_kind, traffic_json=True,
+                   sm_mhz=None):
+    """Per-stage device time per trial (CUDA events around every launch
+    group of a profiled run: prof from AccelSearch.profile) and each stage's
+    algorithmic bytes per trial; the dominant stage's achieved HBM bytes/s
+    against the measured copy bandwidth.  Algorithmic bytes per trial of N
+    samples (B = N/2 + 1 bins): resample 8N (read + write the series), the
+    transform 4N + 8B, forming and normalising 12B, the harmonic kernel 4B
+    (the normalised spectrum read once); with the two-pass transform, pass 1
+    8N (gather the series, write M complex) and pass 2 8N."""
+    B = n // 2 + 1
+    per_trial_bytes = {"resample": 8.0 * n, "fft": 4.0 * n + 8.0 * B, "form": 12.0 * B,
+                       "harm": 4.0 * B}
+    stage_kernels = {"resample": "k_resample", "fft": "cuFFT", "form": "k_unpack_form_norm",
+                     "harm": "k_harm_rows" if shape_used >= 6 else "k_harm_tiles"}
+    if form_used == 3:
+        per_trial_bytes.update(resample=8.0 * n, fft=8.0 * n)
+        stage_kernels.update(resample="k_fft4_cols (gather + column transforms)",
+                             fft="k_fft4_rows (row transforms)", form="k_unpack_form_norm_t")
+    stage_ms = {"resample": prof["resample_ms"], "fft": prof["fft_ms"],
+                "form": prof["form_ms"], "harm": prof["harm_ms"]}
+    trials_prof = max(1, prof["trials"])
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if traffic_json and os.path.exists(tp) and n == N_FFT:
+        tj = json.load(open(tp))
+        tkey = "harm_rows" if (dom == "harm" and shape_used >= 6) else dom
+        traffic = (tj.get("two_pass", {}) if form_used == 3 else tj).get(tkey)
+    stages = {}
+    for k, ms in stage_ms.items():
+        sec = ms / 1e3 / trials_prof
+        stages[k] = {"us_per_trial": sec * 1e6, "kernel": stage_kernels[k],
+                     "gbs": per_trial_bytes[k] / sec / 1e9 if sec > 0 else None}
+    achieved = stages[dom]["gbs"]
+    out = {"bound": "hbm", "kernel": stage_kernels[dom], "stage": dom, "achieved": achieved,
+           "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+           "traffic": traffic, "peak_kind": peak_kind, "bytes_per_trial": per_trial_bytes[dom],
+           "stages": stages}
+    if dom == "harm":
+        # the harmonic kernel's limiter is the SM's shared-memory bandwidth
+        # (128 B per clock): per output bin 31 fraction loads + 1 tile load
+        # (one 4-byte lane word each, 128 B) plus the windows the tensor
+        # copies write (16.5 floats, 66 B)
+        out["limiter"] = "shared-memory bandwidth (tensor-copy writes + 32 loads per bin)"
+        out["smem_bytes_per_trial"] = 194.0 * B
+        if sm_mhz:
+            sec = stages["harm"]["us_per_trial"] / 1e6
+            smem_peak = 128.0 * 148 * sm_mhz * 1e6
+            out["smem_gbs"] = 194.0 * B / sec / 1e9
+            out["smem_peak_gbs"] = smem_peak / 1e9
+            out["smem_frac"] = 194.0 * B / sec / smem_peak
+    return out
+
+
 def _timed_block(eng, rows, dms, stream, chunk):
     """Searches rows in chunks through psx_search_block; CUDA-event time on
     the engine's stream.  Returns (seconds, candidate arrays per chunk)."""
@@ -560,6 +599,18 @@ def run_config3(args):
     with ClockSampler(0) as clk:
         tb, outs_b = _timed_block(eng, rows, dms, stream, 64)
     clocks = clk.summary()
+    # per-stage device times (CUDA events around every launch group, no
+    # graph capture) on the first 128 DM trials, for the stage roofline
+    eng.set_profile(True)
+    eng.profile(reset=True)
+    _timed_block(eng, rows[:128], dms[:128], stream, 64)
+    prof = eng.profile(reset=True)
+    eng.set_profile(False)
+    info = eng.info()
+    peak, peak_kind = peaks()
+    roofline = stage_roofline(prof, n, info["fft_form"], info["harm_shape"], peak, peak_kind,
+                              sm_mhz=clocks.get("sm_mhz"))
+    roofline["prologue_span_us_per_dm"] = 1e3 * prof["prologue_ms"] / max(1, prof["dms"])
     nsample = min(ndm, args.plain_sample)
     sel = np.linspace(0, ndm - 1, nsample).astype(int)
     engp = search.AccelSearch(params("plain"))
@@ -593,6 +644,7 @@ def run_config3(args):
         "candidate_sets_equal_on_plain_sample": bool(same),
         "candidates_compared": len(kp), "snr_worst_rel": worst,
         "hbm_roofline_frac": (ndm * 24.0 * n + tot_b * 12.0 * n) / tb / (peaks()[0] * 1e9),
+        "roofline": roofline,
         "clocks": clocks,
         "workload": "2048 DM x 2^22, tsamp 64us, white N(0,1) + P=5.7ms 5% duty 0.3 sigma "
                     "pulsar at +12 m/s^2 in every row, acc -50..50 (15 trials at DM 0), "
@@ -659,6 +711,17 @@ def run_config5(args):
         res[mode] = {"value": tot / est, "per_trial_us": 1e6 * per_trial,
                      "per_dm_ms": 1e3 * per_dm, "subset": [{"trials": a, "seconds": b}
                                                            for a, b in fit]}
+    # per-stage device times of the batched engine (CUDA events around every
+    # launch group) on the larger subset, for the roofline of its stages
+    eng = search.AccelSearch(params("batched", 2.0, tune["batch"], tune["harm_shape"]))
+    eng.set_stream(stream.cuda_stream)
+    eng.set_profile(True)
+    _timed_block(eng, rows, plan.dms[dsel], stream, nuse)
+    prof = eng.profile(reset=True)
+    info = eng.info()
+    eng.close()
+    peak, peak_kind = peaks()
+    roofline = stage_roofline(prof, n, info["fft_form"], info["harm_shape"], peak, peak_kind)
     print(json.dumps({
         "metric": "DM x accel trials/s, config 5 (2^27, 64 DM, acc +-500), extrapolated",
         "config_id": 5, "value": res["batched"]["value"], "unit": "trials/s",
@@ -666,6 +729,8 @@ def run_config5(args):
         "batched_over_plain": res["batched"]["value"] / res["plain"]["value"],
         "trials_full": int(sum(full)), "trials_dm0": full[0],
         "batch": tune["batch"], "harm_shape": tune["harm_shape"],
+        "fft_form": FFT_FORMS.get(info["fft_form"], str(info["fft_form"])),
+        "roofline": roofline,
         "hbm_roofline_frac": ((24.0 * n * ndm + 12.0 * n * sum(full)) /
                               (ndm * res["batched"]["per_dm_ms"] / 1e3 +
                                sum(full) * res["batched"]["per_trial_us"] / 1e6) /
@@ -818,50 +883,15 @@ def run_psx(args, ws, rank, local):
         eng_p.close()
 
     # ---- roofline of the dominant stage (CUDA events on the engine stream)
-    B = N_FFT // 2 + 1
-    per_trial_bytes = {  # algorithmic bytes per acceleration trial and stage
-        "resample": 8.0 * N_FFT,          # read + write the series
-        "fft": 4.0 * N_FFT + 8.0 * B,     # read the series, write the spectrum
-        "form": 8.0 * B + 4.0 * B,        # read the spectrum, write the amplitudes
-        "harm": 4.0 * B,                  # read the normalised spectrum once
-    }
-    stage_kernels = {"resample": "k_resample", "fft": "cuFFT", "form": "k_unpack_form_norm",
-                     "harm": "k_harm_rows" if shape_used >= 6 else "k_harm_tiles"}
-    if form_used == 3:
-        # the two-pass transform: pass 1 (timed as "resample") gathers the
-        # series (4N bytes) and writes the column transforms (M complex =
-        # 4N bytes); pass 2 reads them and writes the spectrum (4N + 4N)
-        per_trial_bytes["resample"] = 8.0 * N_FFT
-        per_trial_bytes["fft"] = 8.0 * N_FFT
-        stage_kernels.update(resample="k_fft4_cols (gather + column transforms)",
-                             fft="k_fft4_rows (row transforms)", form="k_unpack_form_norm_t")
-    stage_ms = {"resample": prof["resample_ms"], "fft": prof["fft_ms"],
-                "form": prof["form_ms"], "harm": prof["harm_ms"]}
-    trials_prof = max(1, prof["trials"])
-    dom = max(stage_ms, key=lambda k: stage_ms[k])
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tp):
-        tj = json.load(open(tp))
-        tkey = "harm_rows" if (dom == "harm" and shape_used >= 6) else dom
-        traffic = (tj.get("two_pass", {}) if form_used == 3 else tj).get(tkey)
-    stages = {}
-    for k, ms in stage_ms.items():
-        sec = ms / 1e3 / trials_prof
-        stages[k] = {"us_per_trial": sec * 1e6, "kernel": stage_kernels[k],
-                     "gbs": per_trial_bytes[k] / sec / 1e9 if sec > 0 else None}
-    achieved = stages[dom]["gbs"]
-    roofline = {"bound": "hbm", "kernel": stage_kernels[dom], "stage": dom,
-                "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                "traffic": traffic, "peak_kind": peak_kind,
-                "bytes_per_trial": per_trial_bytes[dom], "stages": stages,
-                "prologue_span_us_per_dm": 1e3 * prof["prologue_ms"] / max(1, prof["dms"]),
-                "prologue_note": "the prologue of DM d+1 runs on its own stream alongside the "
-                                 "trials of DM d, so its span includes sharing the GPU",
-                "timing": "CUDA events per launch group on the engine stream, over a "
-                          "re-run of the timed steps without graph capture "
-                          f"({value_profiled:.0f} trials/s)"}
+    roofline = stage_roofline(prof, N_FFT, form_used, shape_used, peak, peak_kind,
+                              sm_mhz=clocks.get("sm_mhz"))
+    roofline.update({
+        "prologue_span_us_per_dm": 1e3 * prof["prologue_ms"] / max(1, prof["dms"]),
+        "prologue_note": "the prologue of DM d+1 runs on its own stream alongside the "
+                         "trials of DM d, so its span includes sharing the GPU",
+        "timing": "CUDA events per launch group on the engine stream, over a "
+                  "re-run of the timed steps without graph capture "
+                  f"({value_profiled:.0f} trials/s)"})
     # end-to-end algorithmic roofline of the whole search (12N per trial,
     # 24N per DM prologue)
     ndm_total = sum_over_ranks(ws, sum(len(st) for st in timed))
@@ -872,17 +902,13 @@ def run_psx(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu:
         d0 = timed[0][0]
         x = block[row[d0]].cpu().numpy()
-        per_trial, per_dm, cores, eff, spent = cpu_baseline(plan, x, plan.dms[d0])
-        avg_trials = ntr / max(1, sum(len(st) for st in timed))
-        cpu_v = cores * eff * avg_trials / (per_dm + avg_trials * per_trial)
-        cpu = {"value": cpu_v, "unit": "trials/s", "cores": cores, "kind": "port",
-               "sample": (f"FP64 oracle (the project's C restatement; no FFTW in the image), "
-                          f"one 2^23 DM trial with 1 and with 3 acceleration trials on one "
-                          f"core: {per_trial:.2f}s per trial, {per_dm:.2f}s per DM prologue; "
-                          f"the 3-trial search on {cores} spawned processes at once ran at "
-                          f"{eff:.2f} of the one-core speed; extrapolated to "
-                          f"{avg_trials:.1f} trials per DM over {cores} cores "
-                          f"({spent:.1f}s of sampling)")}
+        cpu_v, threads, cpu_tr, cpu_s = cpu_baseline(plan, x, plan.dms[d0])
+        cpu = {"value": cpu_v, "unit": "trials/s", "cores": threads, "kind": "port",
+               "sample": (f"FP32 C++ rendering of the same stages (oracle/cpu_render.cpp; "
+                          f"libtorch's MKL FFT in place of FFTW, absent in the image) on one "
+                          f"whole DM trial of the workload (DM {float(plan.dms[d0]):g}, "
+                          f"{cpu_tr} acceleration trials) on {threads} host threads: "
+                          f"{cpu_s:.2f}s; the FP64 oracle is the checker only")}
     eng.close()
     served = None
     if rank == 0 and ws == 1 and args.served > 0:
@@ -932,17 +958,22 @@ def run_case(args):
     from peasoup_b200.build import build
     build()
     ndm = args.ndm or 2
-    plan = synth.survey_plan(ndm=NDM, nsamps=N_FFT, tsamp=TSAMP)
+    n = args.case_nsamps or N_FFT
+    plan = synth.survey_plan(ndm=NDM, nsamps=n, tsamp=TSAMP)
     block = synth.survey_block_torch(plan, dm_indices=list(range(ndm)))
     pr = make_params(plan, "batched", args.batch, args.harm_shape)
+    pr.fft_size = n
     pr.fft_form = args.fft_form
+    if args.case_acc > 0:
+        pr.acc_lo, pr.acc_hi = -args.case_acc, args.case_acc
     s = search.AccelSearch(pr)
     s.set_profile(True)
     counts = []
     for d in range(ndm):
         counts.append(len(s.search(block[d], float(plan.dms[d]), d)[0]))
     torch.cuda.synchronize()
-    print(json.dumps({"workload": "case", "ndm": ndm, "candidates": counts, "info": s.info(),
+    print(json.dumps({"workload": "case", "nsamps": n, "ndm": ndm, "candidates": counts,
+                      "info": s.info(),
                       "profile": s.profile()}), flush=True)
     s.close()
     return 0
@@ -1114,6 +1145,10 @@ def main():
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
                     help="2: the headline survey workload; 3 and 5: the other throughput "
                          "configurations (one JSON line each)")
+    ap.add_argument("--case-nsamps", type=int, default=0,
+                    help="--workload case: transform length (default 2^23)")
+    ap.add_argument("--case-acc", type=float, default=0.0,
+                    help="--workload case: acceleration half-range (default 100 m/s^2)")
     ap.add_argument("--ndm", type=int, default=0,
                     help="configs 3/5: DM trials to time; --workload case: DM trials searched")
     ap.add_argument("--plain-sample", type=int, default=128,

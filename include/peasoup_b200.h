@@ -604,8 +604,10 @@ double psx_server_clock(psx_server* srv);
    request completes; the config (birdies included) is copied.  Requests
    are admitted first in, first out, when a worker is free and the new
    instance they need fits the budget (a pooled instance with the same
-   shape is reused).  PSX_ERR_BUSY: queue full; PSX_ERR_ALLOC: larger than
-   the whole budget. */
+   shape is reused).  Of the requests running at once, the one with the
+   least work (acceleration trials times transform length over its DM
+   trials) runs at the higher stream priority (psx_search_set_priority).
+   PSX_ERR_BUSY: queue full; PSX_ERR_ALLOC: larger than the whole budget. */
 int psx_server_submit(psx_server* srv, const psx_search_config* cfg,
                       const float* const* series, size_t nsamps,
                       int series_on_device, const float* dms,

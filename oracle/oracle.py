@@ -407,6 +407,57 @@ def search_dm(series, p: SearchParams, tap_trial: int = -1):
     return res
 
 
+# ------------------------------------------------- FP32 CPU rendering
+CPU_RENDER_PATH = os.path.join(HERE, "_build", "libcpu_render.so")
+_cpu = None
+
+
+def build_cpu_render() -> None:
+    """Compile the FP32 CPU rendering (g++ against libtorch; about 30 s)."""
+    subprocess.run(["make", "-s", "-C", HERE, "cpu"], check=True)
+
+
+def cpu_render():
+    global _cpu
+    if _cpu is None:
+        if not os.path.exists(CPU_RENDER_PATH):
+            build_cpu_render()
+        lib()  # the stage functions it links are the oracle's
+        L = C.CDLL(CPU_RENDER_PATH)
+        L.cpu_search_dm.restype = C.c_size_t
+        L.cpu_search_dm.argtypes = [_fp, C.c_size_t, C.POINTER(_Params), C.c_int, C.c_void_p,
+                                    C.c_void_p, C.c_size_t, C.POINTER(C.c_double)]
+        _cpu = L
+    return _cpu
+
+
+def cpu_search_dm(series, p: SearchParams, nthreads: int):
+    """The FP32 CPU rendering of one DM trial on `nthreads` host threads:
+    per-trial harmonic-distilled candidates (as search_dm), the trial index
+    of each, and the wall time of the DM trial in seconds."""
+    series = np.ascontiguousarray(series, np.float32)
+    bf = np.ascontiguousarray(p.birdie_freqs, np.float32)
+    bw = np.ascontiguousarray(p.birdie_widths, np.float32)
+    cp = _Params(p.fft_size, p.tsamp, p.dm, p.cdm, p.dm_idx, p.acc_lo, p.acc_hi,
+                 p.acc_tol, p.acc_pulse_width, p.cfreq, p.ch_bw, p.nharmonics,
+                 p.min_snr, p.min_freq, p.max_freq, p.min_gap, p.freq_tol, p.max_harm,
+                 bf.ctypes.data_as(C.POINTER(C.c_float)),
+                 bw.ctypes.data_as(C.POINTER(C.c_float)), bf.size, p.resample_fused)
+    cap = 1 << 16
+    sec = C.c_double()
+    while True:
+        out = np.zeros(cap, CAND_DTYPE)
+        trial = np.zeros(cap, np.int32)
+        n = cpu_render().cpu_search_dm(series, series.size, C.byref(cp), int(nthreads),
+                                       out.ctypes.data, trial.ctypes.data, cap, C.byref(sec))
+        if n != (1 << 64) - 1:
+            break
+        if cap > (1 << 24):
+            raise RuntimeError("CPU rendering failed")
+        cap *= 4
+    return out[:n].copy(), trial[:n].copy(), sec.value
+
+
 # ---------------------------------------------------------------- reference
 _ref_host = None
 _ref_gpu = None

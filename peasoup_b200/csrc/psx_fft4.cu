@@ -37,7 +37,6 @@ namespace psx {
 
 namespace {
 
-constexpr int kColsW = 8;  // columns per pass-1 CTA
 
 // cos(k pi / 16), k = 0..8
 __host__ __device__ constexpr float cos_pi16(int k)
@@ -139,41 +138,61 @@ __device__ __forceinline__ void dft3(float2& a, float2& b, float2& c)
 }
 
 // ------------------------------------------------------------- pass 1
-// Shared layout [e][col], e the row index 0..1023; a row of 8 columns is 64
-// bytes.  Flipping bit 0 of e by bit 4 spreads the four rows a warp touches
-// at once (four consecutive t) two to each half of the banks in every
-// exchange below.
-__device__ __forceinline__ unsigned swz_a(unsigned e) { return e ^ ((e >> 4) & 1u); }
+// Column shape of pass 1 for column length R: W columns per CTA, J = R/16
+// radix-16 butterflies per column in the first two stages, TPC threads per
+// column (J, at least 64), a last stage of radix R3 = R/256 with U = 256/TPC
+// butterflies per thread.  Every shape has 512 threads, 16 elements (12 for
+// R = 768) per thread and R * W * 8 <= 64 KB of shared memory.
+template <int R>
+struct ColShape {
+    static constexpr int W = R == 4096 ? 2 : R == 2048 ? 4 : 8;
+    static constexpr int J = R / 16;
+    static constexpr int TPC = J < 64 ? 64 : J;
+    static constexpr int R3 = R / 256;
+    static constexpr int U = 256 / TPC;
+    static constexpr int THREADS = W * TPC;
+    static constexpr size_t SMEM = (size_t)R * W * sizeof(float2);
+};
 
-// Column length R = 1024 (stages of radix 16, 16, 4) or 768 (16, 16, 3, for
-// transform lengths 3 * 2^k); 64 threads per column, of which R/16 take the
-// radix-16 stages and all take 4 butterflies of the last stage.
+// Shared layout [e][col], e the row index 0..R-1; a row of W columns spans
+// 2W of the 32 banks.  XOR-ing the low bits of e with bits 4.. of e (16/W
+// row groups) spreads the rows a warp touches at once (32/W consecutive t)
+// over all the banks in every exchange below: two wavefronts per 64-bit
+// access, the minimum.
+template <int W>
+__device__ __forceinline__ unsigned swz_a(unsigned e)
+{
+    return e ^ ((e >> 4) & (16u / W - 1u));
+}
+
+// Column length R = 768 (stages of radix 16, 16, 3, for transform lengths
+// 3 * 2^k), 1024 (16, 16, 4), 2048 (16, 16, 8) or 4096 (16, 16, 16).
 // DUMP: write the gathered pairs z[e C + c] (the resampled series as it is
 // read, interleaved) to y instead of transforming them (the debug tap).
 template <int R, bool DUMP>
-__global__ void __launch_bounds__(kColsW * 64, 2)
+__global__ void __launch_bounds__(ColShape<R>::THREADS, 2)
     k_fft4_cols(const float* __restrict__ x, unsigned long long n, const double* __restrict__ ktab,
                 const float2* __restrict__ tab, unsigned offA2, unsigned offA3, unsigned offQ,
                 unsigned offP, unsigned C, float2* __restrict__ y, size_t ypitch)
 {
-    static_assert(R == 1024 || R == 768, "column length");
-    constexpr int W = kColsW;
-    constexpr int J = R / 16;   // radix-16 butterflies per column and stage
-    constexpr int R3 = R / 256;  // radix of the last stage
+    using S = ColShape<R>;
+    static_assert(R == 768 || R == 1024 || R == 2048 || R == 4096, "column length");
+    static_assert(S::THREADS == 512 && S::U * S::R3 <= 16, "column shape");
+    constexpr int W = S::W, J = S::J, TPC = S::TPC, R3 = S::R3, U = S::U;
     extern __shared__ float2 sm_a[];
-    const unsigned col = threadIdx.x % W, t = threadIdx.x / W;  // t in [0, 64)
+    const unsigned col = threadIdx.x % W, t = threadIdx.x / W;  // t in [0, TPC)
     const unsigned c = blockIdx.x * W + col;
     const double k = ktab[blockIdx.y], size = (double)n;
     float2 v[16];
     // stage 1 (radix 16, span 1): rows e = t + J q of column c, where
     // z[e C + c] = (x'[2m], x'[2m+1]); out[16 t + q]
-    if (J == 64 || t < (unsigned)J) {  // every thread when R = 1024
+    if (J == TPC || t < (unsigned)J) {  // every thread unless R = 768
         const double i_first = 2.0 * ((double)t * (double)C + (double)c);
         const double i_step = 2.0 * J * (double)C;
         const unsigned n32 = (unsigned)n;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
-            const double i0 = i_first + (double)q * i_step;  // exact: integers < 2^26
+            const double i0 = i_first + (double)q * i_step;  // exact: integers < 2^28
             v[q].x = resampleII_read(x, i0, k, size, n32);
             v[q].y = resampleII_read(x, i0 + 1.0, k, size, n32);
         }
@@ -184,58 +203,60 @@ __global__ void __launch_bounds__(kColsW * 64, 2)
         } else {
             dft<16>(v);
 #pragma unroll
-            for (int q = 0; q < 16; ++q) sm_a[swz_a(16 * t + q) * W + col] = v[q];
+            for (int q = 0; q < 16; ++q) sm_a[swz_a<W>(16 * t + q) * W + col] = v[q];
         }
     }
     if constexpr (DUMP) return;
     __syncthreads();
     // stage 2 (radix 16, span 16): in[t + J q] * W_256^((t mod 16) q),
     // out[(t / 16) 256 + t mod 16 + 16 q]
-    if (J == 64 || t < (unsigned)J) {  // every thread when R = 1024
+    if (J == TPC || t < (unsigned)J) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = sm_a[swz_a(t + J * q) * W + col];
+        for (int q = 0; q < 16; ++q) v[q] = sm_a[swz_a<W>(t + J * q) * W + col];
     }
     __syncthreads();
-    if (J == 64 || t < (unsigned)J) {  // every thread when R = 1024
+    if (J == TPC || t < (unsigned)J) {
 #pragma unroll
         for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], __ldg(tab + offA2 + q * 16 + (t & 15)));
         dft<16>(v);
         const unsigned base2 = (t >> 4) * 256 + (t & 15);
 #pragma unroll
-        for (int q = 0; q < 16; ++q) sm_a[swz_a(base2 + 16 * q) * W + col] = v[q];
+        for (int q = 0; q < 16; ++q) sm_a[swz_a<W>(base2 + 16 * q) * W + col] = v[q];
     }
     __syncthreads();
-    // stage 3 (radix R3, span 256): butterflies j = t + 64 u, in[j + 256 q]
-    // * W_R^(j q), out[j + 256 q] = row k1 = t + 64 (u + 4 q)
+    // stage 3 (radix R3, span 256): butterflies j = t + TPC u, in[j + 256 q]
+    // * W_R^(j q), out[j + 256 q] = row k1 = t + TPC (u + U q)
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int q = 0; q < R3; ++q) v[4 * u + q] = sm_a[swz_a(t + 64 * u + 256 * q) * W + col];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        float2 b[4];
+    for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int q = 0; q < R3; ++q)
-            b[q] = q ? cmul(v[4 * u + q], __ldg(tab + offA3 + q * 256 + t + 64 * u)) : v[4 * u];
-        if constexpr (R3 == 4) {
-            dft<4>(b);
-        } else {
+            v[R3 * u + q] = sm_a[swz_a<W>(t + TPC * u + 256 * q) * W + col];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        float2 b[R3];
+#pragma unroll
+        for (int q = 0; q < R3; ++q)
+            b[q] = q ? cmul(v[R3 * u + q], __ldg(tab + offA3 + q * 256 + t + TPC * u))
+                     : v[R3 * u];
+        if constexpr (R3 == 3) {
             dft3(b[0], b[1], b[2]);
+        } else {
+            dft<R3>(b);
         }
 #pragma unroll
-        for (int q = 0; q < R3; ++q) v[4 * u + q] = b[q];
+        for (int q = 0; q < R3; ++q) v[R3 * u + q] = b[q];
     }
-    // four-step twiddle W_M^(c k1), k1 = t + 64 w (w = u + 4 q):
-    // W_M^(c t) * W_M^(64 c w)
+    // four-step twiddle W_M^(c k1), k1 = t + TPC w (w = u + U q):
+    // W_M^(c t) * W_M^(TPC c w)
     const float2 wt = __ldg(tab + offQ + (size_t)t * C + c);
     float2* yo = y + (size_t)blockIdx.y * ypitch;
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < U; ++u)
 #pragma unroll
         for (int q = 0; q < R3; ++q) {
-            const unsigned w = u + 4 * q;
+            const unsigned w = u + U * q;
             const float2 tw = w ? cmul(wt, __ldg(tab + offP + (size_t)w * C + c)) : wt;
-            yo[(size_t)(t + 64 * w) * C + c] = cmul(v[4 * u + q], tw);
+            yo[(size_t)(t + TPC * w) * C + c] = cmul(v[R3 * u + q], tw);
         }
 }
 
@@ -458,13 +479,63 @@ void row_stages(int logc, std::vector<std::pair<int, int>>& out)
     }
 }
 
+template <int R>
+int configure_cols()
+{
+    using S = ColShape<R>;
+    // (the default shared/L1 split: measured on B200, forcing the largest
+    // shared carve-out slowed the gather of pass 1 and the twiddle reads of
+    // pass 2, both served from L1)
+    return cuda_status(cudaFuncSetAttribute(k_fft4_cols<R, false>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)S::SMEM),
+                       "fft4 column pass attribute");
+}
+
 }  // namespace
+
+template <int R, bool DUMP>
+void Fft4Plan::launch_cols(const Fft4Plan& f, const float* series, const double* ktab,
+                           int ntrials, float2* y, size_t ypitch, cudaStream_t s)
+{
+    using S = ColShape<R>;
+    dim3 ga(f.C / S::W, (unsigned)ntrials);
+    k_fft4_cols<R, DUMP><<<ga, S::THREADS, DUMP ? 0 : S::SMEM, s>>>(
+        series, (unsigned long long)f.n, ktab, f.d_tab, f.offA2, f.offA3, f.offQ, f.offP, f.C, y,
+        ypitch);
+}
 
 bool Fft4Plan::supported(size_t n)
 {
     auto pow2 = [](size_t v) { return v && (v & (v - 1)) == 0; };
-    if (pow2(n)) return n >= (size_t(1) << 19) && n <= (size_t(1) << 25);
+    if (pow2(n)) return n >= (size_t(1) << 19) && n <= (size_t(1) << 27);
     return n % 3 == 0 && pow2(n / 3) && n / 3 >= (size_t(1) << 17) && n / 3 <= (size_t(1) << 23);
+}
+
+// Rows of the four-step split: 768 for 3 * 2^k, else 1024 up to M = 2^24
+// (N = 2^25), 2048 at M = 2^25 and 4096 at M = 2^26, so that the row length
+// C = M / R never exceeds 2^14 (one CTA's shared memory).
+unsigned Fft4Plan::rows_for(size_t n)
+{
+    const size_t m = n / 2;
+    if (n % 3 == 0) return 768u;
+    return m <= (size_t(1) << 24) ? 1024u : m == (size_t(1) << 25) ? 2048u : 4096u;
+}
+
+// Threads per column of pass 1 (the range of t in the four-step twiddle).
+static unsigned cols_tpc(unsigned r) { return r / 16 < 64 ? 64u : r / 16; }
+
+size_t Fft4Plan::table_floats2(size_t n)
+{
+    const unsigned r = rows_for(n), c = (unsigned)(n / 2 / r);
+    int lc = 0;
+    while ((1u << lc) < c) ++lc;
+    std::vector<std::pair<int, int>> st;
+    row_stages(lc, st);
+    size_t rows = 0;
+    for (auto& e : st) rows += (size_t)e.first * e.second;
+    return 256 + (size_t)(r / 256) * 256 + (size_t)cols_tpc(r) * c + 16 * (size_t)c +
+           (r + 33) + c / 2 + rows;
 }
 
 void Fft4Plan::destroy()
@@ -479,13 +550,14 @@ int Fft4Plan::create(size_t n_)
 {
     destroy();
     if (!supported(n_)) {
-        set_error("fft4: unsupported length %zu (2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23)", n_);
+        set_error("fft4: unsupported length %zu (2^19 .. 2^27 or 3 * 2^17 .. 3 * 2^23)", n_);
         return PSX_ERR_INVALID;
     }
     const unsigned long long M = n_ / 2;
-    const unsigned Rn = (n_ % 3 == 0) ? 768u : 1024u;
+    const unsigned Rn = rows_for(n_);
     const unsigned R3 = Rn / 256;
     const unsigned Cn = (unsigned)(M / Rn);
+    const unsigned tpc = cols_tpc(Rn);
     const double two_pi = 6.283185307179586476925286766559;
     // W_L^e = exp(-2 pi i e / L), rounded once from double
     auto W = [&](unsigned long long e, unsigned long long L) {
@@ -494,23 +566,23 @@ int Fft4Plan::create(size_t n_)
         return make_float2((float)std::cos(a), (float)-std::sin(a));
     };
     std::vector<float2> h;
-    h.reserve(2400 + 82 * (size_t)Cn);
+    h.reserve(table_floats2(n_));
     offA2 = 0;  // [q * 16 + m] = W_256^(m q)
     for (unsigned q = 0; q < 16; ++q)
         for (unsigned m = 0; m < 16; ++m) h.push_back(W((unsigned long long)m * q, 256));
     offA3 = (unsigned)h.size();  // [q * 256 + j] = W_R^(j q)
     for (unsigned q = 0; q < R3; ++q)
         for (unsigned j = 0; j < 256; ++j) h.push_back(W((unsigned long long)j * q, Rn));
-    offQ = (unsigned)h.size();  // [t * C + c] = W_M^(c t)
-    for (unsigned t = 0; t < 64; ++t)
+    offQ = (unsigned)h.size();  // [t * C + c] = W_M^(c t), t < threads per column
+    for (unsigned t = 0; t < tpc; ++t)
         for (unsigned c = 0; c < Cn; ++c) h.push_back(W((unsigned long long)c * t, M));
-    offP = (unsigned)h.size();  // [w * C + c] = W_M^(64 c w)
-    for (unsigned w = 0; w < 4 * R3; ++w)
-        for (unsigned c = 0; c < Cn; ++c) h.push_back(W(64ull * c * w, M));
-    // unpack rotations (cos, sin)(pi k1 / M), k1 = -1 .. 1055, and (pi k2 / C)
+    offP = (unsigned)h.size();  // [w * C + c] = W_M^(tpc c w), w < 16
+    for (unsigned w = 0; w < 16; ++w)
+        for (unsigned c = 0; c < Cn; ++c) h.push_back(W((unsigned long long)tpc * c * w, M));
+    // unpack rotations (cos, sin)(pi k1 / M), k1 = -1 .. R + 31, and (pi k2 / C)
     const double pi = two_pi / 2;
     offRv = (unsigned)h.size();
-    for (int k1 = -1; k1 <= 1055; ++k1)
+    for (int k1 = -1; k1 <= (int)Rn + 31; ++k1)
         h.push_back(make_float2((float)std::cos(pi * k1 / (double)M),
                                 (float)std::sin(pi * k1 / (double)M)));
     offRk = (unsigned)h.size();
@@ -532,17 +604,12 @@ int Fft4Plan::create(size_t n_)
     C = Cn;
     R = Rn;
     logc = lc;
-    // (the default shared/L1 split: measured on B200, forcing the largest
-    // shared carve-out slowed the gather of pass 1 and the twiddle reads of
-    // pass 2, both served from L1)
-    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<1024, false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(1024 * kColsW * sizeof(float2))),
-                        "fft4 column pass attribute"));
-    PSX_TRY(cuda_status(cudaFuncSetAttribute(k_fft4_cols<768, false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(768 * kColsW * sizeof(float2))),
-                        "fft4 column pass attribute"));
+    switch (R) {
+    case 768: PSX_TRY(configure_cols<768>()); break;
+    case 1024: PSX_TRY(configure_cols<1024>()); break;
+    case 2048: PSX_TRY(configure_cols<2048>()); break;
+    default: PSX_TRY(configure_cols<4096>()); break;
+    }
 
     switch (logc) {
     case 8: return configure_rows<8>();
@@ -572,13 +639,12 @@ int Fft4Plan::exec_cols(const float* series, const double* ktab, int ntrials, fl
         set_error("fft4: bad arguments");
         return PSX_ERR_INVALID;
     }
-    dim3 ga(C / kColsW, (unsigned)ntrials);
-    if (R == 768)
-        k_fft4_cols<768, false><<<ga, kColsW * 64, 768 * kColsW * sizeof(float2), s>>>(
-            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
-    else
-        k_fft4_cols<1024, false><<<ga, kColsW * 64, 1024 * kColsW * sizeof(float2), s>>>(
-            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C, y, ypitch);
+    switch (R) {
+    case 768: launch_cols<768, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
+    case 1024: launch_cols<1024, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
+    case 2048: launch_cols<2048, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
+    default: launch_cols<4096, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
+    }
     return launch_status("fft4 column pass");
 }
 
@@ -589,15 +655,13 @@ int Fft4Plan::dump_gather(const float* series, const double* ktab, float* out,
         set_error("fft4 dump: bad arguments");
         return PSX_ERR_INVALID;
     }
-    dim3 ga(C / kColsW, 1);
-    if (R == 768)
-        k_fft4_cols<768, true><<<ga, kColsW * 64, 0, s>>>(
-            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C,
-            reinterpret_cast<float2*>(out), n / 2);
-    else
-        k_fft4_cols<1024, true><<<ga, kColsW * 64, 0, s>>>(
-            series, (unsigned long long)n, ktab, d_tab, offA2, offA3, offQ, offP, C,
-            reinterpret_cast<float2*>(out), n / 2);
+    float2* o = reinterpret_cast<float2*>(out);
+    switch (R) {
+    case 768: launch_cols<768, true>(*this, series, ktab, 1, o, n / 2, s); break;
+    case 1024: launch_cols<1024, true>(*this, series, ktab, 1, o, n / 2, s); break;
+    case 2048: launch_cols<2048, true>(*this, series, ktab, 1, o, n / 2, s); break;
+    default: launch_cols<4096, true>(*this, series, ktab, 1, o, n / 2, s); break;
+    }
     return launch_status("fft4 gather dump");
 }
 
@@ -634,12 +698,14 @@ int Fft4Plan::form(const float2* zt, size_t zpitch, int ntrials, float* p, size_
     }
     const unsigned nck = (R + 29) / 30;
     dim3 grid(nck * (C / 64), (unsigned)ntrials);
-    if (R == 768)
-        k_unpack_form_norm_t<768><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch,
-                                                       d_tab + offRv, d_tab + offRk, stat);
-    else
-        k_unpack_form_norm_t<1024><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch,
-                                                        d_tab + offRv, d_tab + offRk, stat);
+    const float2* rv = d_tab + offRv;
+    const float2* rk = d_tab + offRk;
+    switch (R) {
+    case 768: k_unpack_form_norm_t<768><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
+    case 1024: k_unpack_form_norm_t<1024><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
+    case 2048: k_unpack_form_norm_t<2048><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
+    default: k_unpack_form_norm_t<4096><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
+    }
     return launch_status("fft4 unpack kernel");
 }
 

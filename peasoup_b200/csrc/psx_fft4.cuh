@@ -13,16 +13,20 @@ namespace psx {
 
 struct Fft4Plan {
     size_t n = 0;      // real samples N
-    unsigned R = 1024; // rows of the four-step split: 1024, or 768 for 3 * 2^k
+    unsigned R = 1024; // rows of the four-step split: 768 for 3 * 2^k, 1024
+                       // up to N = 2^25, 2048 at 2^26, 4096 at 2^27
     unsigned C = 0;    // row length of the second pass (M / R)
     int logc = 0;
     float2* d_tab = nullptr;  // twiddle tables (offsets below, in float2)
     size_t tab_len = 0;
     unsigned offA2 = 0, offA3 = 0, offQ = 0, offP = 0, offB = 0, offRv = 0, offRk = 0;
 
-    // N = 2^19 .. 2^25 (R = 1024) or 3 * 2^17 .. 3 * 2^23 (R = 768), i.e.
-    // C = 2^8 .. 2^14.
+    // N = 2^19 .. 2^27 (R = 1024, 2048, 4096) or 3 * 2^17 .. 3 * 2^23
+    // (R = 768), i.e. C = 2^8 .. 2^14.
     static bool supported(size_t n);
+    static unsigned rows_for(size_t n);
+    // float2 entries of the twiddle tables of a plan for n
+    static size_t table_floats2(size_t n);
     int create(size_t n);
     void destroy();
     ~Fft4Plan() { destroy(); }
@@ -49,6 +53,11 @@ struct Fft4Plan {
     // p + t * ppitch.
     int form(const float2* zt, size_t zpitch, int ntrials, float* p, size_t ppitch,
              const float* stat, cudaStream_t s) const;
+
+private:
+    template <int R, bool DUMP>
+    static void launch_cols(const Fft4Plan& f, const float* series, const double* ktab,
+                            int ntrials, float2* y, size_t ypitch, cudaStream_t s);
 };
 
 }  // namespace psx

@@ -1333,7 +1333,7 @@ static int check_config(const psx_search_config* c)
     }
     if (c->fft_form == 3 && (c->mode != PSX_MODE_BATCHED || !Fft4Plan::supported(c->fft_size))) {
         set_error("search: fft_form 3 needs the batched mode and "
-                  "fft_size 2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23");
+                  "fft_size 2^19 .. 2^27 or 3 * 2^17 .. 3 * 2^23");
         return PSX_ERR_INVALID;
     }
     if (c->lanes < 0 || c->lanes > 2) {
@@ -1413,7 +1413,7 @@ size_t psx_search_footprint(const psx_search_config* c)
     // instead), plus the batch-1 plans of the two slots' prologues and the
     // plain path
     if (effective_form(c) == 3)
-        bytes += sizeof(float) * 2 * Bp * 6 + sizeof(float2) * (2400 + 82 * (N / 2048));
+        bytes += sizeof(float) * 2 * Bp * 6 + sizeof(float2) * Fft4Plan::table_floats2(N);
     else
         bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
     return bytes;

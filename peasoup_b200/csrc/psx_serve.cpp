@@ -14,6 +14,12 @@
 // retargeted onto a pooled instance (psx_search_retarget) instead of
 // allocating, and idle pooled instances are destroyed, oldest first, when a
 // new one needs their memory.
+//
+// Between running requests, the one with the least work (acceleration
+// trials times transform length, summed over its DM trials) runs at the
+// device's greatest stream priority: a short request admitted beside a long
+// one finishes close to its isolated time, and the long one loses only the
+// short one's work.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
@@ -64,6 +70,7 @@ struct Engine {
 
 struct Request {
     long long id = 0;
+    double work = 0;  // sum over DM trials of (acceleration trials + 3) * N
     psx_search_config cfg{};
     std::vector<float> bf, bw;
     std::vector<const float*> series;
@@ -94,18 +101,23 @@ struct psx_server {
     long long next_id = 1;
     bool stop = false;
     std::vector<std::thread> workers;
-    // Requests running on the device, by admission order: the oldest runs
-    // at the higher stream priority, so a request shares the GPU with a
-    // later one without being slowed by it beyond the gaps it leaves.
-    std::map<long long, psx_search*> running;
+    // Requests running on the device (by admission order) with their work:
+    // the one with the least work runs at the higher stream priority (the
+    // older one on a tie), so a short request is not held back by a long
+    // one, and the long one shares the GPU only for the short one's work.
+    struct Running {
+        psx_search* s;
+        double work;
+    };
+    std::map<long long, Running> running;
     long long admit_seq = 0;
     void reprioritise()  // under `mu`
     {
-        bool first = true;
-        for (auto& r : running) {
-            psx_search_set_priority(r.second, first ? 1 : 0);
-            first = false;
-        }
+        auto best = running.end();
+        for (auto it = running.begin(); it != running.end(); ++it)
+            if (best == running.end() || it->second.work < best->second.work) best = it;
+        for (auto it = running.begin(); it != running.end(); ++it)
+            psx_search_set_priority(it->second.s, it == best ? 1 : 0);
     }
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
@@ -206,7 +218,7 @@ void psx_server::worker()
         if (!eng.s) rc = psx_search_create(&r->cfg, &eng.s);
         if (rc == PSX_OK) {
             std::lock_guard<std::mutex> lock(mu);
-            running[my_seq] = eng.s;
+            running[my_seq] = Running{eng.s, r->work};
             reprioritise();
         }
         if (rc == PSX_OK) {
@@ -340,6 +352,18 @@ int psx_server_submit(psx_server* s, const psx_search_config* cfg, const float* 
     r->dm_idx.resize(ndm);
     for (int d = 0; d < ndm; ++d) r->dm_idx[d] = dm_idx ? dm_idx[d] : d;
     r->st.ndm = ndm;
+    // work estimate for the scheduling between running requests: every DM
+    // trial's acceleration trials plus about three trials' worth of
+    // prologue, times the transform length
+    for (int d = 0; d < ndm; ++d) {
+        size_t nacc = 0;
+        if (psx_accel_list(cfg->acc_lo, cfg->acc_hi, cfg->acc_tol, cfg->acc_pulse_width,
+                           cfg->fft_size, cfg->tsamp, cfg->cfreq_hz, cfg->ch_bw_hz, dms[d],
+                           cfg->cdm, nullptr, 0, &nacc) != PSX_OK)
+            nacc = 1;
+        r->work += (double)(nacc + 3) * (double)cfg->fft_size;
+    }
+    psx::clear_error();
     {
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->stop) {

@@ -52,11 +52,11 @@ def test_invalid_arguments_fail_loudly(psx):
     cfg.nharmonics = 6
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
     assert b"nharmonics" in psx.psx_last_error()
-    # the library's own transform: batched, 2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23
+    # the library's own transform: batched, 2^19 .. 2^27 or 3 * 2^17 .. 3 * 2^23
     # points
     for n, mode in ((1 << 16, _lib.PSX_MODE_BATCHED), (3 << 16, _lib.PSX_MODE_BATCHED),
                     (3 << 24, _lib.PSX_MODE_BATCHED),
-                    (1 << 26, _lib.PSX_MODE_BATCHED), (1 << 20, _lib.PSX_MODE_PLAIN)):
+                    (1 << 28, _lib.PSX_MODE_BATCHED), (1 << 20, _lib.PSX_MODE_PLAIN)):
         psx.psx_search_config_defaults(C.byref(cfg), n, 64e-6)
         cfg.mode, cfg.fft_form = mode, 3
         assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
@@ -140,11 +140,11 @@ def test_binding_constants_match_header():
 
 def test_two_pass_transform_lengths(psx):
     """Host rule of the two-pass transform (fft_form 3): batched mode,
-    2^19 .. 2^25 or 3 * 2^17 .. 3 * 2^23 points; a configuration outside it
+    2^19 .. 2^27 or 3 * 2^17 .. 3 * 2^23 points; a configuration outside it
     has no footprint (it is rejected before any device work)."""
     cfg = _lib.SearchConfig()
-    ok = [1 << 19, 1 << 23, 1 << 25, 3 << 17, 3 << 20, 3 << 23]
-    bad = [1 << 18, 1 << 26, 3 << 16, 3 << 24, 5 << 20, 1000]
+    ok = [1 << 19, 1 << 23, 1 << 25, 1 << 26, 1 << 27, 3 << 17, 3 << 20, 3 << 23]
+    bad = [1 << 18, 1 << 28, 3 << 16, 3 << 24, 5 << 20, 1000]
     for n in ok + bad:
         psx.psx_search_config_defaults(C.byref(cfg), n, 64e-6)
         cfg.mode, cfg.fft_form = _lib.PSX_MODE_BATCHED, 3

@@ -5,7 +5,8 @@ interleaved pairs, then the unpack + interbin + normalise kernel):
   * the normalised interbinned spectrum of tapped trials against FP64
     (numpy's real transform of the same resampled series) within 1e-5
     relative, |a - b| <= 1e-5 (|b| + RMS), at every row length the two
-    passes support and for both row counts (1024, and 768 for 3 * 2^k);
+    passes support and for every row count (768 for 3 * 2^k, 1024, and
+    2048 / 4096 for the long segments of 2^26 / 2^27 points);
   * candidate lists identical to cuFFT's complex transform (fft_form 1) and
     to the reference's real transform (plain mode), S/N within 1e-5.
 """
@@ -62,6 +63,52 @@ def test_spectrum_vs_fp64(S, oracle, n):
         err = err_vs_mag_or_rms(ps, want)
         assert err < 1e-5, (logn, t, err)
     s.close()
+
+
+@pytest.mark.parametrize("n,acc", [(1 << 26, 0.05), (1 << 27, 0.02)])
+def test_long_segment_vs_fp64_and_plain(S, oracle, n, acc):
+    """Long segments (2^26 and 2^27 points, tsamp 64 us: 1.2 and 2.4 h) on
+    the two-pass transform with 2048- and 4096-row columns: the normalised
+    spectrum of the first and last trial against FP64 (within 1e-5, as at
+    the shorter lengths), and the candidates against the plain path (the
+    reference's cuFFT real transform, include/transforms/ffter.hpp:54-80),
+    S/N within 1e-5.  A narrow acceleration range keeps the trial count
+    small (the step shrinks as 1/tobs^2)."""
+    import torch
+    search, synth = S
+    ts = 64e-6
+    g = torch.Generator(device="cuda").manual_seed(n.bit_length())
+    x = torch.randn(n, device="cuda", generator=g)
+    t = torch.arange(n, device="cuda", dtype=torch.float64)
+    k = 0.01 * ts / (2.0 * 299792458.0)
+    ph = torch.frac((t - k * t * (t - n)) * ts / 9.7e-3)
+    x += (0.05 * torch.exp(-0.5 * ((ph - 0.5) / 0.02) ** 2)).float()
+    del t, ph
+    kw = dict(acc_lo=-acc, acc_hi=acc, nharmonics=5, min_snr=7.0)
+    s = search.AccelSearch(_params(S, n, ts, batch=4, **kw))
+    own = s.search(x, 0.0, 0, per_dm=False)[0]
+    assert s.info()["fft_form"] == 3
+    from peasoup_b200.transforms import AccelerationPlan
+    accs = AccelerationPlan(-acc, acc, 1.10, 64e-6, n, ts, synth.CFREQ_HZ,
+                            synth.CH_BW_HZ).generate_accel_list(0.0, 0.0)
+    assert 2 <= len(accs) <= 16
+    for tr_i in sorted({0, len(accs) - 1}):
+        tim, tr, ps, norm2 = s.debug_tap(tr_i)
+        idx = oracle.resampleII_index(n, float(accs[tr_i]), ts)
+        assert np.array_equal(tr, tim[idx.astype(np.int64)])
+        err = err_vs_mag_or_rms(ps, _fp64_spectrum(tim, idx, norm2))
+        del tim, tr, idx
+        assert err < 1e-5, (n, tr_i, err)
+    s.close()
+    p = search.AccelSearch(_params(S, n, ts, mode="plain", **kw))
+    plain = p.search(x, 0.0, 0, per_dm=False)[0]
+    p.close()
+    assert len(own) > 3
+    nm, ua, ub, worst = match_candidates(own, plain, 7.0, margin=1e-4)
+    assert not ua and not ub and worst < 1e-5, (ua[:3], ub[:3], worst)
+    f0 = 1 / 9.7e-3
+    r = own["freq"] / f0
+    assert np.any(np.abs(r - np.round(r)) < 1e-4)
 
 
 @pytest.mark.parametrize("n", [1 << 20, 1 << 22, 3 << 20])

@@ -158,7 +158,9 @@ def test_survey_production_vs_oracle(S, survey, production, oracle):
         assert set(np.unique(want["acc"])) <= {np.float32(0.0), np.float32(a)}
         nm, flips, worst = flip_report(cands[sel], want, 9.0, FLIP_MARGIN_ORACLE,
                                        f"survey 2^23 DM {d} acc 0/{a:.3f} vs oracle")
-        assert nm > 0 and worst < SNR_RTOL
+        assert worst < SNR_RTOL
+        # the pulsars' DM trials have candidates; the noise-only one may have none
+        assert nm > 0 if pos < 2 else nm == len(want) == int(sel.sum())
 
 
 def test_survey_autotuned_equals_production(S, survey, production):

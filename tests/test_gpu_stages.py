@@ -162,8 +162,10 @@ def _red_amp(rng, nb):
             (1 + 50.0 / (1 + np.arange(nb) / 40.0))).astype(np.float32)
 
 
-@pytest.mark.parametrize("nb", [(1 << 16) + 1, (3 << 15) + 1, (1 << 20) + 1])
+@pytest.mark.parametrize("nb", [(1 << 16) + 1, (3 << 15) + 1, (1 << 20) + 1, (1 << 26) + 1])
 def test_running_median_vs_oracle(T, oracle, nb):
+    """The 5/25/125-bin running median against FP64; 2^26 + 1 bins is the
+    spectrum of a 2^27-point segment (256 MB, twice the L2)."""
     rng = np.random.default_rng(nb)
     amp = _red_amp(rng, nb)
     bw = float(np.float32(1.0 / np.float32(np.float32(2 * (nb - 1)) * TS)))
