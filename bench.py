@@ -454,6 +454,7 @@ def run_served(nreq, rank, log_prefix):
     isolated_tps = trials / (sum(iso) / 1e3)
     ratio = [a / b for a, b in zip(lat_adm, iso)]
     failed = sum(1 for s in mixed + alone if s["status"] != 0)
+    worst = sorted(range(len(reqs)), key=lambda i: -ratio[i])[:4]
     return {
         "requests": len(reqs), "failed": failed, "arrival_rate_per_s": 4.0,
         "trials": int(trials), "trials_per_s": served_tps,
@@ -464,6 +465,11 @@ def run_served(nreq, rank, log_prefix):
         "isolated_ms": {"p50": _pct(iso, 50), "p99": _pct(iso, 99)},
         "p99_admitted_over_p99_isolated": _pct(lat_adm, 99) / _pct(iso, 99),
         "per_request_ratio_p99": _pct(ratio, 99),
+        "per_request_ratio_p50": _pct(ratio, 50),
+        "worst_ratio_requests": [
+            {"fft_size": reqs[i].fft_size, "ndm": reqs[i].ndm, "trials": mixed[i]["ntrials"],
+             "admitted_ms": lat_adm[i], "isolated_ms": iso[i], "ratio": ratio[i]}
+            for i in worst],
         "throughput_over_isolated_back_to_back": served_tps / isolated_tps,
         "max_active": SERVED_SLOTS, "hbm_budget_gb": SERVED_BUDGET / 1e9,
         "engines_reused": int(sum(s["engine_reused"] for s in mixed)),

@@ -141,11 +141,14 @@ __device__ __forceinline__ void dft3(float2& a, float2& b, float2& c)
 // Column shape of pass 1 for column length R: W columns per CTA, J = R/16
 // radix-16 butterflies per column in the first two stages, TPC threads per
 // column (J, at least 64), a last stage of radix R3 = R/256 with U = 256/TPC
-// butterflies per thread.  Every shape has 512 threads, 16 elements (12 for
-// R = 768) per thread and R * W * 8 <= 64 KB of shared memory.
+// butterflies per thread; 16 elements (12 for R = 768) per thread.  W is at
+// least 4 so that every row a CTA reads or writes is one whole 32-byte
+// sector (the series of a long segment does not stay in L2): 512 threads
+// and 64 KB of shared memory for R <= 2048, 1024 threads and 128 KB (one
+// CTA per SM) for R = 4096.
 template <int R>
 struct ColShape {
-    static constexpr int W = R == 4096 ? 2 : R == 2048 ? 4 : 8;
+    static constexpr int W = R >= 2048 ? 4 : 8;
     static constexpr int J = R / 16;
     static constexpr int TPC = J < 64 ? 64 : J;
     static constexpr int R3 = R / 256;
@@ -170,14 +173,15 @@ __device__ __forceinline__ unsigned swz_a(unsigned e)
 // DUMP: write the gathered pairs z[e C + c] (the resampled series as it is
 // read, interleaved) to y instead of transforming them (the debug tap).
 template <int R, bool DUMP>
-__global__ void __launch_bounds__(ColShape<R>::THREADS, 2)
+__global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THREADS)
     k_fft4_cols(const float* __restrict__ x, unsigned long long n, const double* __restrict__ ktab,
                 const float2* __restrict__ tab, unsigned offA2, unsigned offA3, unsigned offQ,
                 unsigned offP, unsigned C, float2* __restrict__ y, size_t ypitch)
 {
     using S = ColShape<R>;
     static_assert(R == 768 || R == 1024 || R == 2048 || R == 4096, "column length");
-    static_assert(S::THREADS == 512 && S::U * S::R3 <= 16, "column shape");
+    static_assert((S::THREADS == 512 || S::THREADS == 1024) && S::U * S::R3 <= 16,
+                  "column shape");
     constexpr int W = S::W, J = S::J, TPC = S::TPC, R3 = S::R3, U = S::U;
     extern __shared__ float2 sm_a[];
     const unsigned col = threadIdx.x % W, t = threadIdx.x / W;  // t in [0, TPC)
