@@ -602,9 +602,13 @@ def run_config3(args):
     eng.set_stream(stream.cuda_stream)
     rows = [block[i] for i in range(ndm)]
     _timed_block(eng, rows[:16], dms[:16], stream, 16)          # warm-up
+    eng.profile(reset=True)
     with ClockSampler(0) as clk:
         tb, outs_b = _timed_block(eng, rows, dms, stream, 64)
     clocks = clk.summary()
+    hostp = eng.profile(reset=True)   # host times of the timed pass (no events)
+    host_us = {k: 1e3 * hostp[k] / ndm for k in ("host_enqueue_ms", "host_wait_ms",
+                                                  "host_collect_ms")}
     # per-stage device times (CUDA events around every launch group, no
     # graph capture) on the first 128 DM trials, for the stage roofline
     eng.set_profile(True)
@@ -651,6 +655,7 @@ def run_config3(args):
         "candidates_compared": len(kp), "snr_worst_rel": worst,
         "hbm_roofline_frac": (ndm * 24.0 * n + tot_b * 12.0 * n) / tb / (peaks()[0] * 1e9),
         "roofline": roofline,
+        "host_us_per_dm": host_us,
         "clocks": clocks,
         "workload": "2048 DM x 2^22, tsamp 64us, white N(0,1) + P=5.7ms 5% duty 0.3 sigma "
                     "pulsar at +12 m/s^2 in every row, acc -50..50 (15 trials at DM 0), "
@@ -798,6 +803,7 @@ def run_psx(args, ws, rank, local):
     ntr = sum(trials_of(plan, st) for st in timed)
     launches = 0
     ncand = 0
+    eng.profile(reset=True)
     with ClockSampler(local) as clk:
         barrier(ws)
         torch.cuda.synchronize()
@@ -812,6 +818,10 @@ def run_psx(args, ws, rank, local):
         torch.cuda.synchronize()
         barrier(ws)
     dt = e0.elapsed_time(e1) / 1e3
+    hostp = eng.profile(reset=True)   # host times of the timed steps (no events)
+    ndm_timed = max(1, sum(len(st) for st in timed))
+    host_us = {k: 1e3 * hostp[k] / ndm_timed for k in ("host_enqueue_ms", "host_wait_ms",
+                                                        "host_collect_ms")}
     batch_used = eng.info()["batch"]
     shape_used = eng.info()["harm_shape"]
     form_used = eng.info()["fft_form"]
@@ -942,6 +952,7 @@ def run_psx(args, ws, rank, local):
             "hbm_roofline_frac": hbm_frac,
             "plain": plain, "e2e": e2e, "served": served, "roofline": roofline,
             "cpu_baseline": cpu,
+            "host_us_per_dm": host_us,
             "clocks": clocks, "gpu_launches": launches, "candidates": ncand,
             "trials": int(tot_trials),
         }

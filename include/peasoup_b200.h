@@ -531,6 +531,12 @@ typedef struct {
     long long dms;        /* DM trials timed */
     long long event_errors; /* event pairs that could not be timed */
     int last_event_error;   /* cudaError_t of the last such pair */
+    /* host time of the calling thread (wall clock, recorded always):
+       queuing each DM trial's work, blocked waiting for a DM trial's device
+       work to finish, and reading back + distilling its records */
+    double host_enqueue_ms;
+    double host_wait_ms;
+    double host_collect_ms;
 } psx_search_profile;
 
 /* Scheduling hint for a server running several instances on one device

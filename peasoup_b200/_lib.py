@@ -77,7 +77,9 @@ class SearchProfile(C.Structure):
     _fields_ = [("prologue_ms", C.c_double), ("resample_ms", C.c_double),
                 ("fft_ms", C.c_double), ("form_ms", C.c_double), ("harm_ms", C.c_double),
                 ("groups", C.c_longlong), ("trials", C.c_longlong), ("dms", C.c_longlong),
-                ("event_errors", C.c_longlong), ("last_event_error", C.c_int)]
+                ("event_errors", C.c_longlong), ("last_event_error", C.c_int),
+                ("host_enqueue_ms", C.c_double), ("host_wait_ms", C.c_double),
+                ("host_collect_ms", C.c_double)]
 
 
 class CandidateScore(C.Structure):

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
@@ -430,6 +431,11 @@ using namespace psx;
 namespace {
 
 size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+double ms_since(std::chrono::steady_clock::time_point t)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
 
 // Untuned trials per launch group: about 2^28 samples (1 GB of resampled
 // series) per group, 1..32; cuFFT's batched transforms get faster with the
@@ -1029,6 +1035,7 @@ int psx_search::run_trials(Slot& s, int nacc)
 int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
                         int dm_idx)
 {
+    const auto t_host = std::chrono::steady_clock::now();
     const psx_search_config& c = cfg;
     PSX_TRY(apply_priority());
     s.series = series;
@@ -1052,6 +1059,7 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
     PSX_TRY(run_trials(s, nacc));
     PSX_CUDA(cudaMemcpyAsync(s.h_count, s.d_count, sizeof(unsigned) * 4, cudaMemcpyDeviceToHost, st));
     PSX_CUDA(cudaEventRecord(s.done, st));
+    prof.host_enqueue_ms += ms_since(t_host);
     return PSX_OK;
 }
 
@@ -1221,7 +1229,9 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
                        std::vector<int>& nassoc, std::vector<int>& trial_of)
 {
     for (int attempt = 0; attempt < 3; ++attempt) {
+        const auto t_wait = std::chrono::steady_clock::now();
         PSX_CUDA(cudaEventSynchronize(s.done));
+        prof.host_wait_ms += ms_since(t_wait);
         const size_t hits = s.h_count[0];
         if (s.h_count[1] != 0) {
             set_error("search: harmonic-sum staging did not complete (status 0x%x)", s.h_count[1]);
@@ -1241,6 +1251,7 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
         }
         PSX_TRY(enqueue(s, s.series, s.nsamps, s.on_device, s.dm, s.dm_idx));
     }
+    const auto t_collect = std::chrono::steady_clock::now();
     const size_t nrec = s.h_count[0];
     info.baseline_passes = s.host_baseline ? -1 : (int)s.h_count[3];
     s.host_baseline = false;
@@ -1257,6 +1268,7 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
     info.fft_launches += s.ffts;
     info.above_threshold += (long long)nrec;
     collect(s, nrec, output, out, nassoc, trial_of);
+    prof.host_collect_ms += ms_since(t_collect);
     return PSX_OK;
 }
 
