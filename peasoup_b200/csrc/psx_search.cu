@@ -28,6 +28,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <functional>
 #include <map>
 #include <memory>
@@ -660,9 +661,16 @@ struct psx_search {
     int run_trials(Slot& s, int nacc);
     int enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
                 int dm_idx);
-    int finish(Slot& s, int output, std::vector<psx_candidate>& out, std::vector<int>& nassoc,
-               std::vector<int>& trial_of);
-    void collect(Slot& s, size_t nrec, int output, std::vector<psx_candidate>& out,
+    // The records of one DM trial, copied out of its slot so that the slot
+    // can take the next DM trial while they are distilled.
+    struct DmRecords {
+        std::vector<int4> recs;
+        std::vector<float> accs;
+        float dm = 0.f;
+        int dm_idx = 0;
+    };
+    int finish(Slot& s, DmRecords& job);
+    void collect(const DmRecords& job, int output, std::vector<psx_candidate>& out,
                  std::vector<int>& nassoc, std::vector<int>& trial_of);
     void read_profile(Slot& s);
 };
@@ -1097,15 +1105,16 @@ void psx_search::read_profile(Slot& s)
 // bucket by bin (the order the reference's copy_if leaves them in),
 // cluster (peakfinder.hpp:72-94), form candidate frequencies, distil per
 // trial (pipeline_multi.cu:283-289) and optionally per DM (:294).
-void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candidate>& out,
+void psx_search::collect(const DmRecords& job, int output, std::vector<psx_candidate>& out,
                          std::vector<int>& nassoc, std::vector<int>& trial_of)
 {
-    const int nacc = (int)s.accs.size();
+    const int nacc = (int)job.accs.size();
+    const size_t nrec = job.recs.size();
     const int nf = F + 1;
     const size_t nkeys = (size_t)nacc * nf;
     std::vector<unsigned> off(nkeys + 1, 0);
     for (size_t r = 0; r < nrec; ++r) {
-        const int4 q = s.h_rec[r];
+        const int4 q = job.recs[r];
         if (q.x >= 0 && q.x < nacc && q.y >= 0 && q.y < nf) ++off[(size_t)q.x * nf + q.y + 1];
     }
     for (size_t k = 0; k < nkeys; ++k) off[k + 1] += off[k];
@@ -1113,7 +1122,7 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
     {
         std::vector<unsigned> pos(off.begin(), off.end() - 1);
         for (size_t r = 0; r < nrec; ++r) {
-            const int4 q = s.h_rec[r];
+            const int4 q = job.recs[r];
             if (q.x < 0 || q.x >= nacc || q.y < 0 || q.y >= nf) continue;
             float v;
             std::memcpy(&v, &q.w, sizeof v);
@@ -1147,7 +1156,7 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
                 const size_t np = unique_peaks(idx.data(), snr.data(), n, cfg.min_gap, pidx.data(),
                                                psnr.data());
                 for (size_t i = 0; i < np; ++i)
-                    tc.push_back(psx_candidate{s.dm, s.dm_idx, s.accs[t], h, psnr[i],
+                    tc.push_back(psx_candidate{job.dm, job.dm_idx, job.accs[t], h, psnr[i],
                                                (float)pidx[i] * factor[h]});
             }
             if (tc.empty()) continue;
@@ -1202,8 +1211,8 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
         fs.resize(nn);
         trial_of.assign(nn, -1);
         for (size_t k = 0; k < nn; ++k) {
-            auto it = std::lower_bound(s.accs.begin(), s.accs.end(), f[k].acc);
-            if (it != s.accs.end() && *it == f[k].acc) trial_of[k] = (int)(it - s.accs.begin());
+            auto it = std::lower_bound(job.accs.begin(), job.accs.end(), f[k].acc);
+            if (it != job.accs.end() && *it == f[k].acc) trial_of[k] = (int)(it - job.accs.begin());
         }
         out.swap(f);
         nassoc.swap(fs);
@@ -1216,8 +1225,8 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
         nassoc.resize(keep);
         trial_of.assign(keep, -1);
         for (size_t k = 0; k < keep; ++k) {
-            auto it = std::lower_bound(s.accs.begin(), s.accs.end(), c[k].acc);
-            if (it != s.accs.end() && *it == c[k].acc) trial_of[k] = (int)(it - s.accs.begin());
+            auto it = std::lower_bound(job.accs.begin(), job.accs.end(), c[k].acc);
+            if (it != job.accs.end() && *it == c[k].acc) trial_of[k] = (int)(it - job.accs.begin());
         }
         out.swap(c);
     } else {
@@ -1225,8 +1234,7 @@ void psx_search::collect(Slot& s, size_t nrec, int output, std::vector<psx_candi
     }
 }
 
-int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
-                       std::vector<int>& nassoc, std::vector<int>& trial_of)
+int psx_search::finish(Slot& s, DmRecords& job)
 {
     for (int attempt = 0; attempt < 3; ++attempt) {
         const auto t_wait = std::chrono::steady_clock::now();
@@ -1251,7 +1259,6 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
         }
         PSX_TRY(enqueue(s, s.series, s.nsamps, s.on_device, s.dm, s.dm_idx));
     }
-    const auto t_collect = std::chrono::steady_clock::now();
     const size_t nrec = s.h_count[0];
     info.baseline_passes = s.host_baseline ? -1 : (int)s.h_count[3];
     s.host_baseline = false;
@@ -1267,8 +1274,10 @@ int psx_search::finish(Slot& s, int output, std::vector<psx_candidate>& out,
     info.kernel_launches += s.launches;
     info.fft_launches += s.ffts;
     info.above_threshold += (long long)nrec;
-    collect(s, nrec, output, out, nassoc, trial_of);
-    prof.host_collect_ms += ms_since(t_collect);
+    job.recs.assign(s.h_rec, s.h_rec + nrec);
+    job.accs = s.accs;
+    job.dm = s.dm;
+    job.dm_idx = s.dm_idx;
     return PSX_OK;
 }
 
@@ -1792,10 +1801,45 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
     s->info.harm_shape = s->harm_shape;
     s->info.fft_form = effective_form(&s->cfg);
     s->info.graph = s->batched() && s->cfg.use_graph && !s->profile ? 1 : 0;
-    std::vector<psx_candidate> all, out;
-    std::vector<int> all_na, all_tr, all_dm, na, tr;
     // prologues wait for the caller's work queued on the compute stream so far
     PSX_CUDA(cudaEventRecord(s->call_start, s->st));
+    std::vector<psx_candidate> all;
+    std::vector<int> all_na, all_tr, all_dm;
+    // DM d's records are distilled (collect) on a collector thread while
+    // this thread queues DM d+2: with few acceleration trials per DM trial
+    // the host's distillation would otherwise leave the device idle.  Jobs
+    // are taken in DM order, so the output order is that of the loop.
+    std::mutex jmu;
+    std::condition_variable jcv;
+    std::deque<std::pair<int, psx_search::DmRecords>> jobs;
+    bool jobs_closed = false;
+    auto take = [&](int d, psx_search::DmRecords& job) {
+        std::vector<psx_candidate> out;
+        std::vector<int> na, tr;
+        const auto t0 = std::chrono::steady_clock::now();
+        s->collect(job, output, out, na, tr);
+        s->prof.host_collect_ms += ms_since(t0);
+        all.insert(all.end(), out.begin(), out.end());
+        all_na.insert(all_na.end(), na.begin(), na.end());
+        all_tr.insert(all_tr.end(), tr.begin(), tr.end());
+        all_dm.insert(all_dm.end(), out.size(), d);
+    };
+    std::thread collector;
+    if (ndm > 1)
+        collector = std::thread([&] {
+            for (;;) {
+                std::pair<int, psx_search::DmRecords> j;
+                {
+                    std::unique_lock<std::mutex> lock(jmu);
+                    jcv.wait(lock, [&] { return jobs_closed || !jobs.empty(); });
+                    if (jobs.empty()) return;
+                    j = std::move(jobs.front());
+                    jobs.pop_front();
+                }
+                take(j.first, j.second);
+            }
+        });
+    // (no early return from here until the collector is joined)
     int rc = s->enqueue(s->slot[0], series[0], nsamps, series_on_device != 0, dms[0],
                         dm_idx ? dm_idx[0] : 0);
     for (int d = 0; d < ndm && rc == PSX_OK; ++d) {
@@ -1804,12 +1848,25 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
                             dms[d + 1], dm_idx ? dm_idx[d + 1] : d + 1);
         if (rc != PSX_OK) break;
         s->last_slot = d & 1;
-        rc = s->finish(s->slot[d & 1], output, out, na, tr);
+        psx_search::DmRecords job;
+        rc = s->finish(s->slot[d & 1], job);
         if (rc != PSX_OK) break;
-        all.insert(all.end(), out.begin(), out.end());
-        all_na.insert(all_na.end(), na.begin(), na.end());
-        all_tr.insert(all_tr.end(), tr.begin(), tr.end());
-        all_dm.insert(all_dm.end(), out.size(), d);
+        if (ndm == 1) {
+            take(d, job);
+        } else {
+            std::lock_guard<std::mutex> lock(jmu);
+            jobs.emplace_back(d, std::move(job));
+            jcv.notify_one();
+        }
+    }
+    if (collector.joinable()) {
+        {
+            std::lock_guard<std::mutex> lock(jmu);
+            jobs_closed = true;
+            if (rc != PSX_OK) jobs.clear();
+        }
+        jcv.notify_one();
+        collector.join();
     }
     if (rc != PSX_OK) {
         cudaStreamSynchronize(s->st);
