@@ -386,7 +386,7 @@ def _served_series(r, seed):
     return x
 
 
-def run_served(nreq, rank, log_prefix):
+def run_served(nreq, rank, log_prefix, policy="least_work"):
     """The served workload (Poisson arrivals, uneven requests) through the
     C++ server, then every request alone on a one-slot server: latency
     from arrival and from admission, throughput, and the ratios to the
@@ -404,7 +404,7 @@ def run_served(nreq, rank, log_prefix):
     torch.cuda.synchronize()
 
     def one_pass(max_active, paced):
-        srv = serve.Server(SERVED_BUDGET, max_active=max_active)
+        srv = serve.Server(SERVED_BUDGET, max_active=max_active, policy=policy)
         res = [None] * len(reqs)
         tickets = [None] * len(reqs)
         ready = [th.Event() for _ in reqs]
@@ -471,7 +471,7 @@ def run_served(nreq, rank, log_prefix):
              "admitted_ms": lat_adm[i], "isolated_ms": iso[i], "ratio": ratio[i]}
             for i in worst],
         "throughput_over_isolated_back_to_back": served_tps / isolated_tps,
-        "max_active": SERVED_SLOTS, "hbm_budget_gb": SERVED_BUDGET / 1e9,
+        "max_active": SERVED_SLOTS, "policy": policy, "hbm_budget_gb": SERVED_BUDGET / 1e9,
         "engines_reused": int(sum(s["engine_reused"] for s in mixed)),
         "series": "made on the GPU before the passes" if pre else "made at each arrival",
         "workload": (f"{len(reqs)} requests, Poisson 4/s (seed 1), fft_size in 2^20..2^25 "
@@ -931,7 +931,7 @@ def run_psx(args, ws, rank, local):
         del block
         torch.cuda.empty_cache()
         t0 = time.perf_counter()
-        served = run_served(args.served, rank, "served")
+        served = run_served(args.served, rank, "served", args.served_policy)
         log(f"[rank {rank}] served workload in {time.perf_counter() - t0:.1f}s")
     if rank == 0:
         line = {
@@ -1159,6 +1159,8 @@ def main():
                     help="launch the trial schedules directly instead of as CUDA graphs")
     ap.add_argument("--served", type=int, default=SERVED_REQUESTS,
                     help="requests of the served workload (0: skip)")
+    ap.add_argument("--served-policy", default="least_work", choices=["least_work", "even"],
+                    help="scheduling between running requests of the served workload")
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
                     help="2: the headline survey workload; 3 and 5: the other throughput "
                          "configurations (one JSON line each)")

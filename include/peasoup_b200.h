@@ -584,7 +584,14 @@ typedef struct {
     int max_active;     /* requests searched at once (1..64), one host thread
                            and one instance each; their GPU work overlaps */
     int max_queue;      /* pending requests before submit refuses */
+    int policy;         /* scheduling between running requests:
+                           PSX_SERVE_LEAST_WORK (0) -- the one with the least
+                           work at the device's greatest stream priority;
+                           PSX_SERVE_EVEN (1) -- no priority hint: running
+                           requests share the device evenly */
 } psx_server_config;
+
+enum { PSX_SERVE_LEAST_WORK = 0, PSX_SERVE_EVEN = 1 };
 
 typedef struct {
     double t_submit;    /* seconds on the server clock (psx_server_clock) */
@@ -610,9 +617,11 @@ double psx_server_clock(psx_server* srv);
    request completes; the config (birdies included) is copied.  Requests
    are admitted first in, first out, when a worker is free and the new
    instance they need fits the budget (a pooled instance with the same
-   shape is reused).  Of the requests running at once, the one with the
-   least work (acceleration trials times transform length over its DM
-   trials) runs at the higher stream priority (psx_search_set_priority).
+   shape is reused).  With policy PSX_SERVE_LEAST_WORK, of the requests
+   running at once the one with the least work (acceleration trials times
+   transform length over its DM trials) runs at the higher stream priority
+   (psx_search_set_priority); with PSX_SERVE_EVEN they share the device
+   without a hint.
    PSX_ERR_BUSY: queue full; PSX_ERR_ALLOC: larger than the whole budget. */
 int psx_server_submit(psx_server* srv, const psx_search_config* cfg,
                       const float* const* series, size_t nsamps,

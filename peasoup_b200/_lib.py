@@ -90,7 +90,7 @@ class CandidateScore(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_active", C.c_int),
-                ("max_queue", C.c_int)]
+                ("max_queue", C.c_int), ("policy", C.c_int)]
 
 
 class RequestStats(C.Structure):

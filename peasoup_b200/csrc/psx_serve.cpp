@@ -113,6 +113,7 @@ struct psx_server {
     long long admit_seq = 0;
     void reprioritise()  // under `mu`
     {
+        if (cfg.policy == PSX_SERVE_EVEN) return;  // every instance at the normal level
         auto best = running.end();
         for (auto it = running.begin(); it != running.end(); ++it)
             if (best == running.end() || it->second.work < best->second.work) best = it;
@@ -268,9 +269,10 @@ int psx_server_create(const psx_server_config* cfg, psx_server** out)
 {
     psx::clear_error();
     if (!cfg || !out || cfg->max_active < 1 || cfg->max_active > 64 || cfg->max_queue < 1 ||
-        cfg->hbm_budget == 0) {
+        cfg->hbm_budget == 0 ||
+        (cfg->policy != PSX_SERVE_LEAST_WORK && cfg->policy != PSX_SERVE_EVEN)) {
         psx::set_error("server_create: bad configuration (max_active 1..64, max_queue >= 1, "
-                       "hbm_budget > 0)");
+                       "hbm_budget > 0, policy 0 or 1)");
         return PSX_ERR_INVALID;
     }
     *out = nullptr;

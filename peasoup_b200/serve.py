@@ -26,12 +26,17 @@ class Server:
     """One served loop on the current CUDA device."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, max_queue: int = 4096,
-                 device: Optional[int] = None):
+                 device: Optional[int] = None, policy: str = "least_work"):
+        """policy: "least_work" (the running request with the least work at
+        the device's greatest stream priority) or "even" (no hint)."""
         if device is None:
             import torch
             device = torch.cuda.current_device()
+        if policy not in ("least_work", "even"):
+            raise ValueError("policy: least_work or even")
         cfg = ServerConfig(device=int(device), hbm_budget=int(hbm_budget_bytes),
-                           max_active=int(max_active), max_queue=int(max_queue))
+                           max_active=int(max_active), max_queue=int(max_queue),
+                           policy=0 if policy == "least_work" else 1)
         self._h = C.c_void_p()
         check(load().psx_server_create(C.byref(cfg), C.byref(self._h)), "server_create")
         self._keep = {}

@@ -46,11 +46,12 @@ def _alone(M, p, xs, dms):
     return c, na, dm
 
 
-def test_mixed_equals_alone(M):
+@pytest.mark.parametrize("policy", ["least_work", "even"])
+def test_mixed_equals_alone(M, policy):
     search, serve, synth = M
     import torch
     reqs = _requests(M)
-    srv = serve.Server(40 << 30, max_active=3)
+    srv = serve.Server(40 << 30, max_active=3, policy=policy)
     # half of the requests from device memory, half from host memory
     tickets = []
     for i, (p, xs, dms) in enumerate(reqs):
