@@ -573,7 +573,7 @@ def _timed_block(eng, rows, dms, stream, chunk):
     return e0.elapsed_time(e1) / 1e3, outs
 
 
-def run_config3(args):
+def run_config3(args, emit=True):
     """2048 DM trials x 2^22 samples of the small benchmark's statistics,
     acc +-50, 4 folds, S/N 7: batched (autotuned) over every DM trial, plain
     on a sample, and the candidate sets of the sampled DM trials compared."""
@@ -644,7 +644,7 @@ def run_config3(args):
     vb, vp = tot_b / tb, tot_p / tp
     eng.close()
     engp.close()
-    print(json.dumps({
+    line = {
         "metric": "DM x accel trials/s, config 3 (2048 DM x 2^22)", "config_id": 3,
         "value": vb, "unit": "trials/s", "higher_is_better": True,
         "batched": {"value": vb, "seconds": tb, "dm_trials": ndm, "trials": tot_b,
@@ -660,11 +660,16 @@ def run_config3(args):
         "workload": "2048 DM x 2^22, tsamp 64us, white N(0,1) + P=5.7ms 5% duty 0.3 sigma "
                     "pulsar at +12 m/s^2 in every row, acc -50..50 (15 trials at DM 0), "
                     "4 folds, S/N 7, no zap list; series resident on the GPU",
-    }), flush=True)
-    return 0
+    }
+    del block, rows
+    torch.cuda.empty_cache()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
-def run_config5(args):
+
+def run_config5(args, emit=True):
     """2^27 samples, 64 DM trials, acc +-500 (123,653 trials at DM 0), 5
     folds: a fixed subset timed and extrapolated.  Per-trial and per-DM
     costs come from two subsets of different trial counts on the same DM
@@ -733,7 +738,7 @@ def run_config5(args):
     eng.close()
     peak, peak_kind = peaks()
     roofline = stage_roofline(prof, n, info["fft_form"], info["harm_shape"], peak, peak_kind)
-    print(json.dumps({
+    line = {
         "metric": "DM x accel trials/s, config 5 (2^27, 64 DM, acc +-500), extrapolated",
         "config_id": 5, "value": res["batched"]["value"], "unit": "trials/s",
         "higher_is_better": True, "batched": res["batched"], "plain": res["plain"],
@@ -751,8 +756,13 @@ def run_config5(args):
                     f"timed on {nuse} DM trials with narrowed acceleration ranges "
                     f"(batched +-0.5 and +-2, plain +-0.25 and +-1 m/s^2) and extrapolated "
                     f"to the full {sum(full)} trials",
-    }), flush=True)
-    return 0
+    }
+    del block, rows
+    torch.cuda.empty_cache()
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
 
 # ----------------------------------------------------------------- main arm
 def run_psx(args, ws, rank, local):
@@ -927,12 +937,22 @@ def run_psx(args, ws, rank, local):
                           f"{cpu_s:.2f}s; the FP64 oracle is the checker only")}
     eng.close()
     served = None
+    block = None   # the survey block is not needed any more
+    torch.cuda.empty_cache()
     if rank == 0 and ws == 1 and args.served > 0:
-        del block
-        torch.cuda.empty_cache()
         t0 = time.perf_counter()
         served = run_served(args.served, rank, "served", args.served_policy)
         log(f"[rank {rank}] served workload in {time.perf_counter() - t0:.1f}s")
+    other_configs = None
+    if rank == 0 and ws == 1 and not args.no_configs:
+        # the batched form at scale (config 3) and the long segment (config
+        # 5), each with its plain comparison and stage roofline
+        import argparse as _ap
+        t0 = time.perf_counter()
+        sub = _ap.Namespace(**vars(args))
+        sub.ndm = 0
+        other_configs = {"3": run_config3(sub, emit=False), "5": run_config5(sub, emit=False)}
+        log(f"[rank {rank}] configs 3 and 5 in {time.perf_counter() - t0:.1f}s")
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "trials/s", "n_gpus": ws,
@@ -951,6 +971,7 @@ def run_psx(args, ws, rank, local):
                        "l2": "inputs larger than L2 (8 x 32 MB series per step)"},
             "hbm_roofline_frac": hbm_frac,
             "plain": plain, "e2e": e2e, "served": served, "roofline": roofline,
+            "other_configs": other_configs,
             "cpu_baseline": cpu,
             "host_us_per_dm": host_us,
             "clocks": clocks, "gpu_launches": launches, "candidates": ncand,
@@ -1148,6 +1169,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip configs 3 and 5 in the default run")
     ap.add_argument("--fft-form", type=int, default=0,
                     help="0: default (3 where the length allows it); 1: cuFFT complex "
                          "transform + fused unpack/interbin/normalise; 2: the reference's "
@@ -1193,9 +1216,11 @@ def main():
         elif args.impl == "reference":
             rc = run_reference(args, ws, rank)
         elif args.config == 3:
-            rc = run_config3(args)
+            run_config3(args)
+            rc = 0
         elif args.config == 5:
-            rc = run_config5(args)
+            run_config5(args)
+            rc = 0
         else:
             rc = run_psx(args, ws, rank, local)
     finally:
