@@ -594,7 +594,10 @@ def run_config3(args, emit=True):
                                    nharmonics=4, min_snr=7.0, cfreq_hz=synth.CFREQ_HZ,
                                    ch_bw_hz=synth.CH_BW_HZ, mode=mode, batch=batch,
                                    harm_shape=shape)
-    tune = search.autotune(params("batched"), batches=(4, 8, 16, 32), reps=4)
+    if args.batch:
+        tune = {"batch": args.batch, "harm_shape": args.harm_shape}
+    else:
+        tune = search.autotune(params("batched"), batches=(4, 8, 16, 32), reps=4)
     ap = AccelerationPlan(-50.0, 50.0, 1.10, 64e-6, n, ts, synth.CFREQ_HZ, synth.CH_BW_HZ)
     ntr = [len(ap.generate_accel_list(float(d), 0.0)) for d in dms]
     stream = torch.cuda.Stream()
@@ -951,6 +954,7 @@ def run_psx(args, ws, rank, local):
         t0 = time.perf_counter()
         sub = _ap.Namespace(**vars(args))
         sub.ndm = 0
+        sub.batch, sub.harm_shape = 0, 0   # each config tunes its own
         other_configs = {"3": run_config3(sub, emit=False), "5": run_config5(sub, emit=False)}
         log(f"[rank {rank}] configs 3 and 5 in {time.perf_counter() - t0:.1f}s")
     if rank == 0:
