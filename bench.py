@@ -593,7 +593,7 @@ def run_config3(args, emit=True):
         return search.SearchParams(fft_size=n, tsamp=ts, acc_lo=-50.0, acc_hi=50.0,
                                    nharmonics=4, min_snr=7.0, cfreq_hz=synth.CFREQ_HZ,
                                    ch_bw_hz=synth.CH_BW_HZ, mode=mode, batch=batch,
-                                   harm_shape=shape)
+                                   harm_shape=shape, group_dms=args.group_dms)
     if args.batch:
         tune = {"batch": args.batch, "harm_shape": args.harm_shape}
     else:
@@ -651,7 +651,8 @@ def run_config3(args, emit=True):
         "metric": "DM x accel trials/s, config 3 (2048 DM x 2^22)", "config_id": 3,
         "value": vb, "unit": "trials/s", "higher_is_better": True,
         "batched": {"value": vb, "seconds": tb, "dm_trials": ndm, "trials": tot_b,
-                    "batch": tune["batch"], "harm_shape": tune["harm_shape"]},
+                    "batch": tune["batch"], "harm_shape": tune["harm_shape"],
+                    "group_dms": info["group_dms"]},
         "plain": {"value": vp, "seconds": tp, "dm_trials": int(nsample), "trials": tot_p},
         "batched_over_plain": vb / vp,
         "candidate_sets_equal_on_plain_sample": bool(same),
@@ -1170,6 +1171,8 @@ def main():
                     help="trials per launch group (0: autotuned together with the shape)")
     ap.add_argument("--harm-shape", type=int, default=0,
                     help="with --batch: harmonic-kernel shape (0: the default shape)")
+    ap.add_argument("--group-dms", type=int, default=0,
+                    help="DM trials per grouped prologue (0: default rule, 1: off)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

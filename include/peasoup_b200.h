@@ -421,6 +421,16 @@ typedef struct {
                                   gather in its first pass, then the unpack
                                   kernel (fft_size 2^19 .. 2^25 or
                                   3 * 2^17 .. 3 * 2^23) */
+    int group_dms;             /* batched: DM trials of a psx_search_block
+                                  call whose per-DM prologues (baseline
+                                  removal through the inverse transform) run
+                                  as one batch of row-indexed launches and
+                                  batched cuFFT plans.  0 = default: 4 when
+                                  fft_size <= 2^22 and the call's DM trials
+                                  average at most 32 acceleration trials,
+                                  else off; 1 = off; 2..16 = that many
+                                  whenever the call has more DM trials than
+                                  that.  Results do not depend on it. */
 } psx_search_config;
 
 /* Number of tile shapes of the fused harmonic-sum kernel (tile bins,
@@ -513,6 +523,8 @@ typedef struct {
                              transform + fused unpack, 2 real transform (the
                              reference's), 3 the library's own two-pass
                              transform with the resample in its first pass */
+    int group_dms;        /* DM trials per grouped prologue in the last call
+                             (0: one prologue per DM trial) */
 } psx_search_info;
 
 int psx_search_last_info(const psx_search* s, psx_search_info* info);
@@ -563,8 +575,9 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
                          float* h_tim_r, float* h_pspec, float* h_norm2);
 
 /* Reuses an instance for another request with the same transform length,
-   folds, mode, batch, harmonic shape and lanes (the things its
-   buffers and plans depend on): acceleration range, tsamp, thresholds,
+   folds, mode, batch, harmonic shape, lanes, transform path and prologue
+   grouping rows (the things its buffers and plans depend on):
+   acceleration range, tsamp, thresholds,
    frequency limits and birdies may all change.  Waits for the instance's
    queued work first.  No counterpart in the reference (whose Worker builds
    its transforms once per process, src/pipeline_multi.cu:114-149). */

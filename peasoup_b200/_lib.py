@@ -62,7 +62,7 @@ class SearchConfig(C.Structure):
                 ("birdie_freqs", C.POINTER(C.c_float)), ("birdie_widths", C.POINTER(C.c_float)),
                 ("nbirdies", C.c_size_t), ("mode", C.c_int), ("batch", C.c_int),
                 ("use_fft_callback", C.c_int), ("use_graph", C.c_int), ("harm_shape", C.c_int),
-                ("lanes", C.c_int), ("fft_form", C.c_int)]
+                ("lanes", C.c_int), ("fft_form", C.c_int), ("group_dms", C.c_int)]
 
 
 class SearchInfo(C.Structure):
@@ -70,7 +70,8 @@ class SearchInfo(C.Structure):
                 ("fft_launches", C.c_int), ("above_threshold", C.c_longlong),
                 ("fft_callback", C.c_int), ("graph", C.c_int), ("batch", C.c_int),
                 ("baseline_passes", C.c_int), ("harm_shape", C.c_int),
-                ("capture_fallbacks", C.c_int), ("fft_form", C.c_int)]
+                ("capture_fallbacks", C.c_int), ("fft_form", C.c_int),
+                ("group_dms", C.c_int)]
 
 
 class SearchProfile(C.Structure):

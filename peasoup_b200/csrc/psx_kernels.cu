@@ -196,8 +196,15 @@ __device__ __forceinline__ float median_at(const MedianLevels& L, unsigned k)
 
 __global__ void __launch_bounds__(256) k_median_apply(MedianLevels L, size_t nbins,
                                                       float* __restrict__ median_out,
-                                                      float* __restrict__ X)
+                                                      float* __restrict__ X, size_t x_stride = 0,
+                                                      size_t m_stride = 0)
 {
+    if (blockIdx.y) {  // row blockIdx.y of a batch (strides in floats)
+        L.m5 += (size_t)blockIdx.y * m_stride;
+        L.m25 += (size_t)blockIdx.y * m_stride;
+        L.m125 += (size_t)blockIdx.y * m_stride;
+        if (X) X += (size_t)blockIdx.y * x_stride;
+    }
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nbins; k += stride) {
         const float m = median_at(L, (unsigned)k);
@@ -256,8 +263,14 @@ constexpr int kScrGroups = 16;  // 125-bin groups per CTA step
 __global__ void __launch_bounds__(256) k_amp_scrunch3(const float* __restrict__ X, size_t nbins,
                                                       float* __restrict__ m5, size_t n5,
                                                       float* __restrict__ m25, size_t n25,
-                                                      float* __restrict__ m125, size_t n125)
+                                                      float* __restrict__ m125, size_t n125,
+                                                      size_t x_stride = 0, size_t m_stride = 0)
 {
+    // row blockIdx.y of a batch: its spectrum and its scratch (strides in floats)
+    X += (size_t)blockIdx.y * x_stride;
+    m5 += (size_t)blockIdx.y * m_stride;
+    m25 += (size_t)blockIdx.y * m_stride;
+    m125 += (size_t)blockIdx.y * m_stride;
     __shared__ float s5[kScrGroups * 25];
     __shared__ float s25[kScrGroups * 5];
     const size_t ngroups = (n5 + 24) / 25;  // groups holding any 5-level value
@@ -392,8 +405,9 @@ int launch_running_median(const float* d_powers, size_t nbins, double bin_width,
 // One warp per birdie; lanes stride the birdie's bin range.
 __global__ void k_zap(float* __restrict__ X, const float* __restrict__ freqs,
                       const float* __restrict__ widths, float bin_width, unsigned nbirdies,
-                      unsigned nbins)
+                      unsigned nbins, size_t x_stride = 0)
 {
+    X += (size_t)blockIdx.y * x_stride;  // row blockIdx.y of a batch
     const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const unsigned lane = threadIdx.x & 31;
     if (warp >= nbirdies) return;
@@ -464,9 +478,15 @@ __global__ void __launch_bounds__(256) k_sum_partials(Src src, size_t first, siz
 // code does (stats.hpp:20-31 and src/kernels.cu:443,458), without
 // contraction.
 __global__ void k_finish_stats(const double2* __restrict__ partials, int nparts, double count,
-                               double* __restrict__ sums, float* __restrict__ stat, float scale)
+                               double* __restrict__ sums, float* __restrict__ stat, float scale,
+                               size_t part_stride = 0, size_t sums_stride = 0,
+                               size_t stat_stride = 0)
 {
     if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    // row blockIdx.y of a batch (strides in elements)
+    partials += (size_t)blockIdx.y * part_stride;
+    sums += (size_t)blockIdx.y * sums_stride;
+    if (stat) stat += (size_t)blockIdx.y * stat_stride;
     double a, b;
     warp_sum_partials(partials, nparts, a, b);
     if (threadIdx.x != 0) return;
@@ -542,8 +562,15 @@ constexpr int kVecThreads = 512;
 __global__ void __launch_bounds__(kVecThreads) k_partials_v4(const float* __restrict__ x, size_t n,
                                                              double2* __restrict__ partials,
                                                              float* __restrict__ copy,
-                                                             unsigned* __restrict__ state)
+                                                             unsigned* __restrict__ state,
+                                                             size_t x_stride = 0,
+                                                             size_t part_stride = 0,
+                                                             size_t state_stride = 0)
 {
+    // row blockIdx.y of a batch (strides in elements; no copy in a batch)
+    x += (size_t)blockIdx.y * x_stride;
+    partials += (size_t)blockIdx.y * part_stride;
+    if (state) state += (size_t)blockIdx.y * state_stride;
     if (state && blockIdx.x == 0 && threadIdx.x == 0) {
         state[0] = 1u;
         state[1] = 0u;
@@ -579,8 +606,20 @@ __global__ void __launch_bounds__(kVecThreads) k_baseline_pass_v4(
     float* __restrict__ x, size_t n, double count, const double2* __restrict__ part_in,
     int nparts, double2* __restrict__ part_out, const unsigned* __restrict__ flag_in,
     unsigned* __restrict__ flag_out, unsigned* __restrict__ passes,
-    unsigned* __restrict__ fin_flag, unsigned* __restrict__ fin_passes)
+    unsigned* __restrict__ fin_flag, unsigned* __restrict__ fin_passes, size_t x_stride = 0,
+    size_t part_stride = 0, size_t flag_stride = 0)
 {
+    if (blockIdx.y) {  // row blockIdx.y of a batch (strides in elements)
+        const size_t r = blockIdx.y;
+        x += r * x_stride;
+        part_in += r * part_stride;
+        part_out += r * part_stride;
+        flag_in += r * flag_stride;
+        flag_out += r * flag_stride;
+        passes += r * flag_stride;
+        if (fin_flag) fin_flag += r * flag_stride;
+        if (fin_passes) fin_passes += r * flag_stride;
+    }
     __shared__ float s_mean;
     __shared__ int s_go;
     if (*flag_in == 0u) {
@@ -641,8 +680,12 @@ __global__ void __launch_bounds__(kVecThreads) k_baseline_pass_v4(
 // bin's pair from a 64-bit load; the odd last bin is added by block 0.
 __global__ void __launch_bounds__(kVecThreads) k_interbin_partials_v4(const float* __restrict__ X,
                                                                       size_t nbins,
-                                                                      double2* __restrict__ partials)
+                                                                      double2* __restrict__ partials,
+                                                                      size_t x_stride = 0,
+                                                                      size_t part_stride = 0)
 {
+    X += (size_t)blockIdx.y * x_stride;  // row blockIdx.y of a batch
+    partials += (size_t)blockIdx.y * part_stride;
     double s = 0.0, s2 = 0.0;
     const size_t npairs = nbins / 2, stride = (size_t)gridDim.x * blockDim.x;
     const float4* X4 = reinterpret_cast<const float4*>(X);
@@ -694,6 +737,101 @@ int launch_interbin_stats_v4(const float* d_X, size_t nbins, double2* d_partials
     return launch_status("interbin statistics kernels");
 }
 
+// ---- row-batched prologue stages (the grouped prologue of the engine)
+int launch_partials_rows(const float* d_x, size_t n, size_t x_stride, int rows,
+                         double2* d_partials, size_t part_stride, unsigned* d_state,
+                         size_t state_stride, cudaStream_t s)
+{
+    if (rows < 1 || rows > 65535) {
+        set_error("partial sums: bad row count %d", rows);
+        return PSX_ERR_INVALID;
+    }
+    k_partials_v4<<<dim3(reduction_blocks(), rows), kVecThreads, 0, s>>>(
+        d_x, n, d_partials, nullptr, d_state, x_stride, part_stride, state_stride);
+    return launch_status("partial sums kernel (rows)");
+}
+
+int launch_baseline_pass_rows(float* d_x, size_t n, size_t x_stride, int rows,
+                              const double2* d_part_in, double2* d_part_out, size_t part_stride,
+                              const unsigned* d_flag_in, unsigned* d_flag_out,
+                              unsigned* d_passes, unsigned* d_fin_flag, unsigned* d_fin_passes,
+                              size_t flag_stride, cudaStream_t s)
+{
+    const int nb = reduction_blocks();
+    k_baseline_pass_v4<<<dim3(nb, rows), kVecThreads, 0, s>>>(
+        d_x, n, (double)n, d_part_in, nb, d_part_out, d_flag_in, d_flag_out, d_passes, d_fin_flag,
+        d_fin_passes, x_stride, part_stride, flag_stride);
+    return launch_status("baseline pass kernel (rows)");
+}
+
+int launch_running_median_spectrum_rows(float* d_X, size_t x_stride, int rows, size_t nbins,
+                                        double bin_width, float b5, float b25, void* d_scratch,
+                                        size_t scratch_stride_floats, cudaStream_t s)
+{
+    if (!d_X || !d_scratch || nbins < 125 || nbins > 0xffffffffu) {
+        set_error("running median: bad arguments (nbins=%zu)", nbins);
+        return PSX_ERR_INVALID;
+    }
+    auto up = [](size_t v) { return (v + 63) / 64 * 64; };
+    float* m5 = static_cast<float*>(d_scratch);
+    float* m25 = m5 + up(nbins / 5 + 1);
+    float* m125 = m25 + up(nbins / 25 + 1);
+    const size_t n5 = nbins / 5, n25 = n5 / 5, n125 = n25 / 5;
+    const size_t ngroups = (n5 + 24) / 25;
+    const unsigned grid = (unsigned)std::min<size_t>((ngroups + kScrGroups - 1) / kScrGroups,
+                                                     (size_t)sm_count() * 8);
+    k_amp_scrunch3<<<dim3(grid, rows), 256, 0, s>>>(d_X, nbins, m5, n5, m25, n25, m125, n125,
+                                                     x_stride, scratch_stride_floats);
+    PSX_TRY(launch_status("amplitude + scrunch kernel (rows)"));
+    int pos5 = (int)((double)b5 / bin_width);
+    int pos25 = (int)((double)b25 / bin_width);
+    MedianLevels L;
+    L.m5 = m5;
+    L.m25 = m25;
+    L.m125 = m125;
+    L.n5 = (unsigned)n5;
+    L.n25 = (unsigned)n25;
+    L.n125 = (unsigned)n125;
+    L.step5 = stretch_step(n5, nbins);
+    L.step25 = stretch_step(n25, nbins);
+    L.step125 = stretch_step(n125, nbins);
+    L.pos5 = (unsigned)(pos5 < 0 ? 0 : (size_t)pos5 > nbins ? nbins : pos5);
+    L.pos25 = (unsigned)(pos25 < 0 ? 0 : (size_t)pos25 > nbins ? nbins : pos25);
+    if (L.pos25 < L.pos5) L.pos25 = L.pos5;
+    k_median_apply<<<dim3(grid_for(nbins, 256), rows), 256, 0, s>>>(
+        L, nbins, nullptr, d_X, x_stride, scratch_stride_floats);
+    return launch_status("median apply kernel (rows)");
+}
+
+int launch_zap_rows(float* d_X, size_t x_stride, int rows, const float* d_freqs,
+                    const float* d_widths, float bin_width, size_t nbirdies, size_t nbins,
+                    cudaStream_t s)
+{
+    if (nbirdies == 0) return PSX_OK;
+    if (!d_X || !d_freqs || !d_widths) {
+        set_error("zap: null pointer");
+        return PSX_ERR_INVALID;
+    }
+    const unsigned T = 256;
+    const unsigned blocks = (unsigned)((nbirdies * 32 + T - 1) / T);
+    k_zap<<<dim3(blocks, rows), T, 0, s>>>(d_X, d_freqs, d_widths, bin_width, (unsigned)nbirdies,
+                                          (unsigned)nbins, x_stride);
+    return launch_status("zap kernel (rows)");
+}
+
+int launch_interbin_stats_rows(const float* d_X, size_t x_stride, int rows, size_t nbins,
+                               double2* d_partials, size_t part_stride, double* d_sums,
+                               size_t sums_stride, float* d_stat, size_t stat_stride, float scale,
+                               cudaStream_t s)
+{
+    const int nb = reduction_blocks();
+    k_interbin_partials_v4<<<dim3(nb, rows), kVecThreads, 0, s>>>(d_X, nbins, d_partials, x_stride,
+                                                                  part_stride);
+    k_finish_stats<<<dim3(1, rows), 32, 0, s>>>(d_partials, nb, (double)nbins, d_sums, d_stat,
+                                                scale, part_stride, sums_stride, stat_stride);
+    return launch_status("interbin statistics kernels (rows)");
+}
+
 int launch_partials(const float* d_x, size_t n, double2* d_partials, cudaStream_t s)
 {
     k_sum_partials<PlainSrc><<<reduction_blocks(), 256, 0, s>>>(PlainSrc{d_x}, 0, n, d_partials);
@@ -728,8 +866,9 @@ __global__ void k_sub_scalar(float* __restrict__ x, size_t n, const float* __res
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] -= m;
 }
 
-__global__ void k_fill(float* __restrict__ x, size_t n, float value)
+__global__ void k_fill(float* __restrict__ x, size_t n, float value, size_t x_stride = 0)
 {
+    x += (size_t)blockIdx.y * x_stride;  // row blockIdx.y of a batch
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = value;
 }
@@ -754,6 +893,15 @@ int launch_fill(float* d_x, size_t n, float value, cudaStream_t s)
     if (n == 0) return PSX_OK;
     k_fill<<<grid_for(n, 256), 256, 0, s>>>(d_x, n, value);
     return launch_status("fill kernel");
+}
+
+int launch_fill_rows(float* d_x, size_t n, size_t x_stride, int rows, float value,
+                     cudaStream_t s)
+{
+    if (n == 0) return PSX_OK;
+    dim3 grid(grid_for(n, 256), rows);
+    k_fill<<<grid, 256, 0, s>>>(d_x, n, value, x_stride);
+    return launch_status("fill kernel (rows)");
 }
 
 // Mean of d_x[0..n) in float as the reference forms it (float sum / float

@@ -383,6 +383,29 @@ static int launch_harm(int F, int shape, const float* p, size_t ppitch, unsigned
 
 constexpr int kDeviceBaselinePasses = 4;
 
+// Grouped prologue: DM trials per group by default, the largest transform
+// it applies to by default, and the most acceleration trials per DM trial
+// (averaged over a call) for which the default groups.  Measured on B200
+// with 1-3 trials per DM trial: 4 rows take the per-DM cost from 89 to
+// 55 us at 2^19 points and from 93 to 65 us at 2^20 (8 and 16 rows a
+// little less), 150 to 141 us at 2^22, nothing at 2^23, where the
+// prologue's launches are long enough to fill the device on their own.
+// With many trials per DM trial the trials outweigh the prologue and the
+// two slots' overlap already hides it.
+constexpr int kGroupRowsDefault = 4;
+constexpr int kGroupRowsMax = 16;
+constexpr size_t kGroupMaxPoints = (size_t)1 << 22;
+constexpr double kGroupMaxTrials = 32.0;
+
+// Rows of the group sets an instance of this configuration may use (0: it
+// never groups).
+static int group_rows_for(const psx_search_config* c)
+{
+    if (c->mode != PSX_MODE_BATCHED || c->group_dms == 1) return 0;
+    if (c->group_dms >= 2) return c->group_dms;
+    return c->fft_size <= kGroupMaxPoints ? kGroupRowsDefault : 0;
+}
+
 // Tensor maps of a spectrum buffer of `rows` rows of `pitch` floats for
 // the multi-row harmonic kernel: the rows as 8-byte elements, one map per
 // window width 32 (c + 1) floats, boxes [width, box_rows]; out-of-bounds
@@ -493,6 +516,26 @@ struct Slot {
     int launches = 0;
     int ffts = 0;
     bool profiled = false;
+    // a slot of a group set: its device buffers are rows of the set's
+    // arrays (not freed on their own), its prologue stream is the set's
+    bool grouped = false;
+};
+
+// Grouped prologue (DM trials with few acceleration trials): G slots whose
+// per-DM buffers are rows of contiguous arrays, so that the prologues of G
+// DM trials run as one batch -- batched cuFFT plans and row-indexed
+// kernels -- instead of G sequences of small launches.
+struct GroupSet {
+    std::vector<Slot> slots;  // G slots
+    float* tim = nullptr;     // G x N dereddened series
+    float* Xp = nullptr;      // G x 2 Bp prologue spectra
+    float* med = nullptr;     // G x med_floats median scratch
+    double2* part = nullptr;  // G x 2 nb partial sums
+    double* sums = nullptr;   // G x 2
+    float* stat = nullptr;    // G x 8
+    unsigned* count = nullptr;  // G x 16 counters and flags
+    float* mean = nullptr;    // G x 2
+    FftPlan r2c, c2r;         // batch-G plans over the rows
 };
 
 struct GraphEntry {
@@ -547,6 +590,10 @@ struct psx_search {
     TwSteps tw_steps{};  // unit rotations of the fused unpack kernel
 
     Slot slot[2];
+    // grouped prologue (0 = off): two sets of kGroupRows slots, used in turn
+    int group_rows = 0;
+    size_t med_floats = 0;
+    GroupSet gset[2];
     FftPlan r2c1;                      // plain-mode trials and the debug tap
     Fft4Plan f4;                       // the hand-written transform (fft_form 3)
     bool use_f4 = false;
@@ -555,7 +602,7 @@ struct psx_search {
     std::map<long long, GraphEntry> graphs;
     std::map<long long, int> capture_failures;
 
-    int last_slot = 0;
+    Slot* last_dm = nullptr;  // the slot of the last DM trial finished (debug tap)
     bool profile = false;
     psx_search_profile prof{};
     psx_search_info info{};
@@ -614,6 +661,8 @@ struct psx_search {
         call_start = nullptr;
         if (h_mean) cudaFreeHost(h_mean);
         h_mean = nullptr;
+        last_dm = nullptr;
+        free_groups();
         for (Slot& s : slot) {
             if (s.d_rec) cudaFree(s.d_rec);
             if (s.d_count) cudaFree(s.d_count);
@@ -656,6 +705,12 @@ struct psx_search {
     int grow_ktab(Slot& s, size_t need);
     int ensure_events(Slot& s, int groups);
     int prologue(Slot& s);
+    int prologue_group(GroupSet& g, int count, cudaStream_t ps);
+    int prep(Slot& s, const float* series, size_t nsamps, bool on_device, float dm, int dm_idx);
+    int enqueue_trials(Slot& s);
+    int alloc_groups();
+    void free_groups();
+    int group_rows_for_call(const float* dms, int ndm) const;
     int trials_enqueue(Slot& s, int nacc);
     int trials_range(Slot& s, int t_begin, int t_end, bool reset);
     int run_trials(Slot& s, int nacc);
@@ -783,6 +838,13 @@ int psx_search::ensure_events(Slot& s, int groups)
 // the prologue of DM d+1 runs alongside the trials of DM d.
 int psx_search::prologue(Slot& s)
 {
+    if (!s.r2c) {  // a grouped slot run on its own (a retry): batch-1 plans on first need
+        s.r2c = new (std::nothrow) FftPlan;
+        s.c2r = new (std::nothrow) FftPlan;
+        if (!s.r2c || !s.c2r) return PSX_ERR_ALLOC;
+        PSX_TRY(s.r2c->create(N, 1, PSX_FFT_R2C, 0, 0));
+        PSX_TRY(s.c2r->create(N, 1, PSX_FFT_C2R, 0, 0));
+    }
     cudaStream_t ps = s.pst;
     PSX_CUDA(cudaStreamWaitEvent(ps, call_start, 0));
     PSX_CUDA(cudaStreamWaitEvent(ps, s.done, 0));
@@ -853,6 +915,168 @@ int psx_search::prologue(Slot& s)
     ++s.ffts;
     if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[1], ps));
     PSX_CUDA(cudaEventRecord(s.ready, ps));
+    return PSX_OK;
+}
+
+// Group sets, made on the first call that groups: per set, the per-DM
+// buffers of G slots as rows of contiguous arrays (row strides N, 2 Bp,
+// the median scratch, 2 nb, 2, 8, 16 and 2 elements), the batch-G plans
+// of the prologue's transforms, and per slot its own record buffer, factor
+// table, pinned counters and events.
+int psx_search::alloc_groups()
+{
+    if (!gset[0].slots.empty()) return PSX_OK;
+    const int G = group_rows_for(&cfg);
+    if (G < 2) return PSX_OK;
+    const size_t nb = (size_t)reduction_blocks();
+    med_floats = median_scratch_bytes(B) / sizeof(float);
+    for (GroupSet& g : gset) {
+        PSX_CUDA(cudaMalloc((void**)&g.tim, sizeof(float) * N * G));
+        PSX_CUDA(cudaMalloc((void**)&g.Xp, sizeof(float) * 2 * Bp * G));
+        PSX_CUDA(cudaMalloc((void**)&g.med, sizeof(float) * med_floats * G));
+        PSX_CUDA(cudaMalloc((void**)&g.part, sizeof(double2) * 2 * nb * G));
+        PSX_CUDA(cudaMalloc((void**)&g.sums, sizeof(double) * 2 * G));
+        PSX_CUDA(cudaMalloc((void**)&g.stat, sizeof(float) * 8 * G));
+        PSX_CUDA(cudaMalloc((void**)&g.count, sizeof(unsigned) * 16 * G));
+        PSX_CUDA(cudaMalloc((void**)&g.mean, sizeof(float) * 2 * G));
+        // rows past a call's last DM trial are transformed too (the plans
+        // hold G rows): they start as zeros, never as uninitialised memory
+        PSX_CUDA(cudaMemsetAsync(g.tim, 0, sizeof(float) * N * G, st));
+        PSX_CUDA(cudaMemsetAsync(g.Xp, 0, sizeof(float) * 2 * Bp * G, st));
+        PSX_TRY(g.r2c.create(N, G, PSX_FFT_R2C, N, Bp));
+        PSX_TRY(g.c2r.create(N, G, PSX_FFT_C2R, Bp, N));
+        g.slots.resize(G);
+        for (int i = 0; i < G; ++i) {
+            Slot& sl = g.slots[i];
+            sl.grouped = true;
+            sl.d_tim = g.tim + (size_t)i * N;
+            sl.d_Xp = g.Xp + (size_t)i * 2 * Bp;
+            sl.d_med = g.med + (size_t)i * med_floats;
+            sl.d_part = g.part + (size_t)i * 2 * nb;
+            sl.d_sums = g.sums + 2 * i;
+            sl.d_stat = g.stat + 8 * i;
+            sl.d_count = g.count + 16 * i;
+            sl.d_mean = g.mean + 2 * i;
+            PSX_CUDA(cudaMallocHost(&sl.h_count, sizeof(unsigned) * 4));
+            PSX_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+            PSX_CUDA(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));
+            PSX_CUDA(cudaEventCreateWithFlags(&sl.ready, cudaEventDisableTiming));
+            PSX_TRY(grow_records(sl, (size_t)1 << 18));
+            PSX_TRY(grow_ktab(sl, 64));
+        }
+    }
+    PSX_CUDA(cudaStreamSynchronize(st));
+    return PSX_OK;
+}
+
+void psx_search::free_groups()
+{
+    for (Slot& s : slot)
+        if (s.pst) cudaStreamSynchronize(s.pst);
+    for (GroupSet& g : gset) {
+        for (Slot& s : g.slots) {
+            if (s.d_rec) cudaFree(s.d_rec);
+            if (s.d_ktab) cudaFree(s.d_ktab);
+            if (s.h_rec) cudaFreeHost(s.h_rec);
+            if (s.h_count) cudaFreeHost(s.h_count);
+            if (s.h_ktab) cudaFreeHost(s.h_ktab);
+            for (cudaEvent_t e : {s.done, s.copied, s.ready})
+                if (e) cudaEventDestroy(e);
+            for (cudaEvent_t e : s.ev) cudaEventDestroy(e);
+            delete s.r2c;  // batch-1 plans of a retried DM trial, if any
+            delete s.c2r;
+        }
+        g.slots.clear();
+        void* dev[] = {g.tim, g.Xp, g.med, g.part, g.sums, g.stat, g.count, g.mean};
+        for (void* q : dev)
+            if (q) cudaFree(q);
+        g.tim = g.Xp = g.med = g.stat = g.mean = nullptr;
+        g.part = nullptr;
+        g.sums = nullptr;
+        g.count = nullptr;
+        g.r2c.destroy();
+        g.c2r.destroy();
+    }
+}
+
+// Rows per grouped prologue for a call over these DM trials (0: one
+// prologue per DM trial).  A call groups when it has more DM trials than a
+// group holds; by default also only when its DM trials average at most
+// kGroupMaxTrials acceleration trials.
+int psx_search::group_rows_for_call(const float* dms, int ndm) const
+{
+    const int G = group_rows_for(&cfg);
+    if (G < 2 || ndm <= G) return 0;
+    if (cfg.group_dms >= 2) return G;
+    const psx_search_config& c = cfg;
+    double total = 0.0;
+    for (int d = 0; d < ndm; ++d)
+        total += (double)accel_list(c.acc_lo, c.acc_hi, c.acc_tol, c.acc_pulse_width, N, c.tsamp,
+                                    c.cfreq_hz, c.ch_bw_hz, dms[d], c.cdm)
+                     .size();
+    return total <= kGroupMaxTrials * ndm ? G : 0;
+}
+
+// The prologues of the first `count` slots of a group set as one batch:
+// each launch of prologue() becomes one launch over `count` rows (grid y =
+// row) that computes every row exactly as the single-row launch computes
+// it, and the two transforms run as batch-G plans.  On stream ps, after the
+// caller's work queued before the call and after every slot of the set is
+// done with its previous DM trial; records each slot's ready.
+int psx_search::prologue_group(GroupSet& g, int count, cudaStream_t ps)
+{
+    PSX_CUDA(cudaStreamWaitEvent(ps, call_start, 0));
+    for (Slot& sl : g.slots) PSX_CUDA(cudaStreamWaitEvent(ps, sl.done, 0));
+    Slot& s0 = g.slots[0];
+    if (s0.profiled) PSX_CUDA(cudaEventRecord(s0.ev[0], ps));
+    const size_t ncopy = std::min(s0.nsamps, N);  // one length for every series of a call
+    for (int i = 0; i < count; ++i) {
+        Slot& sl = g.slots[i];
+        sl.pst = ps;
+        PSX_CUDA(cudaMemcpyAsync(sl.d_tim, sl.series, sizeof(float) * ncopy,
+                                 sl.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 ps));
+    }
+    // baseline removal (timeseries.hpp:282-287, src/kernels.cu:463-479):
+    // the device loop of prologue(), row by row
+    const size_t nb = (size_t)reduction_blocks(), pst_ = 2 * nb;
+    unsigned* c = g.count;
+    PSX_TRY(launch_partials_rows(g.tim, ncopy, N, count, g.part, pst_, c + 4, 16, ps));
+    for (int pass = 0; pass < kDeviceBaselinePasses; ++pass) {
+        const bool last = pass == kDeviceBaselinePasses - 1;
+        PSX_TRY(launch_baseline_pass_rows(
+            g.tim, ncopy, N, count, g.part + (pass & 1) * nb, g.part + ((pass + 1) & 1) * nb, pst_,
+            pass == 0 ? c + 4 : c + 6 + pass - 1, c + 6 + pass, c + 5, last ? c + 2 : nullptr,
+            last ? c + 3 : nullptr, 16, ps));
+    }
+    // zero padding (pipeline_multi.cu:179-187)
+    if (ncopy < N) PSX_TRY(launch_fill_rows(g.tim + ncopy, N - ncopy, N, count, 0.f, ps));
+    PSX_TRY(g.r2c.exec(g.tim, g.Xp, ps));
+    // amplitudes, medians and dereddening (spectrumformer.hpp:16-22,
+    // dereddener.hpp:41-66), zapping, interbin statistics
+    // (pipeline_multi.cu:230-234), inverse transform
+    PSX_TRY(launch_running_median_spectrum_rows(g.Xp, 2 * Bp, count, B, bin_width,
+                                                cfg.boundary_5_freq, cfg.boundary_25_freq, g.med,
+                                                med_floats, ps));
+    if (!bf.empty())
+        PSX_TRY(launch_zap_rows(g.Xp, 2 * Bp, count, d_bf, d_bw, bin_width_f, bf.size(), B, ps));
+    PSX_TRY(launch_interbin_stats_rows(g.Xp, 2 * Bp, count, B, g.part, pst_, g.sums, 2, g.stat, 8,
+                                       (float)N, ps));
+    PSX_TRY(g.c2r.exec(g.Xp, g.tim, ps));
+    const int launches = 5 + (ncopy < N ? 1 : 0) + 2 + (bf.empty() ? 0 : 1) + 2;
+    for (int i = 0; i < count; ++i) {
+        Slot& sl = g.slots[i];
+        // the batch's launches and transforms are counted once, on row 0
+        sl.launches += i == 0 ? launches : 0;
+        sl.ffts += i == 0 ? 2 : 0;
+        // profiling: the batch's span is row 0's prologue, the other rows
+        // get an empty one
+        if (sl.profiled) {
+            if (i) PSX_CUDA(cudaEventRecord(sl.ev[0], ps));
+            PSX_CUDA(cudaEventRecord(sl.ev[1], ps));
+        }
+        PSX_CUDA(cudaEventRecord(sl.ready, ps));
+    }
     return PSX_OK;
 }
 
@@ -976,7 +1200,9 @@ int psx_search::run_trials(Slot& s, int nacc)
 {
     // events recorded inside a graph carry no timestamps: profiling runs
     // the schedule without capture
-    const bool graph = batched() && cfg.use_graph && !s.profiled;
+    // (a grouped slot's schedule is launched directly: graphs are keyed by
+    // the two regular slots' buffers)
+    const bool graph = batched() && cfg.use_graph && !s.profiled && !s.grouped;
     if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch, fft4())));
     if (!graph) return trials_enqueue(s, nacc);
     // One lane: the graph holds the counter reset and the full launch groups
@@ -1040,12 +1266,12 @@ int psx_search::run_trials(Slot& s, int nacc)
     return PSX_OK;
 }
 
-int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
-                        int dm_idx)
+// The host half of one DM trial's set-up: its job fields, acceleration list
+// and factors, and the profiling events it needs.
+int psx_search::prep(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
+                     int dm_idx)
 {
-    const auto t_host = std::chrono::steady_clock::now();
     const psx_search_config& c = cfg;
-    PSX_TRY(apply_priority());
     s.series = series;
     s.nsamps = nsamps;
     s.on_device = on_device;
@@ -1061,12 +1287,30 @@ int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_dev
     PSX_TRY(grow_ktab(s, (size_t)nacc));
     for (int t = 0; t < nacc; ++t) s.h_ktab[t] = accel_fact(s.accs[t], c.tsamp);
     if (s.profiled) PSX_TRY(ensure_events(s, count_groups(nacc, batched(), batch, fft4())));
-    PSX_TRY(prologue(s));
+    return PSX_OK;
+}
+
+// The trials of a DM trial whose prologue is queued (s.ready): its factors,
+// the trial schedule, the hit counter's copy back and s.done.
+int psx_search::enqueue_trials(Slot& s)
+{
+    const int nacc = (int)s.accs.size();
     PSX_CUDA(cudaStreamWaitEvent(st, s.ready, 0));
     PSX_CUDA(cudaMemcpyAsync(s.d_ktab, s.h_ktab, sizeof(double) * nacc, cudaMemcpyHostToDevice, st));
     PSX_TRY(run_trials(s, nacc));
     PSX_CUDA(cudaMemcpyAsync(s.h_count, s.d_count, sizeof(unsigned) * 4, cudaMemcpyDeviceToHost, st));
     PSX_CUDA(cudaEventRecord(s.done, st));
+    return PSX_OK;
+}
+
+int psx_search::enqueue(Slot& s, const float* series, size_t nsamps, bool on_device, float dm,
+                        int dm_idx)
+{
+    const auto t_host = std::chrono::steady_clock::now();
+    PSX_TRY(apply_priority());
+    PSX_TRY(prep(s, series, nsamps, on_device, dm, dm_idx));
+    PSX_TRY(prologue(s));
+    PSX_TRY(enqueue_trials(s));
     prof.host_enqueue_ms += ms_since(t_host);
     return PSX_OK;
 }
@@ -1361,6 +1605,10 @@ static int check_config(const psx_search_config* c)
         set_error("search: lanes must be 0..2");
         return PSX_ERR_INVALID;
     }
+    if (c->group_dms < 0 || c->group_dms > kGroupRowsMax) {
+        set_error("search: group_dms must be 0..%d", kGroupRowsMax);
+        return PSX_ERR_INVALID;
+    }
     if (c->harm_shape < 0 || c->harm_shape > PSX_HARM_SHAPES) {
         set_error("search: harm_shape must be 0..%d", PSX_HARM_SHAPES);
         return PSX_ERR_INVALID;
@@ -1437,6 +1685,14 @@ size_t psx_search_footprint(const psx_search_config* c)
         bytes += sizeof(float) * 2 * Bp * 6 + sizeof(float2) * Fft4Plan::table_floats2(N);
     else
         bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
+    // two group sets of G rows (made on the first grouped call): series,
+    // prologue spectra, median scratch, each slot's first record buffer, and
+    // about one batch's worth of transform work area per batch-G plan
+    const size_t G = (size_t)group_rows_for(c);
+    if (G >= 2)
+        bytes += 2 * G *
+                 (sizeof(float) * (N + 2 * Bp) + median_scratch_bytes(B) +
+                  sizeof(int4) * ((size_t)1 << 18) + 2 * sizeof(float) * 2 * Bp);
     return bytes;
 }
 
@@ -1708,9 +1964,10 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
         effective_batch(cfg) != s->batch || shape != s->harm_shape ||
         effective_lanes(cfg) != s->lanes ||
-        effective_form(cfg) != effective_form(&s->cfg)) {
-        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, lanes and "
-                  "transform path must match the instance");
+        effective_form(cfg) != effective_form(&s->cfg) ||
+        group_rows_for(cfg) != group_rows_for(&s->cfg)) {
+        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, lanes, "
+                  "transform path and prologue grouping must match the instance");
         return PSX_ERR_INVALID;
     }
     PSX_CUDA(cudaSetDevice(s->device));
@@ -1840,23 +2097,57 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
             }
         });
     // (no early return from here until the collector is joined)
-    int rc = s->enqueue(s->slot[0], series[0], nsamps, series_on_device != 0, dms[0],
-                        dm_idx ? dm_idx[0] : 0);
-    for (int d = 0; d < ndm && rc == PSX_OK; ++d) {
-        if (d + 1 < ndm)
-            rc = s->enqueue(s->slot[(d + 1) & 1], series[d + 1], nsamps, series_on_device != 0,
-                            dms[d + 1], dm_idx ? dm_idx[d + 1] : d + 1);
-        if (rc != PSX_OK) break;
-        s->last_slot = d & 1;
+    auto finish_dm = [&](int d, Slot& sl) -> int {
+        s->last_dm = &sl;
         psx_search::DmRecords job;
-        rc = s->finish(s->slot[d & 1], job);
-        if (rc != PSX_OK) break;
+        const int r = s->finish(sl, job);
+        if (r != PSX_OK) return r;
         if (ndm == 1) {
             take(d, job);
         } else {
             std::lock_guard<std::mutex> lock(jmu);
             jobs.emplace_back(d, std::move(job));
             jcv.notify_one();
+        }
+        return PSX_OK;
+    };
+    const bool on_dev = series_on_device != 0;
+    const int G = s->group_rows_for_call(dms, ndm);
+    int rc = PSX_OK;
+    if (G) {
+        // Grouped prologues: chunks of G DM trials alternate between the two
+        // group sets; chunk c + 1's batched prologue (on slot (c + 1) & 1's
+        // stream) runs while chunk c's trials run, as the per-DM slots do.
+        rc = s->alloc_groups();
+        const int nchunks = (ndm + G - 1) / G;
+        auto enqueue_chunk = [&](int c) -> int {
+            const auto t_host = std::chrono::steady_clock::now();
+            GroupSet& g = s->gset[c & 1];
+            const int d0 = c * G, cnt = std::min(G, ndm - d0);
+            PSX_TRY(s->apply_priority());
+            for (int i = 0; i < cnt; ++i)
+                PSX_TRY(s->prep(g.slots[i], series[d0 + i], nsamps, on_dev, dms[d0 + i],
+                                dm_idx ? dm_idx[d0 + i] : d0 + i));
+            PSX_TRY(s->prologue_group(g, cnt, s->slot[c & 1].pst));
+            for (int i = 0; i < cnt; ++i) PSX_TRY(s->enqueue_trials(g.slots[i]));
+            s->prof.host_enqueue_ms += ms_since(t_host);
+            return PSX_OK;
+        };
+        if (rc == PSX_OK) rc = enqueue_chunk(0);
+        for (int c = 0; c < nchunks && rc == PSX_OK; ++c) {
+            if (c + 1 < nchunks) rc = enqueue_chunk(c + 1);
+            const int d0 = c * G, cnt = std::min(G, ndm - d0);
+            for (int i = 0; i < cnt && rc == PSX_OK; ++i)
+                rc = finish_dm(d0 + i, s->gset[c & 1].slots[i]);
+        }
+        s->info.group_dms = G;
+    } else {
+        rc = s->enqueue(s->slot[0], series[0], nsamps, on_dev, dms[0], dm_idx ? dm_idx[0] : 0);
+        for (int d = 0; d < ndm && rc == PSX_OK; ++d) {
+            if (d + 1 < ndm)
+                rc = s->enqueue(s->slot[(d + 1) & 1], series[d + 1], nsamps, on_dev, dms[d + 1],
+                                dm_idx ? dm_idx[d + 1] : d + 1);
+            if (rc == PSX_OK) rc = finish_dm(d, s->slot[d & 1]);
         }
     }
     if (collector.joinable()) {
@@ -1909,7 +2200,7 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered, float* h_
     clear_error();
     if (!s) return PSX_ERR_INVALID;
     // the dereddened series on the device is the last DM's
-    Slot& sl = s->slot[s->last_slot];
+    Slot& sl = s->last_dm ? *s->last_dm : s->slot[0];
     const std::vector<float>& accs = sl.accs;
     if (h_tim_dered)
         PSX_CUDA(cudaMemcpyAsync(h_tim_dered, sl.d_tim, sizeof(float) * s->N,

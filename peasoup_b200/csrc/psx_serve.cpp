@@ -47,19 +47,20 @@ using Clock = std::chrono::steady_clock;
 
 struct EngineKey {
     size_t n;
-    int folds, mode, batch, shape, callback, lanes, form;
+    int folds, mode, batch, shape, callback, lanes, form, group;
     bool operator==(const EngineKey& o) const
     {
         return n == o.n && folds == o.folds && mode == o.mode && batch == o.batch &&
                shape == o.shape && callback == o.callback && lanes == o.lanes &&
-               form == o.form;
+               form == o.form && group == o.group;
     }
 };
 
 EngineKey key_of(const psx_search_config& c)
 {
     return {c.fft_size, c.nharmonics, c.mode, c.batch, c.harm_shape,
-            c.mode == PSX_MODE_BATCHED && c.use_fft_callback ? 1 : 0, c.lanes, c.fft_form};
+            c.mode == PSX_MODE_BATCHED && c.use_fft_callback ? 1 : 0, c.lanes, c.fft_form,
+            c.group_dms};
 }
 
 struct Engine {

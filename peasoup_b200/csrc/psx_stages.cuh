@@ -65,4 +65,29 @@ int launch_interbin_stats_v4(const float* d_X, size_t nbins, double2* d_partials
 // x[i] -= *d_v.
 int launch_sub_scalar(float* d_x, size_t n, const float* d_v, cudaStream_t s);
 
+// Row-batched forms of the prologue stages over `rows` series laid out at
+// fixed strides (elements; row r of each buffer starts at base + r *
+// stride): the grouped prologue of the search engine.  Each row is computed
+// exactly as the single-row launcher computes it.
+int launch_partials_rows(const float* d_x, size_t n, size_t x_stride, int rows,
+                         double2* d_partials, size_t part_stride, unsigned* d_state,
+                         size_t state_stride, cudaStream_t s);
+int launch_baseline_pass_rows(float* d_x, size_t n, size_t x_stride, int rows,
+                              const double2* d_part_in, double2* d_part_out, size_t part_stride,
+                              const unsigned* d_flag_in, unsigned* d_flag_out,
+                              unsigned* d_passes, unsigned* d_fin_flag, unsigned* d_fin_passes,
+                              size_t flag_stride, cudaStream_t s);
+int launch_fill_rows(float* d_x, size_t n, size_t x_stride, int rows, float value,
+                     cudaStream_t s);
+int launch_running_median_spectrum_rows(float* d_X, size_t x_stride, int rows, size_t nbins,
+                                        double bin_width, float b5, float b25, void* d_scratch,
+                                        size_t scratch_stride_floats, cudaStream_t s);
+int launch_zap_rows(float* d_X, size_t x_stride, int rows, const float* d_freqs,
+                    const float* d_widths, float bin_width, size_t nbirdies, size_t nbins,
+                    cudaStream_t s);
+int launch_interbin_stats_rows(const float* d_X, size_t x_stride, int rows, size_t nbins,
+                               double2* d_partials, size_t part_stride, double* d_sums,
+                               size_t sums_stride, float* d_stat, size_t stat_stride, float scale,
+                               cudaStream_t s);
+
 }  // namespace psx

@@ -62,6 +62,9 @@ class SearchParams:
                                    # 1 cuFFT complex transform + fused unpack/interbin,
                                    # 2 the reference's real transform + interbin,
                                    # 3 the library's two-pass transform (resample in pass 1)
+    group_dms: int = 0             # batched: DM trials whose prologues run as one batch
+                                   # (0 default: 4 for <= 2^22 points and few trials
+                                   # per DM trial; 1 off; 2..16 that many)
 
     def to_c(self):
         cfg = SearchConfig()
@@ -83,6 +86,7 @@ class SearchParams:
         cfg.harm_shape = int(self.harm_shape)
         cfg.lanes = int(self.lanes)
         cfg.fft_form = int(self.fft_form)
+        cfg.group_dms = int(self.group_dms)
         return cfg, keep
 
 

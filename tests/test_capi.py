@@ -69,6 +69,12 @@ def test_invalid_arguments_fail_loudly(psx):
     cfg.use_fft_callback = 0
     cfg.fft_form = 4
     assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
+    cfg.fft_form = 0
+    for g in (-1, 17):
+        cfg.group_dms = g
+        assert psx.psx_search_create(C.byref(cfg), C.byref(h)) == _lib.PSX_ERR_INVALID
+        assert b"group_dms" in psx.psx_last_error()
+    cfg.group_dms = 0
     assert psx.psx_search_set_priority(None, 1) == _lib.PSX_ERR_INVALID
 
 
@@ -93,6 +99,16 @@ def test_footprint_model(psx):
     assert 0 < small < big
     plain = footprint(SearchParams(fft_size=1 << 23, tsamp=76e-6, mode="plain"))
     assert plain < big
+    # grouped prologues (default 4 rows up to 2^22 points) hold two sets of
+    # rows; longer transforms do not group unless asked
+    N = 1 << 22
+    grouped = footprint(SearchParams(fft_size=N, tsamp=64e-6, batch=16))
+    single = footprint(SearchParams(fft_size=N, tsamp=64e-6, batch=16, group_dms=1))
+    assert single + 2 * 4 * 12 * N < grouped < single + 2 * 4 * 24 * N
+    assert footprint(SearchParams(fft_size=N, tsamp=64e-6, batch=16, group_dms=8)) > grouped
+    big1 = footprint(SearchParams(fft_size=1 << 23, tsamp=64e-6, batch=16))
+    assert big1 == footprint(SearchParams(fft_size=1 << 23, tsamp=64e-6, batch=16, group_dms=1))
+    assert big1 < footprint(SearchParams(fft_size=1 << 23, tsamp=64e-6, batch=16, group_dms=4))
 
 
 def test_zaplist_parsing(psx):
