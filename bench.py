@@ -403,8 +403,8 @@ def run_served(nreq, rank, log_prefix, policy="least_work"):
     series = [_served_series(r, 1000 + i) for i, r in enumerate(reqs)] if pre else None
     torch.cuda.synchronize()
 
-    def one_pass(max_active, paced):
-        srv = serve.Server(SERVED_BUDGET, max_active=max_active, policy=policy)
+    def one_pass(max_active, paced, pol=policy):
+        srv = serve.Server(SERVED_BUDGET, max_active=max_active, policy=pol)
         res = [None] * len(reqs)
         tickets = [None] * len(reqs)
         ready = [th.Event() for _ in reqs]
@@ -442,43 +442,58 @@ def run_served(nreq, rank, log_prefix, policy="least_work"):
         srv.close()
         return res, arrivals
 
-    mixed, arr = one_pass(SERVED_SLOTS, True)
+    # the requested policy, and the other scheduling of the same stream for
+    # comparison (exclusive with one slot, least work first with two)
+    other = "least_work" if policy == "exclusive" else "exclusive"
+    slots = {p: 1 if p == "exclusive" else SERVED_SLOTS for p in (policy, other)}
+    runs = {p: one_pass(slots[p], True, p) for p in (policy, other)}
     alone, _ = one_pass(1, False)
     del series
-    trials = sum(s["ntrials"] for s in mixed)
-    lat_arr = [1e3 * (s["t_done"] - a) for s, a in zip(mixed, arr)]
-    lat_adm = [1e3 * (s["t_done"] - s["t_admit"]) for s in mixed]
     iso = [1e3 * (s["t_done"] - s["t_admit"]) for s in alone]
-    span = max(s["t_done"] for s in mixed) - min(arr)
-    served_tps = trials / span
-    isolated_tps = trials / (sum(iso) / 1e3)
-    ratio = [a / b for a, b in zip(lat_adm, iso)]
-    failed = sum(1 for s in mixed + alone if s["status"] != 0)
-    worst = sorted(range(len(reqs)), key=lambda i: -ratio[i])[:4]
-    return {
-        "requests": len(reqs), "failed": failed, "arrival_rate_per_s": 4.0,
-        "trials": int(trials), "trials_per_s": served_tps,
-        "latency_from_arrival_ms": {"p50": _pct(lat_arr, 50), "p95": _pct(lat_arr, 95),
-                                    "p99": _pct(lat_arr, 99)},
-        "latency_from_admission_ms": {"p50": _pct(lat_adm, 50), "p95": _pct(lat_adm, 95),
-                                      "p99": _pct(lat_adm, 99)},
-        "isolated_ms": {"p50": _pct(iso, 50), "p99": _pct(iso, 99)},
-        "p99_admitted_over_p99_isolated": _pct(lat_adm, 99) / _pct(iso, 99),
-        "per_request_ratio_p99": _pct(ratio, 99),
-        "per_request_ratio_p50": _pct(ratio, 50),
-        "worst_ratio_requests": [
-            {"fft_size": reqs[i].fft_size, "ndm": reqs[i].ndm, "trials": mixed[i]["ntrials"],
-             "admitted_ms": lat_adm[i], "isolated_ms": iso[i], "ratio": ratio[i]}
-            for i in worst],
-        "throughput_over_isolated_back_to_back": served_tps / isolated_tps,
-        "max_active": SERVED_SLOTS, "policy": policy, "hbm_budget_gb": SERVED_BUDGET / 1e9,
-        "engines_reused": int(sum(s["engine_reused"] for s in mixed)),
-        "series": "made on the GPU before the passes" if pre else "made at each arrival",
-        "workload": (f"{len(reqs)} requests, Poisson 4/s (seed 1), fft_size in 2^20..2^25 "
-                     f"incl. 3*2^k, DM count log-uniform 16..512 cut to <= "
-                     f"{SERVED_TRIAL_BUDGET} 2^23-equivalent trials per request, acc "
-                     f"half-range 10..300, 3..5 folds, white noise + one pulsar per DM"),
-    }
+
+    def summary(pol):
+        mixed, arr = runs[pol]
+        trials = sum(s["ntrials"] for s in mixed)
+        lat_arr = [1e3 * (s["t_done"] - a) for s, a in zip(mixed, arr)]
+        lat_adm = [1e3 * (s["t_done"] - s["t_admit"]) for s in mixed]
+        span = max(s["t_done"] for s in mixed) - min(arr)
+        served_tps = trials / span
+        isolated_tps = trials / (sum(iso) / 1e3)
+        ratio = [a / b for a, b in zip(lat_adm, iso)]
+        # from arrival: the time a request spends in the system over its
+        # isolated time (queueing included)
+        ratio_arr = [a / b for a, b in zip(lat_arr, iso)]
+        failed = sum(1 for s in mixed + alone if s["status"] != 0)
+        worst = sorted(range(len(reqs)), key=lambda i: -ratio[i])[:4]
+        return {
+            "requests": len(reqs), "failed": failed, "arrival_rate_per_s": 4.0,
+            "trials": int(trials), "trials_per_s": served_tps,
+            "latency_from_arrival_ms": {"p50": _pct(lat_arr, 50), "p95": _pct(lat_arr, 95),
+                                        "p99": _pct(lat_arr, 99)},
+            "latency_from_admission_ms": {"p50": _pct(lat_adm, 50), "p95": _pct(lat_adm, 95),
+                                          "p99": _pct(lat_adm, 99)},
+            "isolated_ms": {"p50": _pct(iso, 50), "p99": _pct(iso, 99)},
+            "p99_admitted_over_p99_isolated": _pct(lat_adm, 99) / _pct(iso, 99),
+            "per_request_ratio_p99": _pct(ratio, 99),
+            "per_request_ratio_p50": _pct(ratio, 50),
+            "per_request_arrival_ratio_p50": _pct(ratio_arr, 50),
+            "per_request_arrival_ratio_p99": _pct(ratio_arr, 99),
+            "worst_ratio_requests": [
+                {"fft_size": reqs[i].fft_size, "ndm": reqs[i].ndm, "trials": mixed[i]["ntrials"],
+                 "admitted_ms": lat_adm[i], "isolated_ms": iso[i], "ratio": ratio[i]}
+                for i in worst],
+            "throughput_over_isolated_back_to_back": served_tps / isolated_tps,
+            "max_active": slots[pol], "policy": pol, "hbm_budget_gb": SERVED_BUDGET / 1e9,
+            "engines_reused": int(sum(s["engine_reused"] for s in mixed)),
+            "series": "made on the GPU before the passes" if pre else "made at each arrival",
+            "workload": (f"{len(reqs)} requests, Poisson 4/s (seed 1), fft_size in 2^20..2^25 "
+                         f"incl. 3*2^k, DM count log-uniform 16..512 cut to <= "
+                         f"{SERVED_TRIAL_BUDGET} 2^23-equivalent trials per request, acc "
+                         f"half-range 10..300, 3..5 folds, white noise + one pulsar per DM"),
+        }
+    out = summary(policy)
+    out["compared_policy"] = summary(other)
+    return out
 
 
 # ----------------------------------------------------------------- configs 3, 5
@@ -1189,7 +1204,8 @@ def main():
                     help="launch the trial schedules directly instead of as CUDA graphs")
     ap.add_argument("--served", type=int, default=SERVED_REQUESTS,
                     help="requests of the served workload (0: skip)")
-    ap.add_argument("--served-policy", default="least_work", choices=["least_work", "even"],
+    ap.add_argument("--served-policy", default="least_work",
+                    choices=["least_work", "even", "exclusive"],
                     help="scheduling between running requests of the served workload")
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
                     help="2: the headline survey workload; 3 and 5: the other throughput "

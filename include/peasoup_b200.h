@@ -601,10 +601,14 @@ typedef struct {
                            PSX_SERVE_LEAST_WORK (0) -- the one with the least
                            work at the device's greatest stream priority;
                            PSX_SERVE_EVEN (1) -- no priority hint: running
-                           requests share the device evenly */
+                           requests share the device evenly;
+                           PSX_SERVE_EXCLUSIVE (2) -- one request on the
+                           device at a time (max_active is then the number
+                           of host threads only), admitted least work
+                           first, a request passed over 8 times next */
 } psx_server_config;
 
-enum { PSX_SERVE_LEAST_WORK = 0, PSX_SERVE_EVEN = 1 };
+enum { PSX_SERVE_LEAST_WORK = 0, PSX_SERVE_EVEN = 1, PSX_SERVE_EXCLUSIVE = 2 };
 
 typedef struct {
     double t_submit;    /* seconds on the server clock (psx_server_clock) */
@@ -634,7 +638,9 @@ double psx_server_clock(psx_server* srv);
    running at once the one with the least work (acceleration trials times
    transform length over its DM trials) runs at the higher stream priority
    (psx_search_set_priority); with PSX_SERVE_EVEN they share the device
-   without a hint.
+   without a hint.  With PSX_SERVE_EXCLUSIVE one request runs at a time,
+   to completion; the next is the pending one with the least work, unless
+   one has been passed over 8 times (the oldest of those then goes first).
    PSX_ERR_BUSY: queue full; PSX_ERR_ALLOC: larger than the whole budget. */
 int psx_server_submit(psx_server* srv, const psx_search_config* cfg,
                       const float* const* series, size_t nsamps,

@@ -35,6 +35,9 @@ PSX_OUT_DM_FOREST = 2
 PSX_DISTILL_HARMONIC = 0
 PSX_DISTILL_ACCEL = 1
 PSX_DISTILL_DM = 2
+PSX_SERVE_LEAST_WORK = 0
+PSX_SERVE_EVEN = 1
+PSX_SERVE_EXCLUSIVE = 2
 
 
 class PsxError(RuntimeError):

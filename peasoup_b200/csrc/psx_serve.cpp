@@ -19,7 +19,10 @@
 // trials times transform length, summed over its DM trials) runs at the
 // device's greatest stream priority: a short request admitted beside a long
 // one finishes close to its isolated time, and the long one loses only the
-// short one's work.
+// short one's work.  The exclusive policy runs one request at a time
+// instead (a batched search fills the device by itself, so sharing it adds
+// latency to every request it overlaps), choosing the pending request with
+// the least work, or one that has been passed over kMaxPassedOver times.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
@@ -44,6 +47,10 @@ void clear_error();
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// Exclusive policy: admissions that may go ahead of a pending request
+// before it is admitted regardless of its work (no starvation).
+constexpr int kMaxPassedOver = 8;
 
 struct EngineKey {
     size_t n;
@@ -85,6 +92,7 @@ struct Request {
     psx_request_stats st{};
     std::string error;
     bool done = false;
+    int passed_over = 0;  // exclusive policy: admissions that went ahead of it
 };
 
 }  // namespace
@@ -114,7 +122,8 @@ struct psx_server {
     long long admit_seq = 0;
     void reprioritise()  // under `mu`
     {
-        if (cfg.policy == PSX_SERVE_EVEN) return;  // every instance at the normal level
+        // every instance at the normal level (one runs at a time when exclusive)
+        if (cfg.policy != PSX_SERVE_LEAST_WORK) return;
         auto best = running.end();
         for (auto it = running.begin(); it != running.end(); ++it)
             if (best == running.end() || it->second.work < best->second.work) best = it;
@@ -136,13 +145,31 @@ int psx_server::admit_head(std::shared_ptr<Request>* req, Engine* eng,
                            std::vector<Engine>* evict)
 {
     if (pending.empty() || active >= cfg.max_active) return 0;
-    std::shared_ptr<Request> r = pending.front();
+    auto pick = pending.begin();
+    if (cfg.policy == PSX_SERVE_EXCLUSIVE) {
+        if (active > 0) return 0;  // one request on the device at a time
+        // the oldest request passed over too often, else the least work
+        // (the oldest on a tie)
+        auto starved = pending.end();
+        for (auto it = pending.begin(); it != pending.end(); ++it) {
+            if ((*it)->passed_over >= kMaxPassedOver && starved == pending.end()) starved = it;
+            if ((*it)->work < (*pick)->work) pick = it;
+        }
+        if (starved != pending.end()) pick = starved;
+    }
+    std::shared_ptr<Request> r = *pick;
+    // every pending request ahead of the pick in arrival order was passed
+    // over once more (counted when the pick is admitted)
+    auto admitted = [&]() {
+        for (auto it = pending.begin(); it != pick; ++it) ++(*it)->passed_over;
+        pending.erase(pick);
+    };
     const EngineKey k = key_of(r->cfg);
     for (auto it = idle.begin(); it != idle.end(); ++it) {
         if (it->key == k) {
             *eng = *it;
             idle.erase(it);
-            pending.pop_front();
+            admitted();
             *req = r;
             ++active;
             return 1;
@@ -157,7 +184,7 @@ int psx_server::admit_head(std::shared_ptr<Request>* req, Engine* eng,
     }
     if (used + need > cfg.hbm_budget) {
         if (active == 0) {  // can never fit: fail it rather than wait forever
-            pending.pop_front();
+            pending.erase(pick);
             r->st.status = PSX_ERR_ALLOC;
             r->error = "server: request needs " + std::to_string(need) + " bytes, budget is " +
                        std::to_string(cfg.hbm_budget);
@@ -172,7 +199,7 @@ int psx_server::admit_head(std::shared_ptr<Request>* req, Engine* eng,
     eng->s = nullptr;
     eng->key = k;
     eng->bytes = need;
-    pending.pop_front();
+    admitted();
     *req = r;
     ++active;
     return 1;
@@ -271,9 +298,10 @@ int psx_server_create(const psx_server_config* cfg, psx_server** out)
     psx::clear_error();
     if (!cfg || !out || cfg->max_active < 1 || cfg->max_active > 64 || cfg->max_queue < 1 ||
         cfg->hbm_budget == 0 ||
-        (cfg->policy != PSX_SERVE_LEAST_WORK && cfg->policy != PSX_SERVE_EVEN)) {
+        (cfg->policy != PSX_SERVE_LEAST_WORK && cfg->policy != PSX_SERVE_EVEN &&
+         cfg->policy != PSX_SERVE_EXCLUSIVE)) {
         psx::set_error("server_create: bad configuration (max_active 1..64, max_queue >= 1, "
-                       "hbm_budget > 0, policy 0 or 1)");
+                       "hbm_budget > 0, policy 0, 1 or 2)");
         return PSX_ERR_INVALID;
     }
     *out = nullptr;

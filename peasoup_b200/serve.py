@@ -22,21 +22,27 @@ from ._lib import RequestStats, ServerConfig, check, load
 from .search import CAND_DTYPE, SearchParams
 
 
+POLICIES = {"least_work": _lib.PSX_SERVE_LEAST_WORK, "even": _lib.PSX_SERVE_EVEN,
+            "exclusive": _lib.PSX_SERVE_EXCLUSIVE}
+
+
 class Server:
     """One served loop on the current CUDA device."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, max_queue: int = 4096,
                  device: Optional[int] = None, policy: str = "least_work"):
         """policy: "least_work" (the running request with the least work at
-        the device's greatest stream priority) or "even" (no hint)."""
+        the device's greatest stream priority), "even" (no hint) or
+        "exclusive" (one request on the device at a time, the pending one
+        with the least work next)."""
         if device is None:
             import torch
             device = torch.cuda.current_device()
-        if policy not in ("least_work", "even"):
-            raise ValueError("policy: least_work or even")
+        if policy not in POLICIES:
+            raise ValueError("policy: " + ", ".join(POLICIES))
         cfg = ServerConfig(device=int(device), hbm_budget=int(hbm_budget_bytes),
                            max_active=int(max_active), max_queue=int(max_queue),
-                           policy=0 if policy == "least_work" else 1)
+                           policy=POLICIES[policy])
         self._h = C.c_void_p()
         check(load().psx_server_create(C.byref(cfg), C.byref(self._h)), "server_create")
         self._keep = {}

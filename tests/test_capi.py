@@ -145,7 +145,7 @@ def test_server_needs_a_device(psx):
     assert psx.psx_server_create(C.byref(cfg), C.byref(h)) == PSX_ERR_CUDA
     bad = ServerConfig(device=0, hbm_budget=0, max_active=0, max_queue=0)
     assert psx.psx_server_create(C.byref(bad), C.byref(h)) == 1
-    bad_policy = ServerConfig(device=0, hbm_budget=1 << 30, max_active=2, max_queue=8, policy=2)
+    bad_policy = ServerConfig(device=0, hbm_budget=1 << 30, max_active=2, max_queue=8, policy=3)
     assert psx.psx_server_create(C.byref(bad_policy), C.byref(h)) == 1
     assert b"policy" in psx.psx_last_error()
 

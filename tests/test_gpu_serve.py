@@ -46,7 +46,7 @@ def _alone(M, p, xs, dms):
     return c, na, dm
 
 
-@pytest.mark.parametrize("policy", ["least_work", "even"])
+@pytest.mark.parametrize("policy", ["least_work", "even", "exclusive"])
 def test_mixed_equals_alone(M, policy):
     search, serve, synth = M
     import torch
@@ -61,6 +61,9 @@ def test_mixed_equals_alone(M, policy):
     st = srv.status()
     assert st["active"] == 0 and st["pending"] == 0 and st["pooled"] >= 1
     srv.close()
+    if policy == "exclusive":  # one request on the device at a time
+        spans = sorted((g[3]["t_admit"], g[3]["t_done"]) for g in got)
+        assert all(b[0] >= a[1] for a, b in zip(spans, spans[1:])), spans
     for (p, xs, dms), (c, na, dm, stats) in zip(reqs, got):
         assert stats["status"] == 0 and stats["ndm"] == len(dms) and stats["ntrials"] > 0
         assert stats["t_submit"] <= stats["t_admit"] <= stats["t_done"]
