@@ -386,7 +386,7 @@ def _served_series(r, seed):
     return x
 
 
-def run_served(nreq, rank, log_prefix, policy="least_work"):
+def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS):
     """The served workload (Poisson arrivals, uneven requests) through the
     C++ server, then every request alone on a one-slot server: latency
     from arrival and from admission, throughput, and the ratios to the
@@ -443,9 +443,10 @@ def run_served(nreq, rank, log_prefix, policy="least_work"):
         return res, arrivals
 
     # the requested policy, and the other scheduling of the same stream for
-    # comparison (exclusive with one slot, least work first with two)
+    # comparison (exclusive runs one request at a time; the sharing policies
+    # admit nslots at once)
     other = "least_work" if policy == "exclusive" else "exclusive"
-    slots = {p: 1 if p == "exclusive" else SERVED_SLOTS for p in (policy, other)}
+    slots = {p: 1 if p == "exclusive" else nslots for p in (policy, other)}
     runs = {p: one_pass(slots[p], True, p) for p in (policy, other)}
     alone, _ = one_pass(1, False)
     del series
@@ -960,7 +961,8 @@ def run_psx(args, ws, rank, local):
     torch.cuda.empty_cache()
     if rank == 0 and ws == 1 and args.served > 0:
         t0 = time.perf_counter()
-        served = run_served(args.served, rank, "served", args.served_policy)
+        served = run_served(args.served, rank, "served", args.served_policy,
+                            args.served_slots)
         log(f"[rank {rank}] served workload in {time.perf_counter() - t0:.1f}s")
     other_configs = None
     if rank == 0 and ws == 1 and not args.no_configs:
@@ -1204,7 +1206,9 @@ def main():
                     help="launch the trial schedules directly instead of as CUDA graphs")
     ap.add_argument("--served", type=int, default=SERVED_REQUESTS,
                     help="requests of the served workload (0: skip)")
-    ap.add_argument("--served-policy", default="least_work",
+    ap.add_argument("--served-slots", type=int, default=SERVED_SLOTS,
+                    help="served workload: requests admitted at once by the sharing policies")
+    ap.add_argument("--served-policy", default="exclusive",
                     choices=["least_work", "even", "exclusive"],
                     help="scheduling between running requests of the served workload")
     ap.add_argument("--config", type=int, default=2, choices=[2, 3, 5],

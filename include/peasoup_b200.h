@@ -603,9 +603,9 @@ typedef struct {
                            PSX_SERVE_EVEN (1) -- no priority hint: running
                            requests share the device evenly;
                            PSX_SERVE_EXCLUSIVE (2) -- one request on the
-                           device at a time (max_active is then the number
-                           of host threads only), admitted least work
-                           first, a request passed over 8 times next */
+                           device at a time (more worker threads only wait),
+                           admitted least work first, a request passed
+                           over 8 times next */
 } psx_server_config;
 
 enum { PSX_SERVE_LEAST_WORK = 0, PSX_SERVE_EVEN = 1, PSX_SERVE_EXCLUSIVE = 2 };

@@ -23,6 +23,9 @@
 // instead (a batched search fills the device by itself, so sharing it adds
 // latency to every request it overlaps), choosing the pending request with
 // the least work, or one that has been passed over kMaxPassedOver times.
+// (Building the next request's instance while the current one runs was
+// measured slower: the allocations and frees of the build stall the
+// running request.)
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
