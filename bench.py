@@ -388,9 +388,9 @@ def _served_series(r, seed):
 
 def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS):
     """The served workload (Poisson arrivals, uneven requests) through the
-    C++ server, then every request alone on a one-slot server: latency
-    from arrival and from admission, throughput, and the ratios to the
-    isolated runs."""
+    C++ server under two scheduling policies, and every request alone on a
+    one-slot server before and after them: latency from arrival and from
+    admission, throughput, and the ratios to the isolated runs."""
     import threading as th
     import torch
     from peasoup_b200 import serve
@@ -447,10 +447,18 @@ def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS)
     # admit nslots at once)
     other = "least_work" if policy == "exclusive" else "exclusive"
     slots = {p: 1 if p == "exclusive" else nslots for p in (policy, other)}
+    # isolated latencies: every request alone, before and after the served
+    # passes; each request's ratios use the faster of its two (the device's
+    # clock under the power cap drifts over a run)
+    alone0, _ = one_pass(1, False)
     runs = {p: one_pass(slots[p], True, p) for p in (policy, other)}
-    alone, _ = one_pass(1, False)
+    alone1, _ = one_pass(1, False)
+    alone = alone0 + alone1
     del series
-    iso = [1e3 * (s["t_done"] - s["t_admit"]) for s in alone]
+    iso0 = [1e3 * (s["t_done"] - s["t_admit"]) for s in alone0]
+    iso1 = [1e3 * (s["t_done"] - s["t_admit"]) for s in alone1]
+    iso = [min(a, b) for a, b in zip(iso0, iso1)]
+    iso_spread = _pct([max(a, b) / min(a, b) for a, b in zip(iso0, iso1)], 50)
 
     def summary(pol):
         mixed, arr = runs[pol]
@@ -473,7 +481,8 @@ def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS)
                                         "p99": _pct(lat_arr, 99)},
             "latency_from_admission_ms": {"p50": _pct(lat_adm, 50), "p95": _pct(lat_adm, 95),
                                           "p99": _pct(lat_adm, 99)},
-            "isolated_ms": {"p50": _pct(iso, 50), "p99": _pct(iso, 99)},
+            "isolated_ms": {"p50": _pct(iso, 50), "p99": _pct(iso, 99),
+                            "before_after_spread_p50": iso_spread},
             "p99_admitted_over_p99_isolated": _pct(lat_adm, 99) / _pct(iso, 99),
             "per_request_ratio_p99": _pct(ratio, 99),
             "per_request_ratio_p50": _pct(ratio, 50),
