@@ -575,8 +575,8 @@ int psx_search_debug_tap(psx_search* s, int trial, float* h_tim_dered,
                          float* h_tim_r, float* h_pspec, float* h_norm2);
 
 /* Reuses an instance for another request with the same transform length,
-   folds, mode, batch, harmonic shape, lanes, transform path and prologue
-   grouping rows (the things its buffers and plans depend on):
+   mode, batch, harmonic shape, lanes, transform path and prologue
+   grouping rows (the things its buffers and plans depend on): fold count,
    acceleration range, tsamp, thresholds,
    frequency limits and birdies may all change.  Waits for the instance's
    queued work first.  No counterpart in the reference (whose Worker builds

@@ -1961,12 +1961,12 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     }
     PSX_TRY(check_config(cfg));
     const int shape = cfg->harm_shape ? cfg->harm_shape : kHarmDefaultShape;
-    if (cfg->fft_size != s->N || cfg->nharmonics != s->F || cfg->mode != s->cfg.mode ||
+    if (cfg->fft_size != s->N || cfg->mode != s->cfg.mode ||
         effective_batch(cfg) != s->batch || shape != s->harm_shape ||
         effective_lanes(cfg) != s->lanes ||
         effective_form(cfg) != effective_form(&s->cfg) ||
         group_rows_for(cfg) != group_rows_for(&s->cfg)) {
-        set_error("search_retarget: fft_size, folds, mode, batch, harmonic shape, lanes, "
+        set_error("search_retarget: fft_size, mode, batch, harmonic shape, lanes, "
                   "transform path and prologue grouping must match the instance");
         return PSX_ERR_INVALID;
     }
@@ -1975,6 +1975,9 @@ int psx_search_retarget(psx_search* s, const psx_search_config* cfg)
     PSX_CUDA(cudaStreamSynchronize(s->st));
     PSX_CUDA(cudaStreamSynchronize(s->cst));
     for (Slot& sl : s->slot) PSX_CUDA(cudaStreamSynchronize(sl.pst));
+    // the fold count only selects the harmonic kernel's instantiation (no
+    // buffer depends on it): opt that one into its shared memory
+    PSX_TRY(configure_harm(cfg->nharmonics));
     host_setup(s, cfg);
     if (s->bf.size() > s->bird_cap) {
         cudaFree(s->d_bf);

@@ -10,7 +10,8 @@
 // by device memory: a request is admitted when a worker slot is free and
 // the bytes it needs fit the budget.  Instances outlive their requests in a
 // pool keyed by what their buffers and plans depend on (transform length,
-// folds, mode, batch, harmonic shape); a later request with the same key is
+// mode, batch, harmonic shape; not the fold count, which only selects the
+// harmonic kernel at launch); a later request with the same key is
 // retargeted onto a pooled instance (psx_search_retarget) instead of
 // allocating, and idle pooled instances are destroyed, oldest first, when a
 // new one needs their memory.
@@ -57,10 +58,10 @@ constexpr int kMaxPassedOver = 8;
 
 struct EngineKey {
     size_t n;
-    int folds, mode, batch, shape, callback, lanes, form, group;
+    int mode, batch, shape, callback, lanes, form, group;
     bool operator==(const EngineKey& o) const
     {
-        return n == o.n && folds == o.folds && mode == o.mode && batch == o.batch &&
+        return n == o.n && mode == o.mode && batch == o.batch &&
                shape == o.shape && callback == o.callback && lanes == o.lanes &&
                form == o.form && group == o.group;
     }
@@ -68,7 +69,7 @@ struct EngineKey {
 
 EngineKey key_of(const psx_search_config& c)
 {
-    return {c.fft_size, c.nharmonics, c.mode, c.batch, c.harm_shape,
+    return {c.fft_size, c.mode, c.batch, c.harm_shape,
             c.mode == PSX_MODE_BATCHED && c.use_fft_callback ? 1 : 0, c.lanes, c.fft_form,
             c.group_dms};
 }

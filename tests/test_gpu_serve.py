@@ -74,13 +74,14 @@ def test_mixed_equals_alone(M, policy):
 
 def test_pooled_instance_is_retargeted(M):
     """Two requests with the same instance shape but different acceleration
-    ranges, tsamp-derived limits and birdies: the second reuses the pooled
-    instance and must still equal a fresh instance's result."""
+    ranges, fold counts, tsamp-derived limits and birdies: the second reuses
+    the pooled instance and must still equal a fresh instance's result."""
     search, serve, synth = M
     import dataclasses
     reqs = _requests(M)
     p, xs, dms = reqs[0]
     p2 = dataclasses.replace(p, acc_lo=-75.0, acc_hi=60.0, min_snr=5.5, max_freq=900.0,
+                             nharmonics=3 if p.nharmonics != 3 else 5,
                              birdie_freqs=np.array([50.0, 120.0], np.float32),
                              birdie_widths=np.array([0.3, 0.5], np.float32))
     srv = serve.Server(40 << 30, max_active=1)
