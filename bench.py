@@ -417,7 +417,7 @@ def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS)
             for t in tk:
                 srv.wait(t)
 
-    def one_pass(max_active, paced, pol=policy):
+    def one_pass(max_active, paced, pol=policy, burst=False):
         srv = serve.Server(SERVED_BUDGET, max_active=max_active, policy=pol)
         warm(srv, max_active)
         res = [None] * len(reqs)
@@ -439,11 +439,13 @@ def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS)
             else:
                 x = _served_series(r, 1000 + i)
                 torch.cuda.current_stream().synchronize()   # this stream only
-            if paced:
+            if paced and not burst:
                 delay = t_start + r.arrival - srv.clock()
                 if delay > 0:
                     time.sleep(delay)
                 arrivals.append(t_start + r.arrival)
+            elif paced:  # every request at once: the schedule's capacity
+                arrivals.append(srv.clock())
             tickets[i] = srv.submit(params[i], x, np.arange(r.ndm, dtype=np.float32) * 0.5)
             if not paced:
                 arrivals.append(srv.clock())
@@ -467,6 +469,8 @@ def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS)
     # clock under the power cap drifts over a run)
     alone0, _ = one_pass(1, False)
     runs = {p: one_pass(slots[p], True, p) for p in (policy, other)}
+    # capacity under the requested policy: the same requests all at once
+    burst, _ = one_pass(slots[policy], True, policy, burst=True)
     alone1, _ = one_pass(1, False)
     alone = alone0 + alone1
     del series
@@ -525,6 +529,15 @@ def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS)
         }
     out = summary(policy)
     out["compared_policy"] = summary(other)
+    burst_span = max(s["t_done"] for s in burst) - min(s["t_submit"] for s in burst)
+    burst_tps = sum(s["ntrials"] for s in burst) / burst_span
+    out["burst"] = {
+        "what": "the same requests submitted at once under the requested policy: the "
+                "served loop's capacity",
+        "trials_per_s": burst_tps,
+        "over_isolated_back_to_back": burst_tps / (out["trials"] / (sum(iso) / 1e3)),
+        "failed": sum(1 for s in burst if s["status"] != 0),
+    }
     return out
 
 
