@@ -1113,11 +1113,16 @@ def run_dedisp(args, ws, rank, local):
         build()
     barrier(ws)
     L = _lib.load()
-    n, nchans, nbits, ndm = N_FFT, DD_NCHANS, DD_NBITS, NDM
+    n = args.case_nsamps or N_FFT
+    nchans = args.dd_nchans or DD_NCHANS
+    nbits = args.dd_nbits or DD_NBITS
+    ndm = args.ndm or NDM
     dms = (0.5 * np.arange(ndm)).astype(np.float32)
     plan = C.c_void_p()
-    _lib.check(L.psx_dedisp_create(nchans, TSAMP, synth.FCH1_MHZ, synth.FOFF_MHZ,
-                                   C.byref(plan)), "dedisp_create")
+    # the 64-channel band (1510 MHz down by 64 x 1.09 MHz) split into nchans
+    foff = synth.FOFF_MHZ * DD_NCHANS / nchans
+    _lib.check(L.psx_dedisp_create(nchans, TSAMP, synth.FCH1_MHZ, foff, C.byref(plan)),
+               "dedisp_create")
     _lib.check(L.psx_dedisp_set_dm_list(plan, dms.ctypes.data, ndm), "set_dm_list")
     md = int(L.psx_dedisp_get_max_delay(plan))
     nout = n - md
@@ -1161,11 +1166,11 @@ def run_dedisp(args, ws, rank, local):
     with ClockSampler(local) as clk:
         t_dev = timed(step_dev, args.steps, args.warmup)
     clocks = clk.summary()
-    t_e2e = timed(step_host, max(2, args.steps // 2), 2)
     k_e2e = max(2, args.steps // 2)
+    t_e2e = None if args.no_e2e else timed(step_host, k_e2e, 2)
     per = ndm * nout
     value = ws * per * args.steps / t_dev
-    e2e = ws * per * k_e2e / t_e2e
+    e2e = ws * per * k_e2e / t_e2e if t_e2e else None
     ms = t_dev / args.steps * 1e3
     alg = n * nchans * nbits / 8 + 2.0 * n * nchans + 4.0 * per
     peak, kind = peaks()
@@ -1179,7 +1184,7 @@ def run_dedisp(args, ws, rank, local):
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
         from oracle import oracle as O
-        delays = O.delay_table(nchans, TSAMP, synth.FCH1_MHZ, synth.FOFF_MHZ)
+        delays = O.delay_table(nchans, TSAMP, synth.FCH1_MHZ, foff)
         ns = (1 << 18) + md
         sample = rows[:ns].cpu().numpy()
         cores = _cpu_workers()
@@ -1197,17 +1202,22 @@ def run_dedisp(args, ws, rank, local):
     L.psx_dedisp_destroy(plan)
     if rank == 0:
         print(json.dumps({
-            "metric": "dedispersed samples/s (256 DM x 2^23, 64 ch, 8-bit)",
+            "metric": f"dedispersed samples/s ({ndm} DM x 2^{n.bit_length() - 1}, {nchans} ch, "
+                      f"{nbits}-bit)",
             "value": value, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8->u32 sums->f32",
             "data": "synthetic (uniform random 8-bit rows, seeded)",
-            "config": {"workload": "dedisperse 2^23 x 64-channel 8-bit rows (tsamp 76 us, "
-                                   "1510 MHz, -1.09 MHz) to 256 DM trials DM_i = 0.5 i",
+            "config": {"workload": f"dedisperse {n} samples x {nchans}-channel {nbits}-bit rows "
+                                   f"(tsamp 76 us, 1510 MHz, {foff:.4g} MHz) to {ndm} DM "
+                                   f"trials DM_i = 0.5 i",
                        "rows_mb": n * nchans / 1e6, "output_gb": 4.0 * per / 1e9,
-                       "max_delay": md, "l2": "input 537 MB and output exceed L2"},
-            "e2e": {"value": e2e, "unit": "samples/s",
-                    "h2d_bytes_per_step": n * nchans * nbits // 8, "d2h_bytes_per_step": 16384},
+                       "max_delay": md,
+                       "l2": f"input {n * nchans * nbits / 8e6:.0f} MB, output "
+                             f"{4.0 * per / 1e9:.2f} GB"},
+            "e2e": None if e2e is None else {
+                "value": e2e, "unit": "samples/s",
+                "h2d_bytes_per_step": n * nchans * nbits // 8, "d2h_bytes_per_step": 16384},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "note": f"unpack + dedisperse per launch pair, {alg / 1e9:.2f} GB "
@@ -1232,6 +1242,10 @@ def main():
                     help="trials per launch group (0: autotuned together with the shape)")
     ap.add_argument("--harm-shape", type=int, default=0,
                     help="with --batch: harmonic-kernel shape (0: the default shape)")
+    ap.add_argument("--dd-nchans", type=int, default=0,
+                    help="--workload dedisp: channels (default 64)")
+    ap.add_argument("--dd-nbits", type=int, default=0,
+                    help="--workload dedisp: bits per sample (default 8)")
     ap.add_argument("--group-dms", type=int, default=0,
                     help="DM trials per grouped prologue (0: default rule, 1: off)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -1259,11 +1273,12 @@ def main():
                     help="2: the headline survey workload; 3 and 5: the other throughput "
                          "configurations (one JSON line each)")
     ap.add_argument("--case-nsamps", type=int, default=0,
-                    help="--workload case: transform length (default 2^23)")
+                    help="--workload case / dedisp: samples (default 2^23)")
     ap.add_argument("--case-acc", type=float, default=0.0,
                     help="--workload case: acceleration half-range (default 100 m/s^2)")
     ap.add_argument("--ndm", type=int, default=0,
-                    help="configs 3/5: DM trials to time; --workload case: DM trials searched")
+                    help="configs 3/5: DM trials to time; --workload case: DM trials "
+                         "searched; --workload dedisp: DM trials (default 256)")
     ap.add_argument("--plain-sample", type=int, default=128,
                     help="config 3: DM trials searched by the plain path")
     ap.add_argument("--workload", default="search", choices=["search", "dedisp", "case"],
