@@ -709,6 +709,7 @@ struct psx_search {
     int prep(Slot& s, const float* series, size_t nsamps, bool on_device, float dm, int dm_idx);
     int enqueue_trials(Slot& s);
     int alloc_groups();
+    int alloc_groups_sets();
     void free_groups();
     int group_rows_for_call(const float* dms, int ndm) const;
     int trials_enqueue(Slot& s, int nacc);
@@ -926,6 +927,13 @@ int psx_search::prologue(Slot& s)
 int psx_search::alloc_groups()
 {
     if (!gset[0].slots.empty()) return PSX_OK;
+    const int rc = alloc_groups_sets();
+    if (rc != PSX_OK) free_groups();  // nothing half-made stays for the next call
+    return rc;
+}
+
+int psx_search::alloc_groups_sets()
+{
     const int G = group_rows_for(&cfg);
     if (G < 2) return PSX_OK;
     const size_t nb = (size_t)reduction_blocks();
