@@ -125,3 +125,42 @@ def test_admission_limits(M):
         first = c if first is None else first
         assert np.array_equal(c, first)
     srv.close()
+
+
+def test_exclusive_order_and_no_starvation(M):
+    """PSX_SERVE_EXCLUSIVE admits the pending request with the least work,
+    but a request passed over 8 times goes next: behind a running blocker,
+    a long request L and ten short ones queue; the short ones go first
+    until L has been passed over 8 times, then L, then the last two."""
+    search, serve, synth = M
+    ts = 64e-6
+
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(5)
+
+    def req(n, ndm, acc):  # white noise on the device
+        xs = torch.randn((ndm, n), device="cuda", generator=g)
+        p = search.SearchParams(fft_size=n, tsamp=ts, acc_lo=-acc, acc_hi=acc, nharmonics=3,
+                                min_snr=8.0, cfreq_hz=synth.CFREQ_HZ, ch_bw_hz=synth.CH_BW_HZ)
+        return p, xs, (0.5 * np.arange(ndm)).astype(np.float32)
+
+    blocker = req(1 << 22, 48, 300.0)
+    long_ = req(1 << 18, 16, 200.0)
+    shorts = [req(1 << 16, 2, 20.0) for _ in range(10)]
+    torch.cuda.synchronize()
+    srv = serve.Server(40 << 30, max_active=2, policy="exclusive")
+    tb = srv.submit(*blocker)
+    tl = srv.submit(*long_)
+    ts_ = [srv.submit(*r) for r in shorts]
+    sb = srv.wait(tb)[3]
+    sl = srv.wait(tl)[3]
+    ss = [srv.wait(t)[3] for t in ts_]
+    srv.close()
+    assert all(s["status"] == 0 for s in [sb, sl] + ss)
+    # the queue formed while the blocker ran
+    assert sl["t_submit"] < sb["t_done"] and max(s["t_submit"] for s in ss) < sb["t_done"]
+    order = sorted([("L", sl["t_admit"])] + [("S", s["t_admit"]) for s in ss],
+                   key=lambda x: x[1])
+    assert [o[0] for o in order] == ["S"] * 8 + ["L"] + ["S"] * 2, order
+    spans = sorted((s["t_admit"], s["t_done"]) for s in [sb, sl] + ss)
+    assert all(b[0] >= a[1] for a, b in zip(spans, spans[1:]))
