@@ -212,3 +212,33 @@ def test_config1_plain_and_production_vs_oracle_and_reference(S, oracle, ref_gpu
         assert nm == len(rc) and worst < SNR_RTOL
         best = trials[np.argmax(trials["snr"])]
         assert abs(best["freq"] / f0 - 1) < 1e-4 and best["acc"] == 0.0, best
+
+
+def test_config1_block_grouped_vs_reference(S, ref_gpu):
+    """Config 1's statistics over 10 DM trials in one block call: with about
+    3 acceleration trials per DM trial the engine groups the prologues by 4
+    (batched cuFFT plans, row-indexed prologue kernels); its per-DM lists
+    against the reference's Worker over the same 10 series, and bit for bit
+    against the same block without grouping."""
+    search, synth = S
+    n, ts, ndm = 1 << 20, 64e-6, 10
+    xs = np.stack([synth.config1_series(d) for d in range(ndm)])
+    dms = (0.5 * np.arange(ndm)).astype(np.float32)
+    kw = dict(acc_lo=-50.0, acc_hi=50.0, nharmonics=4, min_snr=7.0)
+    rc, _ = ref_gpu.ref_worker_search(xs, ts, dms, n, _oracle_params(ref_gpu, synth, n, ts, **kw),
+                                      "")
+    outs = []
+    for group in (0, 1):
+        s = search.AccelSearch(search.SearchParams(fft_size=n, tsamp=ts, cfreq_hz=synth.CFREQ_HZ,
+                                                   ch_bw_hz=synth.CH_BW_HZ, batch=96,
+                                                   harm_shape=6, group_dms=group, **kw))
+        c, na, tr, dm = s.search_block(xs, dms, per_dm=True)
+        info = s.info()
+        s.close()
+        assert info["group_dms"] == (4 if group == 0 else 0)
+        outs.append((c, na, dm))
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    nm, _, worst = flip_report(outs[0][0], rc, 7.0, FLIP_MARGIN_REF,
+                               "config 1 block, grouped prologues, vs reference")
+    assert nm == len(rc) and nm >= ndm and worst < SNR_RTOL
