@@ -55,11 +55,15 @@ def _equal(a, b):
         assert np.array_equal(x, y)
 
 
-@pytest.mark.parametrize("n,nsamps", [(1 << 20, 1 << 20), (1 << 20, 900_000), (3 << 18, 3 << 18)])
-def test_grouped_equals_per_dm(S, n, nsamps):
+@pytest.mark.parametrize("n,nsamps,lanes", [(1 << 20, 1 << 20, 1), (1 << 20, 900_000, 1),
+                                            (3 << 18, 3 << 18, 1), (1 << 20, 1 << 20, 2),
+                                            (1 << 17, 1 << 17, 1)])
+def test_grouped_equals_per_dm(S, n, nsamps, lanes):
+    """(2^17 points: the trials on cuFFT's complex transform; lanes 2: launch
+    groups alternate over two streams.)"""
     ts = 64e-6
     xs, dms = _block(S, n, ts, nsamps, 11, 40)
-    kw = dict(acc_lo=-20.0, acc_hi=20.0, nharmonics=4, min_snr=7.0, batch=8,
+    kw = dict(acc_lo=-20.0, acc_hi=20.0, nharmonics=4, min_snr=7.0, batch=8, lanes=lanes,
               birdie_freqs=np.array([50.0, 123.4], np.float32),
               birdie_widths=np.array([0.5, 1.0], np.float32))
     ref, info0, tap0 = _run(S, n, ts, xs, dms, 1, **kw)
