@@ -1177,9 +1177,22 @@ int psx_search::trials_range(Slot& s, int t_begin, int nacc, bool reset)
         PSX_TRY(launch_status("form kernel"));
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 2], ls));
         if (span) {
-            PSX_TRY(launch_harm(F, harm_shape, pp, Bp, (unsigned)Bp, pk, t0, b, s.d_rec,
-                                s.d_count, (unsigned)s.rec_cap, ls, &hmaps[lane]));
-            ++s.launches;
+            // A multi-row shape stages `rows` trials per tile; the group's
+            // last b % rows trials go to the single-row default shape
+            // instead of a tile padded with unused rows (every shape gives
+            // the same records).
+            const int rows = kHarmShapes[harm_shape - 1].rows;
+            const int rem = rows > 1 ? b % rows : 0, bm = b - rem;
+            if (bm > 0) {
+                PSX_TRY(launch_harm(F, harm_shape, pp, Bp, (unsigned)Bp, pk, t0, bm, s.d_rec,
+                                    s.d_count, (unsigned)s.rec_cap, ls, &hmaps[lane]));
+                ++s.launches;
+            }
+            if (rem > 0) {
+                PSX_TRY(launch_harm(F, kHarmDefaultShape, pp + (size_t)bm * Bp, Bp, (unsigned)Bp,
+                                    pk, t0 + bm, rem, s.d_rec, s.d_count, (unsigned)s.rec_cap, ls));
+                ++s.launches;
+            }
         }
         if (s.profiled) PSX_CUDA(cudaEventRecord(s.ev[3 + 4 * g + 3], ls));
         t0 += b;
