@@ -30,11 +30,12 @@ class Server:
     """One served loop on the current CUDA device."""
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, max_queue: int = 4096,
-                 device: Optional[int] = None, policy: str = "least_work"):
-        """policy: "least_work" (the running request with the least work at
-        the device's greatest stream priority), "even" (no hint) or
-        "exclusive" (one request on the device at a time, the pending one
-        with the least work next)."""
+                 device: Optional[int] = None, policy: str = "exclusive"):
+        """policy: "exclusive" (one request on the device at a time, the
+        pending one with the least work next; measured best on the served
+        workload), "least_work" (up to max_active requests at once, the one
+        with the least work at the device's greatest stream priority) or
+        "even" (up to max_active at once, no hint)."""
         if device is None:
             import torch
             device = torch.cuda.current_device()
