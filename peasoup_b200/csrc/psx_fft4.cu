@@ -176,9 +176,12 @@ template <int R, bool DUMP>
 __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THREADS)
     k_fft4_cols(const float* __restrict__ x, unsigned long long n, const double* __restrict__ ktab,
                 const float2* __restrict__ tab, unsigned offA2, unsigned offA3, unsigned offQ,
-                unsigned offP, unsigned C, float2* __restrict__ y, size_t ypitch)
+                unsigned offP, unsigned C, float2* __restrict__ y, size_t ypitch,
+                const unsigned* __restrict__ trow, size_t xpitch)
 {
     using S = ColShape<R>;
+    // trials of several series (trow: trial -> row of x, rows xpitch apart)
+    if (trow) x += (size_t)trow[blockIdx.y] * xpitch;
     static_assert(R == 768 || R == 1024 || R == 2048 || R == 4096, "column length");
     static_assert((S::THREADS == 512 || S::THREADS == 1024) && S::U * S::R3 <= 16,
                   "column shape");
@@ -380,9 +383,11 @@ __global__ void __launch_bounds__(256)
     k_unpack_form_norm_t(const float2* __restrict__ zt, size_t zpitch, unsigned C,
                          float* __restrict__ p, size_t ppitch,
                          const float2* __restrict__ rv, const float2* __restrict__ rk,
-                         const float* __restrict__ stat)
+                         const float* __restrict__ stat, const unsigned* __restrict__ trow)
 {
     __shared__ float2 lo_t[32][33], mi_t[32][33];
+    // trials of several series: trial blockIdx.y's statistics at row trow[]
+    if (trow) stat += 8u * trow[blockIdx.y];
     const unsigned M = R * C;
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned gblocks = C / 64;
@@ -500,13 +505,14 @@ int configure_cols()
 
 template <int R, bool DUMP>
 void Fft4Plan::launch_cols(const Fft4Plan& f, const float* series, const double* ktab,
-                           int ntrials, float2* y, size_t ypitch, cudaStream_t s)
+                           int ntrials, float2* y, size_t ypitch, cudaStream_t s,
+                           const unsigned* trow, size_t xpitch)
 {
     using S = ColShape<R>;
     dim3 ga(f.C / S::W, (unsigned)ntrials);
     k_fft4_cols<R, DUMP><<<ga, S::THREADS, DUMP ? 0 : S::SMEM, s>>>(
         series, (unsigned long long)f.n, ktab, f.d_tab, f.offA2, f.offA3, f.offQ, f.offP, f.C, y,
-        ypitch);
+        ypitch, trow, xpitch);
 }
 
 bool Fft4Plan::supported(size_t n)
@@ -632,22 +638,26 @@ int Fft4Plan::create(size_t n_)
 int Fft4Plan::exec(const float* series, const double* ktab, int ntrials, float2* y,
                    size_t ypitch, float2* zt, size_t zpitch, cudaStream_t s) const
 {
-    PSX_TRY(exec_cols(series, ktab, ntrials, y, ypitch, s));
+    PSX_TRY(exec_cols(series, ktab, ntrials, y, ypitch, s, nullptr, 0));
     return exec_rows(y, ypitch, ntrials, zt, zpitch, s);
 }
 
 int Fft4Plan::exec_cols(const float* series, const double* ktab, int ntrials, float2* y,
-                        size_t ypitch, cudaStream_t s) const
+                        size_t ypitch, cudaStream_t s, const unsigned* trow,
+                        size_t xpitch) const
 {
-    if (!d_tab || !series || !ktab || !y || ntrials <= 0 || ntrials > 65535 || ypitch < n / 2) {
+    if (!d_tab || !series || !ktab || !y || ntrials <= 0 || ntrials > 65535 || ypitch < n / 2 ||
+        (trow && xpitch < n)) {
         set_error("fft4: bad arguments");
         return PSX_ERR_INVALID;
     }
+    const unsigned* tr = trow;
+    const size_t xp = xpitch;
     switch (R) {
-    case 768: launch_cols<768, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
-    case 1024: launch_cols<1024, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
-    case 2048: launch_cols<2048, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
-    default: launch_cols<4096, false>(*this, series, ktab, ntrials, y, ypitch, s); break;
+    case 768: launch_cols<768, false>(*this, series, ktab, ntrials, y, ypitch, s, tr, xp); break;
+    case 1024: launch_cols<1024, false>(*this, series, ktab, ntrials, y, ypitch, s, tr, xp); break;
+    case 2048: launch_cols<2048, false>(*this, series, ktab, ntrials, y, ypitch, s, tr, xp); break;
+    default: launch_cols<4096, false>(*this, series, ktab, ntrials, y, ypitch, s, tr, xp); break;
     }
     return launch_status("fft4 column pass");
 }
@@ -661,10 +671,10 @@ int Fft4Plan::dump_gather(const float* series, const double* ktab, float* out,
     }
     float2* o = reinterpret_cast<float2*>(out);
     switch (R) {
-    case 768: launch_cols<768, true>(*this, series, ktab, 1, o, n / 2, s); break;
-    case 1024: launch_cols<1024, true>(*this, series, ktab, 1, o, n / 2, s); break;
-    case 2048: launch_cols<2048, true>(*this, series, ktab, 1, o, n / 2, s); break;
-    default: launch_cols<4096, true>(*this, series, ktab, 1, o, n / 2, s); break;
+    case 768: launch_cols<768, true>(*this, series, ktab, 1, o, n / 2, s, nullptr, 0); break;
+    case 1024: launch_cols<1024, true>(*this, series, ktab, 1, o, n / 2, s, nullptr, 0); break;
+    case 2048: launch_cols<2048, true>(*this, series, ktab, 1, o, n / 2, s, nullptr, 0); break;
+    default: launch_cols<4096, true>(*this, series, ktab, 1, o, n / 2, s, nullptr, 0); break;
     }
     return launch_status("fft4 gather dump");
 }
@@ -693,7 +703,7 @@ int Fft4Plan::exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt,
 }
 
 int Fft4Plan::form(const float2* zt, size_t zpitch, int ntrials, float* p, size_t ppitch,
-                   const float* stat, cudaStream_t s) const
+                   const float* stat, cudaStream_t s, const unsigned* trow) const
 {
     if (!d_tab || !zt || !p || !stat || ntrials <= 0 || ntrials > 65535 || zpitch < n / 2 ||
         ppitch < n / 2 + 1) {
@@ -705,10 +715,10 @@ int Fft4Plan::form(const float2* zt, size_t zpitch, int ntrials, float* p, size_
     const float2* rv = d_tab + offRv;
     const float2* rk = d_tab + offRk;
     switch (R) {
-    case 768: k_unpack_form_norm_t<768><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
-    case 1024: k_unpack_form_norm_t<1024><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
-    case 2048: k_unpack_form_norm_t<2048><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
-    default: k_unpack_form_norm_t<4096><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat); break;
+    case 768: k_unpack_form_norm_t<768><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat, trow); break;
+    case 1024: k_unpack_form_norm_t<1024><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat, trow); break;
+    case 2048: k_unpack_form_norm_t<2048><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat, trow); break;
+    default: k_unpack_form_norm_t<4096><<<grid, 256, 0, s>>>(zt, zpitch, C, p, ppitch, rv, rk, stat, trow); break;
     }
     return launch_status("fft4 unpack kernel");
 }

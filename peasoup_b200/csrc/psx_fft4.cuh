@@ -40,8 +40,11 @@ struct Fft4Plan {
              float2* zt, size_t zpitch, cudaStream_t s) const;
     // The two passes of exec on their own (pass 1: gather + column
     // transforms into y; pass 2: row transforms of y into zt).
+    // trow (optional): trial t gathers series + trow[t] * xpitch instead
+    // (trials of several series in one launch)
     int exec_cols(const float* series, const double* ktab, int ntrials, float2* y,
-                  size_t ypitch, cudaStream_t s) const;
+                  size_t ypitch, cudaStream_t s, const unsigned* trow = nullptr,
+                  size_t xpitch = 0) const;
     int exec_rows(const float2* y, size_t ypitch, int ntrials, float2* zt, size_t zpitch,
                   cudaStream_t s) const;
     // The N samples pass 1 gathers for one trial (ktab[0]), written to out
@@ -51,13 +54,15 @@ struct Fft4Plan {
     // Real spectrum bins 0..M of each trial from zt, interbinned and
     // normalised with stat[3] (mean*N) and stat[4] (std*N), written at
     // p + t * ppitch.
+    // trow (optional): trial t's statistics at stat + 8 * trow[t]
     int form(const float2* zt, size_t zpitch, int ntrials, float* p, size_t ppitch,
-             const float* stat, cudaStream_t s) const;
+             const float* stat, cudaStream_t s, const unsigned* trow = nullptr) const;
 
 private:
     template <int R, bool DUMP>
     static void launch_cols(const Fft4Plan& f, const float* series, const double* ktab,
-                            int ntrials, float2* y, size_t ypitch, cudaStream_t s);
+                            int ntrials, float2* y, size_t ypitch, cudaStream_t s,
+                            const unsigned* trow, size_t xpitch);
 };
 
 }  // namespace psx

@@ -536,6 +536,23 @@ struct GroupSet {
     unsigned* count = nullptr;  // G x 16 counters and flags
     float* mean = nullptr;    // G x 2
     FftPlan r2c, c2r;         // batch-G plans over the rows
+    // Trial schedule spanning the chunk's DM trials (two-pass transform):
+    // the trials of all its DM trials in one list (DM trial i's at
+    // [off[i], off[i+1])), each with its factor and its series row, and one
+    // record buffer for the chunk.
+    int4* d_rec = nullptr;
+    int4* h_rec = nullptr;
+    size_t rec_cap = 0;
+    unsigned* d_cnt = nullptr;  // [0] hits, [1] staging error
+    unsigned* h_cnt = nullptr;  // d_cnt's two words, then the rows' 16 counters each
+    double* d_ktab = nullptr;
+    double* h_ktab = nullptr;
+    unsigned* d_trow = nullptr;
+    unsigned* h_trow = nullptr;
+    size_t tab_cap = 0;
+    cudaEvent_t done = nullptr;
+    std::vector<int> off;
+    int groups = 0, launches = 0;
 };
 
 struct GraphEntry {
@@ -711,6 +728,12 @@ struct psx_search {
     int alloc_groups();
     int alloc_groups_sets();
     void free_groups();
+    // launch groups spanning a chunk's DM trials: the two-pass path with one
+    // lane and no stage profiling (which times each DM trial's groups)
+    bool span_mode() const { return use_f4 && lanes == 1 && !profile; }
+    int grow_span_records(GroupSet& g, size_t need);
+    int grow_span_tables(GroupSet& g, size_t need);
+    int trials_span(GroupSet& g, int cnt);
     int group_rows_for_call(const float* dms, int ndm) const;
     int trials_enqueue(Slot& s, int nacc);
     int trials_range(Slot& s, int t_begin, int t_end, bool reset);
@@ -726,6 +749,7 @@ struct psx_search {
         int dm_idx = 0;
     };
     int finish(Slot& s, DmRecords& job);
+    int finish_span(GroupSet& g, int cnt, std::vector<DmRecords>& jobs);
     void collect(const DmRecords& job, int output, std::vector<psx_candidate>& out,
                  std::vector<int>& nassoc, std::vector<int>& trial_of);
     void read_profile(Slot& s);
@@ -919,6 +943,169 @@ int psx_search::prologue(Slot& s)
     return PSX_OK;
 }
 
+int psx_search::grow_span_records(GroupSet& g, size_t need)
+{
+    if (need <= g.rec_cap) return PSX_OK;
+    const size_t cap = round_up(need + need / 4, 4096);
+    PSX_CUDA(cudaStreamSynchronize(st));
+    PSX_CUDA(cudaStreamSynchronize(cst));
+    if (g.d_rec) cudaFree(g.d_rec);
+    if (g.h_rec) cudaFreeHost(g.h_rec);
+    g.d_rec = g.h_rec = nullptr;
+    g.rec_cap = 0;
+    PSX_CUDA(cudaMalloc(&g.d_rec, sizeof(int4) * cap));
+    PSX_CUDA(cudaMallocHost(&g.h_rec, sizeof(int4) * cap));
+    g.rec_cap = cap;
+    return PSX_OK;
+}
+
+int psx_search::grow_span_tables(GroupSet& g, size_t need)
+{
+    if (need <= g.tab_cap) return PSX_OK;
+    const size_t cap = round_up(need + need / 4, 256);
+    PSX_CUDA(cudaStreamSynchronize(st));
+    for (void* q : {(void*)g.d_ktab, (void*)g.d_trow})
+        if (q) cudaFree(q);
+    for (void* q : {(void*)g.h_ktab, (void*)g.h_trow})
+        if (q) cudaFreeHost(q);
+    g.d_ktab = g.h_ktab = nullptr;
+    g.d_trow = g.h_trow = nullptr;
+    g.tab_cap = 0;
+    PSX_CUDA(cudaMalloc((void**)&g.d_ktab, sizeof(double) * cap));
+    PSX_CUDA(cudaMalloc((void**)&g.d_trow, sizeof(unsigned) * cap));
+    PSX_CUDA(cudaMallocHost(&g.h_ktab, sizeof(double) * cap));
+    PSX_CUDA(cudaMallocHost(&g.h_trow, sizeof(unsigned) * cap));
+    g.tab_cap = cap;
+    return PSX_OK;
+}
+
+// The trials of a chunk's cnt DM trials (prologues queued, factors in the
+// slots) as one list in launch groups of `batch` that run across DM-trial
+// boundaries: pass 1 gathers each trial from its own series row, the unpack
+// normalises it with its own row's statistics, and the harmonic kernel's
+// records carry the trial's index in the list.  On the compute stream;
+// records g.done and every slot's done.
+int psx_search::trials_span(GroupSet& g, int cnt)
+{
+    const int T = g.off[cnt];
+    for (int i = 0; i < cnt; ++i) {
+        Slot& sl = g.slots[i];
+        PSX_CUDA(cudaStreamWaitEvent(st, sl.ready, 0));
+        // each slot keeps its own factors too (the debug tap reads them)
+        PSX_CUDA(cudaMemcpyAsync(sl.d_ktab, sl.h_ktab, sizeof(double) * sl.accs.size(),
+                                 cudaMemcpyHostToDevice, st));
+    }
+    PSX_CUDA(cudaMemcpyAsync(g.d_ktab, g.h_ktab, sizeof(double) * T, cudaMemcpyHostToDevice, st));
+    PSX_CUDA(cudaMemcpyAsync(g.d_trow, g.h_trow, sizeof(unsigned) * T, cudaMemcpyHostToDevice, st));
+    PSX_CUDA(cudaMemsetAsync(g.d_cnt, 0, sizeof(unsigned) * 2, st));
+    const bool span = pk.hi > pk.lo;
+    float* tr = d_trl[0];
+    float* X = d_Xl[0];
+    float* pp = d_pl[0];
+    g.groups = 0;
+    g.launches = 0;
+    for (int t0 = 0; t0 < T;) {
+        const int b = std::min(batch, T - t0);
+        PSX_TRY(f4.exec_cols(g.tim, g.d_ktab + t0, b, reinterpret_cast<float2*>(tr), N / 2, st,
+                             g.d_trow + t0, N));
+        PSX_TRY(f4.exec_rows(reinterpret_cast<const float2*>(tr), N / 2, b,
+                             reinterpret_cast<float2*>(X), Bp, st));
+        PSX_TRY(f4.form(reinterpret_cast<const float2*>(X), Bp, b, pp, Bp, g.stat, st,
+                        g.d_trow + t0));
+        g.launches += 3;
+        if (span) {  // as trials_range: leftover trials on the single-row shape
+            const int rows = kHarmShapes[harm_shape - 1].rows;
+            const int rem = rows > 1 ? b % rows : 0, bm = b - rem;
+            if (bm > 0) {
+                PSX_TRY(launch_harm(F, harm_shape, pp, Bp, (unsigned)Bp, pk, t0, bm, g.d_rec,
+                                    g.d_cnt, (unsigned)g.rec_cap, st, &hmaps[0]));
+                ++g.launches;
+            }
+            if (rem > 0) {
+                PSX_TRY(launch_harm(F, kHarmDefaultShape, pp + (size_t)bm * Bp, Bp, (unsigned)Bp,
+                                    pk, t0 + bm, rem, g.d_rec, g.d_cnt, (unsigned)g.rec_cap, st));
+                ++g.launches;
+            }
+        }
+        t0 += b;
+        ++g.groups;
+    }
+    // the hit counter, and every row's prologue counters (baseline flags)
+    PSX_CUDA(cudaMemcpyAsync(g.h_cnt, g.d_cnt, sizeof(unsigned) * 2, cudaMemcpyDeviceToHost, st));
+    PSX_CUDA(cudaMemcpyAsync(g.h_cnt + 2, g.count, sizeof(unsigned) * 16 * (size_t)cnt,
+                             cudaMemcpyDeviceToHost, st));
+    PSX_CUDA(cudaEventRecord(g.done, st));
+    for (int i = 0; i < cnt; ++i) PSX_CUDA(cudaEventRecord(g.slots[i].done, st));
+    return PSX_OK;
+}
+
+// Waits for a spanning chunk, grows its record buffer and runs its trials
+// again if they overflowed it, and splits the records into one job per DM
+// trial (trial indices back to each DM trial's own); a DM trial whose
+// baseline needed more passes than the device loop makes runs again alone
+// through the per-DM path with the host loop.
+int psx_search::finish_span(GroupSet& g, int cnt, std::vector<DmRecords>& jobs)
+{
+    for (int attempt = 0;; ++attempt) {
+        const auto t_wait = std::chrono::steady_clock::now();
+        PSX_CUDA(cudaEventSynchronize(g.done));
+        prof.host_wait_ms += ms_since(t_wait);
+        if (g.h_cnt[1] != 0) {
+            set_error("search: harmonic-sum staging did not complete (status 0x%x)", g.h_cnt[1]);
+            return PSX_ERR_CUDA;
+        }
+        if (g.h_cnt[0] <= g.rec_cap) break;
+        if (attempt == 2) {
+            set_error("search: could not complete DM trials %d..", g.slots[0].dm_idx);
+            return PSX_ERR_OVERFLOW;
+        }
+        PSX_TRY(grow_span_records(g, g.h_cnt[0]));
+        PSX_TRY(trials_span(g, cnt));
+    }
+    const size_t nrec = g.h_cnt[0];
+    if (nrec) {
+        PSX_CUDA(cudaStreamWaitEvent(cst, g.done, 0));
+        PSX_CUDA(cudaMemcpyAsync(g.h_rec, g.d_rec, sizeof(int4) * nrec, cudaMemcpyDeviceToHost,
+                                 cst));
+        PSX_CUDA(cudaStreamSynchronize(cst));
+    }
+    jobs.assign(cnt, DmRecords{});
+    for (int i = 0; i < cnt; ++i) {
+        const Slot& sl = g.slots[i];
+        jobs[i].accs = sl.accs;
+        jobs[i].dm = sl.dm;
+        jobs[i].dm_idx = sl.dm_idx;
+    }
+    for (size_t r = 0; r < nrec; ++r) {
+        int4 q = g.h_rec[r];
+        if (q.x < 0 || q.x >= g.off[cnt]) continue;
+        const int i = (int)(std::upper_bound(g.off.begin(), g.off.begin() + cnt + 1, q.x) -
+                            g.off.begin()) - 1;
+        q.x -= g.off[i];
+        jobs[i].recs.push_back(q);
+    }
+    const int T = g.off[cnt];
+    info.ntrials += T;
+    info.nbatches += g.groups;
+    info.kernel_launches += g.launches + g.slots[0].launches;
+    info.fft_launches += g.slots[0].ffts;
+    info.above_threshold += (long long)nrec;
+    for (int i = 0; i < cnt; ++i) {
+        const unsigned* c = g.h_cnt + 2 + 16 * (size_t)i;
+        Slot& sl = g.slots[i];
+        info.baseline_passes = (int)c[3];
+        if (c[2] != 0) {  // rare: the baseline loop needs the host
+            info.ntrials -= (int)sl.accs.size();
+            info.above_threshold -= (long long)jobs[i].recs.size();
+            sl.host_baseline = true;
+            PSX_TRY(enqueue(sl, sl.series, sl.nsamps, sl.on_device, sl.dm, sl.dm_idx));
+            PSX_TRY(finish(sl, jobs[i]));
+        }
+    }
+    last_dm = &g.slots[cnt - 1];
+    return PSX_OK;
+}
+
 // Group sets, made on the first call that groups: per set, the per-DM
 // buffers of G slots as rows of contiguous arrays (row strides N, 2 Bp,
 // the median scratch, 2 nb, 2, 8, 16 and 2 elements), the batch-G plans
@@ -953,6 +1140,13 @@ int psx_search::alloc_groups_sets()
         PSX_CUDA(cudaMemsetAsync(g.Xp, 0, sizeof(float) * 2 * Bp * G, st));
         PSX_TRY(g.r2c.create(N, G, PSX_FFT_R2C, N, Bp));
         PSX_TRY(g.c2r.create(N, G, PSX_FFT_C2R, Bp, N));
+        if (use_f4) {  // the spanning trial schedule's counters and event
+            PSX_CUDA(cudaMalloc((void**)&g.d_cnt, sizeof(unsigned) * 4));
+            PSX_CUDA(cudaMallocHost(&g.h_cnt, sizeof(unsigned) * (2 + 16 * (size_t)G)));
+            PSX_CUDA(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+            PSX_TRY(grow_span_records(g, (size_t)1 << 20));
+            PSX_TRY(grow_span_tables(g, 256));
+        }
         g.slots.resize(G);
         for (int i = 0; i < G; ++i) {
             Slot& sl = g.slots[i];
@@ -995,6 +1189,16 @@ void psx_search::free_groups()
             delete s.c2r;
         }
         g.slots.clear();
+        for (void* q : {(void*)g.d_rec, (void*)g.d_cnt, (void*)g.d_ktab, (void*)g.d_trow})
+            if (q) cudaFree(q);
+        for (void* q : {(void*)g.h_rec, (void*)g.h_cnt, (void*)g.h_ktab, (void*)g.h_trow})
+            if (q) cudaFreeHost(q);
+        if (g.done) cudaEventDestroy(g.done);
+        g.d_rec = g.h_rec = nullptr;
+        g.d_cnt = g.h_cnt = g.d_trow = g.h_trow = nullptr;
+        g.d_ktab = g.h_ktab = nullptr;
+        g.rec_cap = g.tab_cap = 0;
+        g.done = nullptr;
         void* dev[] = {g.tim, g.Xp, g.med, g.part, g.sums, g.stat, g.count, g.mean};
         for (void* q : dev)
             if (q) cudaFree(q);
@@ -1712,8 +1916,10 @@ size_t psx_search_footprint(const psx_search_config* c)
     const size_t G = (size_t)group_rows_for(c);
     if (G >= 2)
         bytes += 2 * G *
-                 (sizeof(float) * (N + 2 * Bp) + median_scratch_bytes(B) +
-                  sizeof(int4) * ((size_t)1 << 18) + 2 * sizeof(float) * 2 * Bp);
+                     (sizeof(float) * (N + 2 * Bp) + median_scratch_bytes(B) +
+                      sizeof(int4) * ((size_t)1 << 18) + 2 * sizeof(float) * 2 * Bp) +
+                 // the spanning schedule's first record buffer per set
+                 (effective_form(c) == 3 ? 2 * sizeof(int4) * ((size_t)1 << 20) : 0);
     return bytes;
 }
 
@@ -2121,11 +2327,7 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
             }
         });
     // (no early return from here until the collector is joined)
-    auto finish_dm = [&](int d, Slot& sl) -> int {
-        s->last_dm = &sl;
-        psx_search::DmRecords job;
-        const int r = s->finish(sl, job);
-        if (r != PSX_OK) return r;
+    auto push_job = [&](int d, psx_search::DmRecords& job) {
         if (ndm == 1) {
             take(d, job);
         } else {
@@ -2133,6 +2335,13 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
             jobs.emplace_back(d, std::move(job));
             jcv.notify_one();
         }
+    };
+    auto finish_dm = [&](int d, Slot& sl) -> int {
+        s->last_dm = &sl;
+        psx_search::DmRecords job;
+        const int r = s->finish(sl, job);
+        if (r != PSX_OK) return r;
+        push_job(d, job);
         return PSX_OK;
     };
     const bool on_dev = series_on_device != 0;
@@ -2142,8 +2351,11 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
         // Grouped prologues: chunks of G DM trials alternate between the two
         // group sets; chunk c + 1's batched prologue (on slot (c + 1) & 1's
         // stream) runs while chunk c's trials run, as the per-DM slots do.
+        // With the two-pass transform the chunk's trials also run as one
+        // list, in launch groups across its DM trials (trials_span).
         rc = s->alloc_groups();
         const int nchunks = (ndm + G - 1) / G;
+        const bool spanning = s->span_mode();
         auto enqueue_chunk = [&](int c) -> int {
             const auto t_host = std::chrono::steady_clock::now();
             GroupSet& g = s->gset[c & 1];
@@ -2153,7 +2365,19 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
                 PSX_TRY(s->prep(g.slots[i], series[d0 + i], nsamps, on_dev, dms[d0 + i],
                                 dm_idx ? dm_idx[d0 + i] : d0 + i));
             PSX_TRY(s->prologue_group(g, cnt, s->slot[c & 1].pst));
-            for (int i = 0; i < cnt; ++i) PSX_TRY(s->enqueue_trials(g.slots[i]));
+            if (spanning) {
+                g.off.assign((size_t)cnt + 1, 0);
+                for (int i = 0; i < cnt; ++i) g.off[i + 1] = g.off[i] + (int)g.slots[i].accs.size();
+                PSX_TRY(s->grow_span_tables(g, (size_t)g.off[cnt]));
+                for (int i = 0; i < cnt; ++i)
+                    for (int t = g.off[i]; t < g.off[i + 1]; ++t) {
+                        g.h_ktab[t] = g.slots[i].h_ktab[t - g.off[i]];
+                        g.h_trow[t] = (unsigned)i;
+                    }
+                PSX_TRY(s->trials_span(g, cnt));
+            } else {
+                for (int i = 0; i < cnt; ++i) PSX_TRY(s->enqueue_trials(g.slots[i]));
+            }
             s->prof.host_enqueue_ms += ms_since(t_host);
             return PSX_OK;
         };
@@ -2161,8 +2385,14 @@ int psx_search_block(psx_search* s, const float* const* series, size_t nsamps,
         for (int c = 0; c < nchunks && rc == PSX_OK; ++c) {
             if (c + 1 < nchunks) rc = enqueue_chunk(c + 1);
             const int d0 = c * G, cnt = std::min(G, ndm - d0);
-            for (int i = 0; i < cnt && rc == PSX_OK; ++i)
-                rc = finish_dm(d0 + i, s->gset[c & 1].slots[i]);
+            if (spanning && rc == PSX_OK) {
+                std::vector<psx_search::DmRecords> cj;
+                rc = s->finish_span(s->gset[c & 1], cnt, cj);
+                for (int i = 0; i < cnt && rc == PSX_OK; ++i) push_job(d0 + i, cj[i]);
+            } else {
+                for (int i = 0; i < cnt && rc == PSX_OK; ++i)
+                    rc = finish_dm(d0 + i, s->gset[c & 1].slots[i]);
+            }
         }
         s->info.group_dms = G;
     } else {
