@@ -107,14 +107,14 @@ def test_default_rule_and_profile(S):
 
 
 def test_grouped_record_growth(S):
-    """A low threshold overflows the grouped slots' first record buffers
-    (2^18 records): the DM trial runs again with a larger buffer, through
-    the per-DM prologue, and the result is as if it had run once."""
+    """A threshold of zero overflows the first record buffers (2^20 records
+    of a chunk's trial list, 2^18 of a grouped slot): the trials run again
+    with a larger buffer, and the result is as if they had run once."""
     n, ts = 1 << 19, 64e-6
     xs, dms = _block(S, n, ts, n, 5, 80)
-    kw = dict(acc_lo=-30.0, acc_hi=30.0, nharmonics=4, min_snr=0.3, batch=8)
+    kw = dict(acc_lo=-30.0, acc_hi=30.0, nharmonics=4, min_snr=0.0, batch=8)
     ref, info0, _ = _run(S, n, ts, xs, dms, 1, **kw)
-    assert info0["above_threshold"] > 5 * (1 << 18)  # so one DM trial at least overflows
+    assert info0["above_threshold"] > 5 * (1 << 20)  # over 2^21 per chunk of two
     got, info2, _ = _run(S, n, ts, xs, dms, 2, **kw)
     assert info2["group_dms"] == 2
     _equal(ref, got)
