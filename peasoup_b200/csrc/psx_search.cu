@@ -1106,7 +1106,8 @@ int psx_search::finish_span(GroupSet& g, int cnt, std::vector<DmRecords>& jobs)
     return PSX_OK;
 }
 
-// Group sets, made on the first call that groups: per set, the per-DM
+// Group sets, made when the instance is created (where its configuration
+// can group): per set, the per-DM
 // buffers of G slots as rows of contiguous arrays (row strides N, 2 Bp,
 // the median scratch, 2 nb, 2, 8, 16 and 2 elements), the batch-G plans
 // of the prologue's transforms, and per slot its own record buffer, factor
@@ -1910,7 +1911,7 @@ size_t psx_search_footprint(const psx_search_config* c)
         bytes += sizeof(float) * 2 * Bp * 6 + sizeof(float2) * Fft4Plan::table_floats2(N);
     else
         bytes += sizeof(float) * 2 * Bp * (2 * b * L + 6);
-    // two group sets of G rows (made on the first grouped call): series,
+    // two group sets of G rows (made with the instance): series,
     // prologue spectra, median scratch, each slot's first record buffer, and
     // about one batch's worth of transform work area per batch-G plan
     const size_t G = (size_t)group_rows_for(c);
@@ -2105,6 +2106,9 @@ int psx_search_create(const psx_search_config* cfg, psx_search** out)
     s->set_st[0] = s->st;
     s->set_st2[0] = s->st2;
     for (int k = 0; k < 2; ++k) s->set_pst[0][k] = s->slot[k].pst;
+    // group sets made now (their bytes are in the footprint), so a call
+    // that groups does not pay for them on first use
+    if ((rc = s->alloc_groups()) != PSX_OK) return fail(rc);
     *out = s;
     return PSX_OK;
 }
