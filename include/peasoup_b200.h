@@ -425,7 +425,10 @@ typedef struct {
                                   call whose per-DM prologues (baseline
                                   removal through the inverse transform) run
                                   as one batch of row-indexed launches and
-                                  batched cuFFT plans.  0 = default: 4 when
+                                  batched cuFFT plans (with fft_form 3 their
+                                  acceleration trials then run as one list,
+                                  in launch groups across the DM trials).
+                                  0 = default: 4 when
                                   fft_size <= 2^22 and the call's DM trials
                                   average at most 32 acceleration trials,
                                   else off; 1 = off; 2..16 = that many
