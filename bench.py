@@ -386,7 +386,7 @@ def _served_series(r, seed):
     return x
 
 
-def run_served(nreq, rank, log_prefix, policy="least_work", nslots=SERVED_SLOTS):
+def run_served(nreq, rank, log_prefix, policy="exclusive", nslots=SERVED_SLOTS):
     """The served workload (Poisson arrivals, uneven requests) through the
     C++ server under two scheduling policies, and every request alone on a
     one-slot server before and after them: latency from arrival and from
