@@ -21,10 +21,12 @@
 //     as zt[k1 * C + k2] = Z[k1 + R k2];
 //   unpack (k_unpack_form_norm_t): a CTA stages a 32-row x 32-column tile of
 //     zt and the tile of its mirror bins through shared memory with
-//     coalesced loads; then lanes take consecutive k1 (30 output lanes and
-//     two helpers per warp), so the neighbour bin k-1 each interbinned value
-//     needs is the previous lane's, and the mirror bin M-k the next lane's.
-// All twiddles come from tables rounded once from double precision.
+//     coalesced asynchronous copies; then lanes take consecutive k1 (30
+//     output lanes and two helpers per warp), so the neighbour bin k-1 each
+//     interbinned value needs is the previous lane's, and the mirror bin
+//     M-k the next lane's.
+// All twiddles come from tables rounded once from double precision (pass 1
+// takes some as the product of two entries, to read fewer of them).
 #include <cuda_runtime.h>
 #include <cmath>
 #include <utility>
@@ -190,6 +192,18 @@ __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THRE
     const unsigned col = threadIdx.x % W, t = threadIdx.x / W;  // t in [0, TPC)
     const unsigned c = blockIdx.x * W + col;
     const double k = ktab[blockIdx.y], size = (double)n;
+    // Table entries of the four-step twiddle (last step below), loaded first
+    // so that their L2 latency passes under the three stages; for R = 4096
+    // (one stage-3 butterfly per thread, fifteen entries W_M^(TPC c U q))
+    // those are loaded where they are used instead.
+    constexpr bool EARLY = U > 1;
+    const float2 wt = __ldg(tab + offQ + (size_t)t * C + c);
+    float2 pu[U], pq[R3];
+#pragma unroll
+    for (int u = 1; u < U; ++u) pu[u] = __ldg(tab + offP + (size_t)u * C + c);
+    if constexpr (EARLY)
+#pragma unroll
+        for (int q = 1; q < R3; ++q) pq[q] = __ldg(tab + offP + (size_t)(U * q) * C + c);
     float2 v[16];
     // stage 1 (radix 16, span 1): rows e = t + J q of column c, where
     // z[e C + c] = (x'[2m], x'[2m+1]); out[16 t + q]
@@ -223,8 +237,17 @@ __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THRE
     }
     __syncthreads();
     if (J == TPC || t < (unsigned)J) {
+        // W_256^(m q) = W_256^(m (q mod 4)) W_256^(4 m (q div 4)): six table
+        // entries instead of fifteen
+        const float2* a2 = tab + offA2 + (t & 15);
+        const float2 one = make_float2(1.0f, 0.0f);
+        const float2 lo[4] = {one, __ldg(a2 + 16), __ldg(a2 + 32), __ldg(a2 + 48)};
+        const float2 hi[4] = {one, __ldg(a2 + 64), __ldg(a2 + 128), __ldg(a2 + 192)};
 #pragma unroll
-        for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], __ldg(tab + offA2 + q * 16 + (t & 15)));
+        for (int q = 1; q < 16; ++q) {
+            const int ql = q & 3, qh = q >> 2;
+            v[q] = cmul(v[q], !qh ? lo[ql] : !ql ? hi[qh] : cmul(lo[ql], hi[qh]));
+        }
         dft<16>(v);
         const unsigned base2 = (t >> 4) * 256 + (t & 15);
 #pragma unroll
@@ -254,17 +277,20 @@ __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THRE
         for (int q = 0; q < R3; ++q) v[R3 * u + q] = b[q];
     }
     // four-step twiddle W_M^(c k1), k1 = t + TPC w (w = u + U q):
-    // W_M^(c t) * W_M^(TPC c w)
-    const float2 wt = __ldg(tab + offQ + (size_t)t * C + c);
+    // W_M^(c t) * W_M^(TPC c U q) * W_M^(TPC c u), from U + R3 - 1 table
+    // entries of W_M^(TPC c w) instead of U R3 - 1
     float2* yo = y + (size_t)blockIdx.y * ypitch;
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+    for (int q = 0; q < R3; ++q) {
+        const float2 wq =
+            q ? cmul(wt, EARLY ? pq[q] : __ldg(tab + offP + (size_t)(U * q) * C + c)) : wt;
 #pragma unroll
-        for (int q = 0; q < R3; ++q) {
+        for (int u = 0; u < U; ++u) {
             const unsigned w = u + U * q;
-            const float2 tw = w ? cmul(wt, __ldg(tab + offP + (size_t)w * C + c)) : wt;
+            const float2 tw = u ? cmul(wq, pu[u]) : wq;
             yo[(size_t)(t + TPC * w) * C + c] = cmul(v[R3 * u + q], tw);
         }
+    }
 }
 
 // ------------------------------------------------------------- pass 2
@@ -366,20 +392,37 @@ __device__ __forceinline__ void unpack_one(float2 a, float2 w, float cs, float s
     hi = make_float2(ar - u, -ai - v);
 }
 
+// 8-byte asynchronous copy from global to shared memory: no register holds
+// the element while it is in flight.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Grid (ceil(R/30) * C/64, trials), 256 threads, R the row count of the
 // four-step split (1024 or 768).  CTA (wk, g): rows
 // k1 = 30 wk - 1 + r, r < 32 ("virtual" rows -1 and >= R continue into
 // the neighbouring columns), columns k2 = 32 g .. 32 g + 31 < C/2: the bins
 // j = k1 + R k2 < M/2 and their mirrors M - j.  Both 32 x 32 tiles are
-// loaded coalesced (a warp reads 32 consecutive columns of a row) into
-// padded shared memory; warp w then takes columns 32 g + 4 w .. + 3 with
+// copied coalesced (a warp reads 32 consecutive columns of a row) into
+// padded shared memory by asynchronous copies; warp w then takes columns 32 g + 4 w .. + 3 with
 // lane = r, and lanes 1..30 write bin j (interbinned with lane-1's X[j-1])
 // and bin M-j (with lane+1's X[M-j-1]); bin M/2 comes from thread 0 of
 // block 0.  The split-step rotation (cos, sin)(pi j / M) is the product of
 // tabulated (cos, sin)(pi k1 / M) (k1 = -1 .. 1055, rv[k1 + 1]) and
 // (cos, sin)(pi k2 / C) (rk[k2]).
 template <unsigned R>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 8)  // 8 CTAs per SM: 32 registers
     k_unpack_form_norm_t(const float2* __restrict__ zt, size_t zpitch, unsigned C,
                          float* __restrict__ p, size_t ppitch,
                          const float2* __restrict__ rv, const float2* __restrict__ rk,
@@ -401,9 +444,11 @@ __global__ void __launch_bounds__(256)
         for (int e = 0; e < 4; ++e) {
             const unsigned r = warp + 8 * e;  // tile row; lane = tile column
             const unsigned v = (unsigned)v0 + r;
-            lo_t[r][lane] = z[(size_t)v * C + k2a + lane];
-            mi_t[r][lane] = z[(size_t)(R - v) * C + (C - 1 - k2a - lane)];
+            cp_async8(&lo_t[r][lane], z + (size_t)v * C + k2a + lane);
+            cp_async8(&mi_t[r][lane], z + (size_t)(R - v) * C + (C - 1 - k2a - lane));
         }
+        cp_async_commit();
+        cp_async_wait<0>();
     } else
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
