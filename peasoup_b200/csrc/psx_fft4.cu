@@ -26,7 +26,8 @@
 //     interbinned value needs is the previous lane's, and the mirror bin
 //     M-k the next lane's.
 // All twiddles come from tables rounded once from double precision (pass 1
-// takes some as the product of two entries, to read fewer of them).
+// takes some as the product of two entries, or of one entry and an exact
+// multiple of pi/8, to read fewer of them).
 #include <cuda_runtime.h>
 #include <cmath>
 #include <utility>
@@ -261,13 +262,26 @@ __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THRE
 #pragma unroll
         for (int q = 0; q < R3; ++q)
             v[R3 * u + q] = sm_a[swz_a<W>(t + TPC * u + 256 * q) * W + col];
+    // With R = 16 TPC, W_R^(j q) = W_R^(t q) W_16^(u q): R3 - 1 table entries
+    // and exact multiples of pi/8 instead of U (R3 - 1) entries (R = 768
+    // reads them all).
+    constexpr bool SPLIT3 = R == 16 * TPC;
+    float2 w3[R3];
+    if constexpr (SPLIT3)
+#pragma unroll
+        for (int q = 1; q < R3; ++q) w3[q] = __ldg(tab + offA3 + q * 256 + t);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         float2 b[R3];
 #pragma unroll
-        for (int q = 0; q < R3; ++q)
-            b[q] = q ? cmul(v[R3 * u + q], __ldg(tab + offA3 + q * 256 + t + TPC * u))
-                     : v[R3 * u];
+        for (int q = 0; q < R3; ++q) {
+            if (!q)
+                b[q] = v[R3 * u];
+            else if constexpr (SPLIT3)
+                b[q] = twiddle(cmul(v[R3 * u + q], w3[q]), u * q, 16);
+            else
+                b[q] = cmul(v[R3 * u + q], __ldg(tab + offA3 + q * 256 + t + TPC * u));
+        }
         if constexpr (R3 == 3) {
             dft3(b[0], b[1], b[2]);
         } else {
