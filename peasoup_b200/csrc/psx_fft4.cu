@@ -200,11 +200,15 @@ __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THRE
     constexpr bool EARLY = U > 1;
     const float2 wt = __ldg(tab + offQ + (size_t)t * C + c);
     float2 pu[U], pq[R3];
+    if constexpr (EARLY) {
+        // P = W_M^(TPC c): P^u and (P^U)^q as products of two entries
+        pu[1] = __ldg(tab + offP + (size_t)C + c);
+        pq[1] = __ldg(tab + offP + (size_t)U * C + c);
 #pragma unroll
-    for (int u = 1; u < U; ++u) pu[u] = __ldg(tab + offP + (size_t)u * C + c);
-    if constexpr (EARLY)
+        for (int u = 2; u < U; ++u) pu[u] = cmul(pu[u / 2], pu[u - u / 2]);
 #pragma unroll
-        for (int q = 1; q < R3; ++q) pq[q] = __ldg(tab + offP + (size_t)(U * q) * C + c);
+        for (int q = 2; q < R3; ++q) pq[q] = cmul(pq[q / 2], pq[q - q / 2]);
+    }
     float2 v[16];
     // stage 1 (radix 16, span 1): rows e = t + J q of column c, where
     // z[e C + c] = (x'[2m], x'[2m+1]); out[16 t + q]
@@ -291,8 +295,9 @@ __global__ void __launch_bounds__(ColShape<R>::THREADS, 1024 / ColShape<R>::THRE
         for (int q = 0; q < R3; ++q) v[R3 * u + q] = b[q];
     }
     // four-step twiddle W_M^(c k1), k1 = t + TPC w (w = u + U q):
-    // W_M^(c t) * W_M^(TPC c U q) * W_M^(TPC c u), from U + R3 - 1 table
-    // entries of W_M^(TPC c w) instead of U R3 - 1
+    // W_M^(c t) * W_M^(TPC c U q) * W_M^(TPC c u), from the entries of
+    // W_M^(c t), W_M^(TPC c) and W_M^(TPC c U) instead of U R3 (R = 4096:
+    // W_M^(c t) and the fifteen W_M^(TPC c q))
     float2* yo = y + (size_t)blockIdx.y * ypitch;
 #pragma unroll
     for (int q = 0; q < R3; ++q) {
