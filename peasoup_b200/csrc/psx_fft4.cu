@@ -343,9 +343,24 @@ __device__ __forceinline__ void row_stage(float2* s, unsigned t, const float2* _
     for (int u = 0; u < G; ++u) {
         const unsigned jb = t + u * T, m = jb % NS;
         float2 w[R];
+        if constexpr (R == 16) {
+            // W^(m q) = W^(m (q mod 4)) W^(4 m (q div 4)): six entries, not 15
+            const float2 one = make_float2(1.0f, 0.0f);
+            const float2 lo[4] = {one, __ldg(tw + NS + m), __ldg(tw + 2 * NS + m),
+                                  __ldg(tw + 3 * NS + m)};
+            const float2 hi[4] = {one, __ldg(tw + 4 * NS + m), __ldg(tw + 8 * NS + m),
+                                  __ldg(tw + 12 * NS + m)};
+            w[0] = v[u * R];
 #pragma unroll
-        for (int q = 0; q < R; ++q)
-            w[q] = q ? cmul(v[u * R + q], __ldg(tw + q * NS + m)) : v[u * R];
+            for (int q = 1; q < 16; ++q) {
+                const int ql = q & 3, qh = q >> 2;
+                w[q] = cmul(v[u * R + q], !qh ? lo[ql] : !ql ? hi[qh] : cmul(lo[ql], hi[qh]));
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; ++q)
+                w[q] = q ? cmul(v[u * R + q], __ldg(tw + q * NS + m)) : v[u * R];
+        }
         dft<R>(w);
         const unsigned base = (jb / NS) * NS * R + m;
 #pragma unroll
@@ -380,8 +395,18 @@ __global__ void __launch_bounds__(RowShape<LOGC>::THREADS, 1024 / RowShape<LOGC>
     constexpr int NSL = C / 16;
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = s[pad16(t + q * T)];
+    {
+        // W_C^(t q) from six entries, as in row_stage
+        const float2* tl = tw + S::OFF_LAST + t;
+        const float2 one = make_float2(1.0f, 0.0f);
+        const float2 lo[4] = {one, __ldg(tl + NSL), __ldg(tl + 2 * NSL), __ldg(tl + 3 * NSL)};
+        const float2 hi[4] = {one, __ldg(tl + 4 * NSL), __ldg(tl + 8 * NSL), __ldg(tl + 12 * NSL)};
 #pragma unroll
-    for (int q = 1; q < 16; ++q) v[q] = cmul(v[q], __ldg(tw + S::OFF_LAST + q * NSL + t));
+        for (int q = 1; q < 16; ++q) {
+            const int ql = q & 3, qh = q >> 2;
+            v[q] = cmul(v[q], !qh ? lo[ql] : !ql ? hi[qh] : cmul(lo[ql], hi[qh]));
+        }
+    }
     dft<16>(v);
     float2* zr = zt + (size_t)blockIdx.y * zpitch + (size_t)row * C;
 #pragma unroll
